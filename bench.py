@@ -1,0 +1,400 @@
+#!/usr/bin/env python
+"""Connected-components benchmark on B200 (one JSON line on rank 0).
+
+Workload (default ``rmat24``): plain single-graph CC on a seeded R-MAT graph,
+scale 24 (16,777,216 vertices), edge factor 16, a/b/c/d = .57/.19/.19/.05,
+symmetrised with self loops and duplicates removed, uint32 CSR - the
+reference's single-GPU headline configuration.  ``grid8192`` is the
+8192 x 8192 4-neighbour grid with 10% of edges deleted.
+
+A step is one full solve (labels = min vertex id per component) of the
+device-resident graph through ccgpu_local_cc.  ``e2e`` repeats the metric
+through the reference-facing call compute_connected_components_pthreads with
+pinned host buffers: the CSR copy to HBM and the label copy back are inside
+its timed region.  ``cpu_baseline`` and ``--impl reference`` time the
+reference's own compute_connected_components_pthreads (compiled unmodified
+into oracle/_ref) on this machine's host cores.
+
+Metric: GTEPS = unique undirected edges / solve time (higher is better).
+Multi-GPU (torchrun): every rank solves its own graph (seed + rank), no
+collective on the data path; value = all ranks' edges / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "rmat24": dict(kind="rmat", scale=24, ef=16),
+    "rmat22": dict(kind="rmat", scale=22, ef=16),
+    "rmat20": dict(kind="rmat", scale=20, ef=16),
+    "grid8192": dict(kind="grid", rows=8192, cols=8192, p=0.1),
+    "grid2048": dict(kind="grid", rows=2048, cols=2048, p=0.1),
+}
+L2_BYTES = 126 * 1024 * 1024
+FALLBACK_HBM_GBS = 6650.0
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def make_graph(torch, wl, seed):
+    from cc_mpi_b200 import graphs
+    spec = WORKLOADS[wl]
+    if spec["kind"] == "rmat":
+        return graphs.rmat_csr_torch(torch, spec["scale"], spec["ef"], seed=seed)
+    return graphs.grid_csr_torch(torch, spec["rows"], spec["cols"], spec["p"], seed=seed)
+
+
+def workload_config(wl, n, m):
+    spec = dict(WORKLOADS[wl])
+    cfg = {"workload": wl, "vertices": n, "undirected_edges": m // 2, "csr_entries": m}
+    if spec["kind"] == "rmat":
+        cfg.update(graph=f"R-MAT scale {spec['scale']}, edge factor {spec['ef']}, "
+                         "a/b/c/d=.57/.19/.19/.05, seeded id permutation")
+    else:
+        cfg.update(graph=f"{spec['rows']}x{spec['cols']} 4-neighbour grid, "
+                         f"{int(spec['p'] * 100)}% of edges deleted")
+    return cfg
+
+
+class ClockSampler:
+    """Polls NVML (read-only) from a thread while the timed region runs."""
+
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
+               0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown",
+               0x2: "applications_clocks_setting", 0x1: "gpu_idle"}
+
+    def __init__(self, index):
+        self.samples, self.reasons = [], 0
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self.ok = False
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception as e:  # pragma: no cover - depends on the driver
+            log("clock sampler unavailable:", e)
+
+    def _reasons(self):
+        nv = self.nv
+        for fn in ("nvmlDeviceGetCurrentClocksEventReasons",
+                   "nvmlDeviceGetCurrentClocksThrottleReasons"):
+            if hasattr(nv, fn):
+                return getattr(nv, fn)(self.h)
+        return 0
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(self.nv.nvmlDeviceGetClockInfo(self.h, self.nv.NVML_CLOCK_SM))
+                self.reasons |= int(self._reasons())
+            except Exception:
+                break
+            time.sleep(0.001)
+
+    def __enter__(self):
+        if self.ok:
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+        return self
+
+    def __exit__(self, *exc):
+        if self.ok:
+            self._stop.set()
+            self.t.join()
+
+    def summary(self):
+        if not self.ok or not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"]}
+        names = [v for k, v in self.REASONS.items() if self.reasons & k and k != 0x1]
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": names, "samples": len(self.samples)}
+
+
+def read_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def algorithmic_bytes(torch, rp_d, n, m, k, st):
+    """Bytes each kernel must move per launch (see the roofline section of
+    the design notes): row pointers, the column entries actually read and
+    the own-label read/write; neighbour-label gathers are cache-served and
+    not counted."""
+    deg = rp_d[1:] - rp_d[:-1]
+    sampled = int(torch.clamp(deg, max=k).sum().item()) if k > 0 else 0
+    return {
+        "init": 4 * n,
+        "sample": 8 * (n + 1) + 4 * sampled + 4 * n,
+        "compress": 8 * n,
+        "giant": 4 * 1024,
+        "link_rows": 4 * n + 8 * int(st.finish_rows) + 4 * int(st.finish_edges),
+        "link_heavy": 4 * 0,
+        "final_compress": 8 * n,
+    }
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's own CPU code on this host."""
+    if rank != 0:
+        return 0
+    import numpy as np
+    import torch
+    import oracle
+    torch.cuda.set_device(0)
+    rp_d, col_d = make_graph(torch, args.workload, args.seed)
+    rp = rp_d.cpu().numpy().view(np.uint64)
+    col = col_d.cpu().numpy().view(np.uint32)
+    del rp_d, col_d
+    n, m = len(rp) - 1, int(rp[-1])
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        oracle.ref_pthreads_labels(rp, col, threads, 8192)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        oracle.ref_pthreads_labels(rp, col, threads, 8192)
+        times.append(time.perf_counter() - t0)
+    t = sum(times) / len(times)
+    gteps = (m / 2) / t / 1e9
+    line = {
+        "impl": "reference", "metric": "CC GTEPS", "value": gteps, "unit": "GTEPS",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic", "config": workload_config(args.workload, n, m),
+        "cpu_baseline": {"value": gteps, "unit": "GTEPS", "cores": threads, "kind": "reference",
+                         "sample": f"full graph, {args.steps} solves, chunk 8192"},
+        "e2e": {"value": gteps, "unit": "GTEPS", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def cpu_baseline(rp, col, budget_s=20.0):
+    import oracle
+    threads = os.cpu_count() or 1
+    m = int(rp[-1])
+    times = []
+    t_start = time.perf_counter()
+    if oracle.have_ref():
+        kind = "reference"
+        while len(times) < 3 and time.perf_counter() - t_start < budget_s:
+            t0 = time.perf_counter()
+            oracle.ref_pthreads_labels(rp, col, threads, 8192)
+            times.append(time.perf_counter() - t0)
+        sample = f"full graph, {len(times)} solves, {threads} threads, chunk 8192"
+        used = threads
+    else:
+        kind = "port"
+        t0 = time.perf_counter()
+        oracle.lp_labels(rp, col)
+        times.append(time.perf_counter() - t0)
+        sample = "full graph, 1 solve, 1 thread (oracle label propagation)"
+        used = 1
+    t = min(times)
+    return {"value": (m / 2) / t / 1e9, "unit": "GTEPS", "cores": used, "kind": kind,
+            "sample": sample, "seconds_per_solve": t}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="rmat24")
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-verify", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+
+    import torch
+    import torch.distributed as dist
+    import datetime
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    if args.impl == "reference":
+        rc = run_reference(args, rank, world)
+        if world > 1:
+            dist.destroy_process_group()
+        return rc
+
+    import numpy as np
+    from cc_mpi_b200 import _lib, cc
+    L = _lib.lib()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    rp_d, col_d = make_graph(torch, args.workload, args.seed + rank)
+    torch.cuda.synchronize()
+    n, m = rp_d.numel() - 1, col_d.numel()
+    lab_d = torch.empty(n, dtype=torch.int32, device=dev)
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+    opts = _lib.opts()
+
+    # one checked solve: stats + device invariants + oracle on rank 0
+    st = cc.local_cc_device(rp_d, col_d, n, m, lab_d, opts, stats=True)
+    viol = cc.check_labels_device(rp_d, col_d, n, m, lab_d)
+    verified = None
+    rp_h = torch.empty(n + 1, dtype=torch.int64, pin_memory=True)
+    col_h = torch.empty(m, dtype=torch.int32, pin_memory=True)
+    rp_h.copy_(rp_d)
+    col_h.copy_(col_d)
+    rp_np = rp_h.numpy().view(np.uint64)
+    col_np = col_h.numpy().view(np.uint32)
+    if rank == 0 and not args.no_verify:
+        import oracle
+        want = oracle.uf_labels(rp_np, col_np)
+        got = lab_d.cpu().numpy().view(np.uint32)
+        verified = bool((got == want).all()) and viol == 0
+        if not verified:
+            log(f"VERIFY FAILED: {int((got != want).sum())} labels differ, {viol} violations")
+    bytes_per = algorithmic_bytes(torch, rp_d, n, m, opts.sample_rounds, st)
+
+    for _ in range(args.warmup):
+        flush.fill_(1)
+        cc.local_cc_device(rp_d, col_d, n, m, lab_d, opts, stream=sptr)
+    torch.cuda.synchronize()
+
+    k = L.ccgpu_prof_kernels()
+    names = [L.ccgpu_prof_name(i).decode() for i in range(k)]
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    _lib.check(L.ccgpu_prof_enable(None, 1))
+    _lib.check(L.ccgpu_prof_collect(None, None, None))
+    launches0 = L.ccgpu_ctx_launches(None)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            flush.fill_(i)  # evicts the labels from L2 between steps (not timed)
+            ev[i][0].record(stream)
+            cc.local_cc_device(rp_d, col_d, n, m, lab_d, opts, stream=sptr)
+            ev[i][1].record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    launches = L.ccgpu_ctx_launches(None) - launches0
+    ms = (C.c_double * k)()
+    cnt = (C.c_uint64 * k)()
+    _lib.check(L.ccgpu_prof_collect(None, ms, cnt))
+    _lib.check(L.ccgpu_prof_enable(None, 0))
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    t_ms = sum(step_ms) / len(step_ms)
+    if world > 1:
+        tt = torch.tensor([t_ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_ms = float(tt.item())
+    edges_all = (m // 2) * world
+    value = edges_all / (t_ms / 1e3) / 1e9
+
+    # per-kernel live timing -> dominant kernel roofline
+    per = {names[i]: (ms[i] / cnt[i], int(cnt[i])) for i in range(k) if cnt[i]}
+    dom = max(per, key=lambda kk: per[kk][0] * per[kk][1])
+    peak, peak_kind = read_peaks()
+    dom_bytes = bytes_per.get(dom, 0)
+    achieved = dom_bytes / (per[dom][0] / 1e3) / 1e9
+    total_bytes = sum(bytes_per.get(kk, 0) for kk in per)
+    whole = total_bytes / (t_ms / 1e3) / 1e9
+
+    # e2e through the reference-facing call with pinned host buffers
+    cc._bind()
+    lab_h = torch.empty(n, dtype=torch.int32, pin_memory=True)
+    g = _lib.CSRGraph()
+    g.n, g.m = n, m
+    g.row_ptr = C.cast(rp_h.data_ptr(), C.POINTER(C.c_uint64))
+    g.col_idx = C.cast(col_h.data_ptr(), C.POINTER(C.c_uint32))
+    L.ccb200_set_exit_on_error(0)
+    L.compute_connected_components_pthreads(C.byref(g), lab_h.data_ptr(), 0, 4096)  # warm
+    e2e_t = []
+    for _ in range(max(args.e2e_steps, 1)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        L.ccgpu_clear_error()
+        L.compute_connected_components_pthreads(C.byref(g), lab_h.data_ptr(), 0, 4096)
+        e2e_t.append(time.perf_counter() - t0)
+        if L.ccgpu_last_error():
+            raise RuntimeError(L.ccgpu_last_error().decode())
+    e2e_s = sum(e2e_t) / len(e2e_t)
+    if world > 1:
+        tt = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    e2e_ok = bool((lab_h.numpy() == lab_d.cpu().numpy()).all())
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(rp_np, col_np)
+
+    if rank == 0:
+        cfg = workload_config(args.workload, n, m)
+        cfg.update(components=int(st.components), giant_label=int(st.giant_label),
+                   l2="2x L2 buffer written between timed steps; col_idx > L2",
+                   opts={"chunk_size": opts.chunk_size, "sample_rounds": opts.sample_rounds,
+                         "heavy_degree": opts.heavy_degree, "skip_giant": opts.skip_giant},
+                   parallelism=f"replicas{world}" if world > 1 else "single",
+                   verified_vs_oracle=verified, e2e_labels_match=e2e_ok)
+        line = {
+            "metric": "CC GTEPS", "value": value, "unit": "GTEPS", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic", "config": cfg,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                         "traffic": None, "bytes_per_launch": dom_bytes,
+                         "ms_per_launch": per[dom][0],
+                         "whole_solve": {"algorithmic_bytes": total_bytes, "achieved": whole,
+                                         "frac": whole / peak}},
+            "kernels": {kk: {"ms": round(v[0], 5), "launches": v[1],
+                             "gbs": round(bytes_per.get(kk, 0) / (v[0] / 1e3) / 1e9, 1)}
+                        for kk, v in per.items()},
+            "cpu_baseline": cpu,
+            "e2e": {"value": (m // 2) * world / e2e_s / 1e9, "unit": "GTEPS",
+                    "h2d_bytes_per_step": 8 * (n + 1) + 4 * m, "d2h_bytes_per_step": 4 * n,
+                    "ms_per_step": e2e_s * 1e3,
+                    "api": "compute_connected_components_pthreads (pinned host CSR)"},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

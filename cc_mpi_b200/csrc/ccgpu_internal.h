@@ -1,0 +1,202 @@
+/*
+ * Internal helpers shared by the CUDA translation units: status/error
+ * plumbing, the per-context scratch arena, launch geometry and the
+ * union-find device primitives every solver uses.
+ */
+#ifndef CCGPU_INTERNAL_H
+#define CCGPU_INTERNAL_H
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+
+#include "ccgpu.h"
+
+/* ---------------------------------------------------------------- errors */
+
+int ccgpu_set_error(int status, const char *fmt, ...);
+int ccgpu_cuda_fail(cudaError_t e, const char *what, const char *file, int line);
+
+#define CC_CUDA(call)                                                          \
+    do {                                                                       \
+        cudaError_t e_ = (call);                                               \
+        if (e_ != cudaSuccess)                                                 \
+            return ccgpu_cuda_fail(e_, #call, __FILE__, __LINE__);             \
+    } while (0)
+
+#define CC_TRY(call)                                                           \
+    do {                                                                       \
+        int s_ = (call);                                                       \
+        if (s_ != CCGPU_OK)                                                    \
+            return s_;                                                         \
+    } while (0)
+
+#define CC_LAUNCH_CHECK() CC_CUDA(cudaGetLastError())
+
+/* ----------------------------------------------------------------- arena */
+
+/* A context's scratch: one grow-only device block carved into aligned
+ * pieces per call.  Growing frees and reallocates (a device-wide sync). */
+struct ccgpu_ctx {
+    int device;
+    void *base;
+    size_t cap;
+    size_t used;      /* bump pointer of the current call */
+    void *host_pinned; /* small pinned staging for stats read-back */
+    size_t host_cap;
+    int sm_count;
+    int owned_by_default;
+    unsigned long long *cell; /* 256-byte device cell for small reductions */
+    unsigned long long launches; /* kernels this context has launched */
+    struct cc_prof *prof;        /* per-kernel event timing, NULL = off */
+};
+
+/* Kernel ids for the launch profiler (names in runtime.cu). */
+enum {
+    CCK_INIT = 0,
+    CCK_SAMPLE,
+    CCK_COMPRESS,
+    CCK_GIANT,
+    CCK_LINK_ROWS,
+    CCK_LINK_HEAVY,
+    CCK_FINAL_COMPRESS,
+    CCK_COUNT_ROOTS,
+    CCK_CHECK,
+    CCK_DIST_SPLIT,
+    CCK_DIST_FILL,
+    CCK_DIST_REPS,
+    CCK_DIST_PAIRS,
+    CCK_SORT_HIST,
+    CCK_SORT_SCAN,
+    CCK_SORT_SCATTER,
+    CCK_DIST_DEDUP,
+    CCK_DIST_GHOSTS,
+    CCK_DIST_PLAN,
+    CCK_MERGE_INIT,
+    CCK_MERGE_HOOK,
+    CCK_MERGE_UPD,
+    CCK_MERGE_EXCH_PACK,
+    CCK_MERGE_EXCH_SCATTER,
+    CCK_DIST_LABELS,
+    CCK_DIST_BOUNDS,
+    CCK_SCAN,
+    CCK_BATCH,
+    CCK_MISC,
+    CCK_NUM
+};
+
+/* Records events around a launch when the context's profiler is on. */
+void cc_prof_mark(ccgpu_ctx *ctx, int kid, int end, cudaStream_t st);
+
+#define CC_KLAUNCH(ctx, kid, kernel, grid, block, smem, st, ...)               \
+    do {                                                                       \
+        if ((ctx)->prof)                                                       \
+            cc_prof_mark((ctx), (kid), 0, (st));                               \
+        kernel<<<(grid), (block), (smem), (st)>>>(__VA_ARGS__);                \
+        CC_LAUNCH_CHECK();                                                     \
+        (ctx)->launches++;                                                     \
+        if ((ctx)->prof)                                                       \
+            cc_prof_mark((ctx), (kid), 1, (st));                               \
+    } while (0)
+
+/* Layout helper: first pass (base == NULL) sums sizes, second pass hands
+ * out pointers.  Pieces are 256-byte aligned. */
+typedef struct {
+    char *base;
+    size_t off;
+} cc_carve;
+
+static inline void *cc_take(cc_carve *c, size_t bytes)
+{
+    size_t off = (c->off + 255) & ~(size_t)255;
+    c->off = off + bytes;
+    return c->base ? (void *)(c->base + off) : NULL;
+}
+
+int ccgpu_ctx_resolve(ccgpu_ctx **ctx);
+/* Ensures the context holds at least `bytes` of scratch; returns its base. */
+int ccgpu_ctx_reserve(ccgpu_ctx *ctx, size_t bytes, void **base);
+int ccgpu_ctx_pinned(ccgpu_ctx *ctx, size_t bytes, void **host);
+/* The context's 256-byte device cell (allocated on first use). */
+int ccgpu_ctx_cell(ccgpu_ctx *ctx, unsigned long long **cell);
+
+/* ------------------------------------------------------------ geometry */
+
+static inline unsigned cc_blocks(uint64_t work, unsigned per_block, unsigned cap)
+{
+    uint64_t b = (work + per_block - 1) / per_block;
+    if (b == 0)
+        b = 1;
+    if (b > cap)
+        b = cap;
+    return (unsigned)b;
+}
+
+/* ----------------------------------------------- union-find primitives */
+#ifdef __CUDACC__
+
+/* Parent reads go through L2 (.cg): L1 is not coherent across SMs and the
+ * parent array is written concurrently by other CTAs. */
+__device__ __forceinline__ uint32_t cc_ldp(const uint32_t *p, uint32_t i)
+{
+    return __ldcg(p + i);
+}
+
+/* Root of x with path halving.  Invariant parent[x] <= x, so the walk is
+ * strictly decreasing and ends.  Halving writes only touch non-roots and
+ * always store an ancestor, so they never break a concurrent hook. */
+__device__ __forceinline__ uint32_t cc_find(uint32_t *parent, uint32_t x)
+{
+    uint32_t p = cc_ldp(parent, x);
+    while (p != x) {
+        uint32_t gp = cc_ldp(parent, p);
+        if (gp == p)
+            return p;
+        parent[x] = gp;
+        x = gp;
+        p = cc_ldp(parent, x);
+    }
+    return x;
+}
+
+/* Root of x without writes (for read-only passes). */
+__device__ __forceinline__ uint32_t cc_find_ro(const uint32_t *parent, uint32_t x)
+{
+    uint32_t p = cc_ldp(parent, x);
+    while (p != x) {
+        x = p;
+        p = cc_ldp(parent, x);
+    }
+    return x;
+}
+
+/* Union of the trees of a and b: the larger root is hooked under the
+ * smaller with a CAS that only succeeds while it is still a root.  A failed
+ * CAS means another thread hooked it first; the retry starts from roots
+ * strictly below the failed one, so the loop ends. */
+__device__ __forceinline__ void cc_link_roots(uint32_t *parent, uint32_t ra, uint32_t rb)
+{
+    while (ra != rb) {
+        uint32_t hi = ra > rb ? ra : rb;
+        uint32_t lo = ra ^ rb ^ hi;
+        uint32_t old = atomicCAS(parent + hi, hi, lo);
+        if (old == hi)
+            return;
+        ra = cc_find(parent, old);
+        rb = cc_find(parent, lo);
+    }
+}
+
+__device__ __forceinline__ void cc_link(uint32_t *parent, uint32_t a, uint32_t b)
+{
+    cc_link_roots(parent, cc_find(parent, a), cc_find(parent, b));
+}
+
+__device__ __forceinline__ uint32_t cc_warp_min(uint32_t v)
+{
+    return __reduce_min_sync(0xffffffffu, v);
+}
+
+#endif /* __CUDACC__ */
+
+#endif /* CCGPU_INTERNAL_H */

@@ -1,0 +1,153 @@
+/*
+ * ccgpu.h - the thin C ABI between host code and the sm_100a kernels of the
+ * B200 connected-components engine.
+ *
+ * Everything here takes plain pointers and sizes.  "d_" pointers are device
+ * (HBM) pointers, "h_" pointers are host pointers; `stream` is a
+ * cudaStream_t passed as void* (NULL = the legacy default stream).
+ *
+ * Every entry point returns a ccgpu_status; on failure a message is kept per
+ * host thread and returned by ccgpu_last_error().  Kernels never trap: device
+ * side waits are bounded and report CCGPU_ERR_TIMEOUT through the status.
+ *
+ * Labels produced by every solver are the minimum vertex id of each vertex's
+ * component - the output contract of the reference's
+ * compute_connected_components_mpi_advanced (include/cc_mpi.h:26-27) and the
+ * value its pthreads label propagation converges to
+ * (src/cc_pthreads.c:32-73,169-170).  Inputs are symmetric CSR graphs, as the
+ * reference requires (its loader neither symmetrises nor drops self loops,
+ * src/graph.c:17-18); neighbour ids >= n are ignored, as the reference's
+ * merge ignores them (src/cc_mpi.c:269,389).
+ */
+#ifndef CCGPU_H
+#define CCGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    CCGPU_OK = 0,
+    CCGPU_ERR_INVALID = 1,  /* bad argument (NULL pointer, size, option)   */
+    CCGPU_ERR_CUDA = 2,     /* a CUDA runtime call failed                   */
+    CCGPU_ERR_OOM = 3,      /* a device or pinned-host allocation failed    */
+    CCGPU_ERR_TIMEOUT = 4,  /* a bounded device-side wait ran out           */
+    CCGPU_ERR_LIMIT = 5,    /* a size is above a stated maximum             */
+    CCGPU_ERR_NODEVICE = 6, /* no CUDA device, or not an sm_100 device      */
+    CCGPU_ERR_IO = 7,       /* file could not be read or written            */
+    CCGPU_ERR_FORMAT = 8    /* file is not in a supported format            */
+} ccgpu_status;
+
+/* Message of the last failing call on this host thread ("" if none). */
+const char *ccgpu_last_error(void);
+/* Empties this thread's error message (lets callers of the void reference
+ * calls tell success from failure). */
+void ccgpu_clear_error(void);
+/* Library version, major*10000 + minor*100 + patch. */
+int ccgpu_version(void);
+/* Checks that a usable sm_100 device is current.  CCGPU_ERR_NODEVICE if not. */
+int ccgpu_device_check(void);
+
+/* ------------------------------------------------------------------------
+ * Contexts.  A context owns the device scratch (grow-only arena) that the
+ * solvers need beyond their inputs and outputs.  Calls that share a context
+ * must not overlap in time; use one context per concurrent host caller.
+ * NULL as a context argument means the calling thread's device default
+ * context, created on first use.
+ * ---------------------------------------------------------------------- */
+typedef struct ccgpu_ctx ccgpu_ctx;
+int ccgpu_ctx_create(ccgpu_ctx **out);
+void ccgpu_ctx_destroy(ccgpu_ctx *ctx);
+/* Bytes of device scratch the context holds right now. */
+size_t ccgpu_ctx_scratch_bytes(const ccgpu_ctx *ctx);
+/* Kernels launched through the context so far (NULL = this thread's
+ * default context). */
+uint64_t ccgpu_ctx_launches(const ccgpu_ctx *ctx);
+
+/* Launch profiler: when on, every kernel the context launches is bracketed
+ * by CUDA events on its stream.  ccgpu_prof_collect synchronises on the
+ * recorded events, writes the summed milliseconds and launch counts per
+ * kernel id (arrays of ccgpu_prof_kernels() entries, either may be NULL)
+ * since the previous collect, and starts a new window. */
+int ccgpu_prof_enable(ccgpu_ctx *ctx, int on);
+int ccgpu_prof_collect(ccgpu_ctx *ctx, double *ms, uint64_t *launches);
+int ccgpu_prof_kernels(void);
+const char *ccgpu_prof_name(int kernel_id);
+
+/* ------------------------------------------------------------------------
+ * Local CC (the kernel behind compute_connected_components_pthreads,
+ * include/cc.h:27-28 of the reference).
+ *
+ * Algorithm: union-find over a CSR in HBM.  Roots are hooked larger-id
+ * under smaller-id with atomicCAS, so each tree's root is its minimum id.
+ *   1. sample   link every vertex with its first `sample_rounds` neighbours
+ *   2. shortcut pointer-jump every vertex to its root
+ *   3. giant    most frequent root of 1024 seeded samples
+ *   4. finish   link the remaining neighbours of every vertex outside the
+ *               giant tree; degree-binned: a CTA gathers the short rows and
+ *               walks them edge-parallel, a warp takes each row of >= 32
+ *               entries with 16-byte loads, rows above `heavy_degree` are
+ *               queued and split across all CTAs
+ *   5. shortcut labels[v] = root(v)
+ * sample_rounds = 0 turns steps 1-3 off (every row is linked in step 4).
+ * ---------------------------------------------------------------------- */
+typedef struct {
+    int chunk_size;     /* vertices a CTA takes per work grab in step 4;
+                         * 1 = static blocks, <= 0 = 4096 (the reference's
+                         * DEFAULT_CHUNK_SIZE, include/cc.h:7)               */
+    int sample_rounds;  /* neighbours linked per vertex in step 1 (0..8);
+                         * < 0 = default (2)                                  */
+    int heavy_degree;   /* rows longer than this go to the grid-wide queue;
+                         * <= 0 = default (8192)                              */
+    int skip_giant;     /* 1 (default) = step 4 skips the giant tree;
+                         * 0 = link every remaining neighbour               */
+} ccgpu_cc_opts;
+
+typedef struct {
+    uint32_t giant_label;   /* root found in step 3 (UINT32_MAX if off)      */
+    uint32_t heavy_rows;    /* rows handled by the grid-wide queue           */
+    uint32_t components;    /* number of distinct labels (roots)             */
+    uint32_t kernels;       /* kernel launches this call made                */
+    uint64_t finish_rows;   /* rows step 4 linked (outside the giant tree)   */
+    uint64_t finish_edges;  /* row entries step 4 linked                     */
+} ccgpu_cc_stats;
+
+/* Fills opts with the defaults. */
+void ccgpu_cc_opts_default(ccgpu_cc_opts *opts);
+
+/* labels[v] = min vertex id of v's component, for a device-resident CSR
+ * (d_row_ptr[n+1], d_col_idx[m]).  opts may be NULL (defaults).  stats may be
+ * NULL; when non-NULL the call synchronises `stream` to fill it.  Otherwise
+ * the call is asynchronous on `stream`. */
+int ccgpu_local_cc(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d_col_idx,
+                   uint32_t n, uint64_t m, uint32_t *d_labels,
+                   const ccgpu_cc_opts *opts, ccgpu_cc_stats *stats, void *stream);
+
+/* Same computation from host buffers: copies h_row_ptr/h_col_idx to HBM
+ * (column copies pipelined with the sampling kernel), solves, and copies the
+ * labels back to h_labels.  Synchronous.  Pinned host buffers go fastest. */
+int ccgpu_local_cc_host(ccgpu_ctx *ctx, const uint64_t *h_row_ptr, const uint32_t *h_col_idx,
+                        uint32_t n, uint64_t m, uint32_t *h_labels,
+                        const ccgpu_cc_opts *opts, ccgpu_cc_stats *stats);
+
+/* Number of v with d_labels[v] == v (one root per component when the labels
+ * are min-id labels).  Synchronous; result in *count. */
+int ccgpu_count_roots(ccgpu_ctx *ctx, const uint32_t *d_labels, uint32_t n,
+                      uint64_t *count, void *stream);
+
+/* Checks, on the device, the invariants a min-id labelling satisfies:
+ * labels[u] == labels[v] for every edge, labels[v] <= v, and
+ * labels[labels[v]] == labels[v].  *violations counts failing vertices/edges.
+ * (With an independent component count this pins the labelling exactly.) */
+int ccgpu_check_labels(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d_col_idx,
+                       uint32_t n, uint64_t m, const uint32_t *d_labels,
+                       uint64_t *violations, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CCGPU_H */
