@@ -228,6 +228,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-verify", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--hook-mode", type=int, default=-1, help="ccgpu_cc_opts.hook_mode")
+    ap.add_argument("--sample-rounds", type=int, default=-1)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -262,7 +264,7 @@ def main():
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device=dev)
     stream = torch.cuda.current_stream()
     sptr = stream.cuda_stream
-    opts = _lib.opts()
+    opts = _lib.opts(hook_mode=args.hook_mode, sample_rounds=args.sample_rounds)
 
     # one checked solve: stats + device invariants + oracle on rank 0
     st = cc.local_cc_device(rp_d, col_d, n, m, lab_d, opts, stats=True)
@@ -364,7 +366,8 @@ def main():
         cfg.update(components=int(st.components), giant_label=int(st.giant_label),
                    l2="2x L2 buffer written between timed steps; col_idx > L2",
                    opts={"chunk_size": opts.chunk_size, "sample_rounds": opts.sample_rounds,
-                         "heavy_degree": opts.heavy_degree, "skip_giant": opts.skip_giant},
+                         "heavy_degree": opts.heavy_degree, "skip_giant": opts.skip_giant,
+                         "hook_mode": opts.hook_mode},
                    parallelism=f"replicas{world}" if world > 1 else "single",
                    verified_vs_oracle=verified, e2e_labels_match=e2e_ok)
         line = {

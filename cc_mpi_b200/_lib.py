@@ -28,7 +28,7 @@ class CCGPUError(RuntimeError):
 
 class CCOpts(C.Structure):
     _fields_ = [("chunk_size", C.c_int), ("sample_rounds", C.c_int),
-                ("heavy_degree", C.c_int), ("skip_giant", C.c_int)]
+                ("heavy_degree", C.c_int), ("skip_giant", C.c_int), ("hook_mode", C.c_int)]
 
 
 class CCStats(C.Structure):
@@ -118,5 +118,9 @@ def check(status):
     return status
 
 
-def opts(chunk_size=4096, sample_rounds=2, heavy_degree=8192, skip_giant=1):
-    return CCOpts(chunk_size, sample_rounds, heavy_degree, skip_giant)
+HOOK_FIRST, HOOK_LAZY, HOOK_CADENCE = 1, 2, 4
+
+
+def opts(chunk_size=4096, sample_rounds=2, heavy_degree=8192, skip_giant=1,
+         hook_mode=HOOK_CADENCE):
+    return CCOpts(chunk_size, sample_rounds, heavy_degree, skip_giant, hook_mode)

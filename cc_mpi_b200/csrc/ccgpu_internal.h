@@ -135,16 +135,39 @@ static inline unsigned cc_blocks(uint64_t work, unsigned per_block, unsigned cap
 /* ----------------------------------------------- union-find primitives */
 #ifdef __CUDACC__
 
-/* Parent reads go through L2 (.cg): L1 is not coherent across SMs and the
- * parent array is written concurrently by other CTAs. */
+/* Parent reads are weak loads cached in L1 (ld.global.ca).  L1 is not
+ * coherent across SMs, so a read may return an older value of parent[i];
+ * that is harmless here: every value parent[i] ever held is an ancestor of
+ * i with parent[i] <= i, so walks still end, and a stale "root" only makes a
+ * hook CAS fail and retry from the fresher value the CAS returns.  Caching
+ * matters because every find ends on the few lines near the giant root:
+ * served from L2 they turn one L2 slice into a hot spot.  The asm is
+ * volatile so the compiler cannot merge or hoist the reads. */
+#ifndef CC_PARENT_LOAD_L2
+#define CC_PARENT_LOAD_L2 0
+#endif
+#ifndef CC_FIND_HALVING
+#define CC_FIND_HALVING 1
+#endif
 __device__ __forceinline__ uint32_t cc_ldp(const uint32_t *p, uint32_t i)
 {
-    return __ldcg(p + i);
+    uint32_t v;
+#if CC_PARENT_LOAD_L2
+    asm volatile("ld.global.cg.u32 %0, [%1];" : "=r"(v) : "l"(p + i));
+#else
+    asm volatile("ld.global.ca.u32 %0, [%1];" : "=r"(v) : "l"(p + i));
+#endif
+    return v;
 }
 
 /* Root of x with path halving.  Invariant parent[x] <= x, so the walk is
  * strictly decreasing and ends.  Halving writes only touch non-roots and
- * always store an ancestor, so they never break a concurrent hook. */
+ * always store an ancestor, so they never break a concurrent hook.  They
+ * are atomicMin (a fire-and-forget red.min): ancestors have smaller ids
+ * than their descendants, so a pointer only ever moves towards the root.
+ * A plain store here would let a slow thread put an intermediate ancestor
+ * back over the root pointer another thread just wrote in the final
+ * shortcut pass, leaving a label that is not the component minimum. */
 __device__ __forceinline__ uint32_t cc_find(uint32_t *parent, uint32_t x)
 {
     uint32_t p = cc_ldp(parent, x);
@@ -152,7 +175,8 @@ __device__ __forceinline__ uint32_t cc_find(uint32_t *parent, uint32_t x)
         uint32_t gp = cc_ldp(parent, p);
         if (gp == p)
             return p;
-        parent[x] = gp;
+        if (CC_FIND_HALVING)
+            atomicMin(parent + x, gp);
         x = gp;
         p = cc_ldp(parent, x);
     }
@@ -190,6 +214,32 @@ __device__ __forceinline__ void cc_link_roots(uint32_t *parent, uint32_t ra, uin
 __device__ __forceinline__ void cc_link(uint32_t *parent, uint32_t a, uint32_t b)
 {
     cc_link_roots(parent, cc_find(parent, a), cc_find(parent, b));
+}
+
+/* Union of the trees of a and b that skips walking b's path when b is
+ * smaller than a's root: the root ra is then hooked directly under b.  That
+ * is safe because a root is the minimum of its tree, so b < ra means b lies
+ * in another tree and no cycle can form.  It trades a longer path later
+ * (ra hangs under b, not under b's root) for one walk fewer now. */
+__device__ __forceinline__ void cc_link_lazy(uint32_t *parent, uint32_t a, uint32_t b)
+{
+    uint32_t ra = cc_find(parent, a);
+    while (b < ra) {
+        uint32_t old = atomicCAS(parent + ra, ra, b);
+        if (old == ra)
+            return;
+        ra = cc_find(parent, old);
+    }
+    cc_link_roots(parent, ra, cc_find(parent, b));
+}
+
+template <bool LAZY>
+__device__ __forceinline__ void cc_union(uint32_t *parent, uint32_t a, uint32_t b)
+{
+    if (LAZY)
+        cc_link_lazy(parent, a, b);
+    else
+        cc_link(parent, a, b);
 }
 
 __device__ __forceinline__ uint32_t cc_warp_min(uint32_t v)

@@ -1,30 +1,34 @@
 /*
- * Local connected components on one device-resident CSR (sm_100a).
+ * Local connected components on a device-resident CSR (sm_100a).
  *
  * Replaces the reference's pthreads label propagation
  * (src/cc_pthreads.c:32-73 relax, :76-150 round loop, :152-229 driver),
  * whose result - each label is the minimum vertex id of its component - is
- * kept bit for bit.  The method here is union-find hooking (the larger root
- * is CAS-hooked under the smaller root, so every root is its tree's
- * minimum id) with Afforest-style neighbour sampling (Sutton, Ben-Nun and
- * Barak, IPDPS 2018): after linking each vertex with its first few
- * neighbours, the most frequent root is found and the remaining rows of its
- * tree are never read.  That skip is valid for symmetric graphs, which is
- * the reference's input contract.
+ * kept bit for bit.  The method is union-find hooking (the larger root is
+ * CAS-hooked under a smaller vertex, so every root is its tree's minimum id)
+ * with Afforest-style neighbour sampling (Sutton, Ben-Nun and Barak, IPDPS
+ * 2018): after linking each vertex with its first few neighbours, the most
+ * frequent root is found and the remaining rows of its tree are never read.
+ * That skip is valid for symmetric graphs, the reference's input contract.
+ * The optional first hook in the init pass follows ECL-CC's initialisation
+ * (Jaiganesh and Burtscher, HPDC 2018).
  *
- * Kernels (all grid-stride, 256 threads):
- *   k_init       parent[v] = v (16-byte stores) and zeroes the counters
- *   k_sample     thread per vertex, links neighbours [r0, r1) of its row
+ * Kernels (256 threads):
+ *   k_init       parent[v] = v, or v's first neighbour when smaller
+ *   k_sample     thread per vertex, links row entries [r0, r1)
  *   k_compress   parent[v] = root(v)
- *   k_giant      one CTA: most frequent root among 1024 seeded samples
- *   k_link_rows  degree-binned finish pass (CTA gather / warp / queue)
- *   k_link_heavy rows above the heavy threshold, split over every CTA
+ *   k_giant      one CTA per segment: most frequent root of 1024 samples
+ *   k_link_rows  degree-binned finish pass: a CTA gathers short rows and
+ *                walks them edge-parallel, a warp takes rows of >= 32 entries
+ *                with 16-byte column loads, rows above the heavy threshold go
+ *                to a queue
+ *   k_link_heavy queued rows split in 4096-entry pieces over every CTA
  *   k_count_roots, k_check_labels   reductions for stats and tests
  */
 #include <cstdio>
 #include <cstring>
 
-#include "ccgpu_internal.h"
+#include "local_cc.h"
 
 namespace {
 
@@ -59,14 +63,46 @@ __device__ __forceinline__ uint32_t mix32(uint32_t h)
     return h;
 }
 
+/* Index s with seg[s] <= v < seg[s+1] (seg ascending, nseg >= 1). */
+__device__ __forceinline__ uint32_t seg_of(const uint64_t *__restrict__ seg, uint32_t nseg,
+                                           uint64_t v)
+{
+    uint32_t lo = 0, hi = nseg;
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(seg + mid) <= v)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
 __global__ void __launch_bounds__(kBlock) k_init(uint32_t *__restrict__ parent, uint32_t n,
-                                                 uint32_t *__restrict__ counters, int ncounters,
-                                                 int vec)
+                                                 LocalCCCounters *counters, int vec,
+                                                 const uint64_t *__restrict__ row_ptr,
+                                                 const uint32_t *__restrict__ col, uint64_t m,
+                                                 int first_hook)
 {
     const uint64_t stride = (uint64_t)gridDim.x * kBlock;
     const uint64_t tid = (uint64_t)blockIdx.x * kBlock + threadIdx.x;
-    if (blockIdx.x == 0 && (int)threadIdx.x < ncounters)
-        counters[threadIdx.x] = 0;
+    if (tid == 0)
+        memset(counters, 0, sizeof(LocalCCCounters));
+    if (first_hook) {
+        /* parent[v] = first neighbour if it is smaller: v is still a root
+         * and only this thread writes parent[v], so a plain store hooks it */
+        for (uint64_t v = tid; v < n; v += stride) {
+            Rows r = row_of(row_ptr, (uint32_t)v, m);
+            uint32_t p = (uint32_t)v;
+            if (r.beg < r.end) {
+                uint32_t u = __ldg(col + r.beg);
+                if (u < p)
+                    p = u;
+            }
+            parent[v] = p;
+        }
+        return;
+    }
     uint64_t done = 0;
     if (vec) {
         uint4 *p4 = reinterpret_cast<uint4 *>(parent);
@@ -81,10 +117,13 @@ __global__ void __launch_bounds__(kBlock) k_init(uint32_t *__restrict__ parent, 
         parent[v] = (uint32_t)v;
 }
 
+/* Links row entries [r0, r1) of every vertex in [v_lo, v_hi).  With the
+ * first hook done by k_init, entry 0 is skipped when it was smaller. */
+template <bool LAZY>
 __global__ void __launch_bounds__(kBlock) k_sample(const uint64_t *__restrict__ row_ptr,
                                                    const uint32_t *__restrict__ col, uint32_t n,
                                                    uint64_t m, uint32_t *parent, uint32_t v_lo,
-                                                   uint32_t v_hi, int r0, int r1)
+                                                   uint32_t v_hi, int r0, int r1, int first_done)
 {
     const uint64_t stride = (uint64_t)gridDim.x * kBlock;
     for (uint64_t v = (uint64_t)v_lo + (uint64_t)blockIdx.x * kBlock + threadIdx.x; v < v_hi;
@@ -95,8 +134,9 @@ __global__ void __launch_bounds__(kBlock) k_sample(const uint64_t *__restrict__ 
             if (j >= r.end)
                 break;
             uint32_t u = __ldg(col + j);
-            if (u < n)
-                cc_link(parent, (uint32_t)v, u);
+            if (u >= n || (k == 0 && first_done && u < (uint32_t)v))
+                continue;
+            cc_union<LAZY>(parent, (uint32_t)v, u);
         }
     }
 }
@@ -111,15 +151,25 @@ __global__ void __launch_bounds__(kBlock) k_compress(uint32_t *parent, uint32_t 
     }
 }
 
-/* Most frequent root among kGiantSamples seeded samples.  Ties go to the
- * smaller root so the choice is deterministic for a given forest. */
+/* Most frequent root among kGiantSamples seeded samples of segment
+ * blockIdx.x.  Ties go to the smaller root, so the choice is deterministic
+ * for a given forest. */
 __global__ void __launch_bounds__(kGiantSamples) k_giant(const uint32_t *parent, uint32_t n,
-                                                         uint32_t seed, uint32_t *out)
+                                                         const uint64_t *seg, uint32_t seed,
+                                                         uint32_t *out)
 {
     __shared__ uint32_t s[kGiantSamples];
     __shared__ unsigned long long s_best[kGiantSamples / 32];
     const uint32_t i = threadIdx.x;
-    uint32_t v = (uint32_t)(((uint64_t)mix32(i * 0x9e3779b9u + seed) * n) >> 32);
+    uint64_t lo = seg ? seg[blockIdx.x] : 0, hi = seg ? seg[blockIdx.x + 1] : n;
+    if (hi <= lo) {
+        if (i == 0)
+            out[blockIdx.x] = kNoGiant;
+        return;
+    }
+    uint64_t size = hi - lo;
+    uint32_t h = mix32(i * 0x9e3779b9u + seed + blockIdx.x);
+    uint32_t v = (uint32_t)(lo + (((uint64_t)h * size) >> 32));
     s[i] = cc_find_ro(parent, v);
     __syncthreads();
     for (uint32_t k = 2; k <= kGiantSamples; k <<= 1) {
@@ -138,15 +188,15 @@ __global__ void __launch_bounds__(kGiantSamples) k_giant(const uint32_t *parent,
     }
     uint32_t cnt = 0, val = s[i];
     if (i == 0 || s[i - 1] != val) {
-        uint32_t lo = i, hi = kGiantSamples;
-        while (lo < hi) {
-            uint32_t mid = (lo + hi) >> 1;
+        uint32_t a = i, b = kGiantSamples;
+        while (a < b) {
+            uint32_t mid = (a + b) >> 1;
             if (s[mid] <= val)
-                lo = mid + 1;
+                a = mid + 1;
             else
-                hi = mid;
+                b = mid;
         }
-        cnt = lo - i;
+        cnt = a - i;
     }
     unsigned long long key = ((unsigned long long)cnt << 32) | (uint32_t)~val;
     for (int o = 16; o > 0; o >>= 1) {
@@ -163,7 +213,7 @@ __global__ void __launch_bounds__(kGiantSamples) k_giant(const uint32_t *parent,
             key = other > key ? other : key;
         }
         if (i == 0)
-            out[0] = ~(uint32_t)key;
+            out[blockIdx.x] = ~(uint32_t)key;
     }
 }
 
@@ -174,25 +224,26 @@ struct LinkParams {
     uint64_t m;
     uint32_t *parent;
     uint32_t skip_from;        /* first row entry the finish pass links   */
-    const uint32_t *giant;     /* device giant root, NULL = no skipping    */
+    const uint32_t *giants;    /* [nseg] giant roots, NULL = no skipping   */
+    const uint64_t *seg;       /* segment offsets or NULL                  */
+    uint32_t nseg;
     uint32_t chunk;            /* vertices per work grab, 0 = static       */
-    unsigned long long *grab;  /* work counter                             */
+    LocalCCCounters *cnt;
     uint32_t *heavy_list;
-    uint32_t *heavy_count;
     uint32_t heavy_cap;
     uint32_t heavy_deg;
     int vec;                   /* col is 16-byte aligned                    */
-    unsigned long long *finish; /* [0] rows linked, [1] entries linked      */
 };
 
 /* One warp links v with row entries [beg, end): 16-byte column loads for
  * the aligned body, scalar head and tail. */
+template <bool LAZY>
 __device__ __forceinline__ void warp_link_row(const LinkParams &P, uint32_t v, uint64_t beg,
                                               uint64_t end, int lane)
 {
-    uint64_t a = beg, body_end = beg;
+    uint64_t body_end = beg;
     if (P.vec) {
-        a = (beg + 3) & ~3ull;
+        uint64_t a = (beg + 3) & ~3ull;
         if (a > end)
             a = end;
         body_end = end & ~3ull;
@@ -201,28 +252,29 @@ __device__ __forceinline__ void warp_link_row(const LinkParams &P, uint32_t v, u
         if (beg + lane < a) {
             uint32_t u = __ldg(P.col + beg + lane);
             if (u < P.n)
-                cc_link(P.parent, v, u);
+                cc_union<LAZY>(P.parent, v, u);
         }
         const uint4 *c4 = reinterpret_cast<const uint4 *>(P.col);
         for (uint64_t q = a / 4 + lane; q < body_end / 4; q += 32) {
             uint4 x = __ldg(c4 + q);
             if (x.x < P.n)
-                cc_link(P.parent, v, x.x);
+                cc_union<LAZY>(P.parent, v, x.x);
             if (x.y < P.n)
-                cc_link(P.parent, v, x.y);
+                cc_union<LAZY>(P.parent, v, x.y);
             if (x.z < P.n)
-                cc_link(P.parent, v, x.z);
+                cc_union<LAZY>(P.parent, v, x.z);
             if (x.w < P.n)
-                cc_link(P.parent, v, x.w);
+                cc_union<LAZY>(P.parent, v, x.w);
         }
     }
     for (uint64_t j = body_end + lane; j < end; j += 32) {
         uint32_t u = __ldg(P.col + j);
         if (u < P.n)
-            cc_link(P.parent, v, u);
+            cc_union<LAZY>(P.parent, v, u);
     }
 }
 
+template <bool LAZY>
 __global__ void __launch_bounds__(kBlock) k_link_rows(LinkParams P)
 {
     __shared__ uint32_t s_off[kBlock + 1];
@@ -230,7 +282,7 @@ __global__ void __launch_bounds__(kBlock) k_link_rows(LinkParams P)
     __shared__ uint32_t s_wsum[kWarps];
     __shared__ unsigned long long s_base;
 
-    const uint32_t giant = P.giant ? *P.giant : kNoGiant;
+    const uint32_t giant0 = (P.giants && P.nseg == 1) ? P.giants[0] : kNoGiant;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint32_t my_rows = 0;
     unsigned long long my_edges = 0;
@@ -251,7 +303,7 @@ __global__ void __launch_bounds__(kBlock) k_link_rows(LinkParams P)
         uint64_t base, cend;
         if (P.chunk) {
             if (threadIdx.x == 0)
-                s_base = atomicAdd(P.grab, (unsigned long long)P.chunk);
+                s_base = atomicAdd(&P.cnt->grab, (unsigned long long)P.chunk);
             __syncthreads();
             base = s_base;
             __syncthreads();
@@ -270,18 +322,23 @@ __global__ void __launch_bounds__(kBlock) k_link_rows(LinkParams P)
             const uint64_t v64 = t0 + threadIdx.x;
             const uint32_t v = (uint32_t)v64;
             uint64_t beg = 0, end = 0;
-            if (v64 < cend && (giant == kNoGiant || cc_ldp(P.parent, v) != giant)) {
-                Rows r = row_of(P.row_ptr, v, P.m);
-                beg = r.beg + P.skip_from;
-                end = r.end;
-                if (beg > end)
-                    beg = end;
-                my_rows++;
-                my_edges += end - beg;
+            if (v64 < cend) {
+                uint32_t giant = giant0;
+                if (P.giants && P.nseg > 1)
+                    giant = P.giants[seg_of(P.seg, P.nseg, v64)];
+                if (giant == kNoGiant || cc_ldp(P.parent, v) != giant) {
+                    Rows r = row_of(P.row_ptr, v, P.m);
+                    beg = r.beg + P.skip_from;
+                    end = r.end;
+                    if (beg > end)
+                        beg = end;
+                    my_rows++;
+                    my_edges += end - beg;
+                }
             }
             uint64_t deg = end - beg;
             if (deg > P.heavy_deg) {
-                uint32_t slot = atomicAdd(P.heavy_count, 1u);
+                uint32_t slot = atomicAdd(&P.cnt->heavy_count, 1u);
                 if (slot < P.heavy_cap) {
                     P.heavy_list[slot] = v;
                     deg = 0;
@@ -295,7 +352,7 @@ __global__ void __launch_bounds__(kBlock) k_link_rows(LinkParams P)
                 uint32_t vv = __shfl_sync(0xffffffffu, v, src);
                 uint64_t bb = __shfl_sync(0xffffffffu, beg, src);
                 uint64_t ee = __shfl_sync(0xffffffffu, end, src);
-                warp_link_row(P, vv, bb, ee, lane);
+                warp_link_row<LAZY>(P, vv, bb, ee, lane);
             }
             /* short rows: CTA-wide gather, walked edge-parallel */
             uint32_t small = deg < 32 ? (uint32_t)deg : 0u;
@@ -332,7 +389,7 @@ __global__ void __launch_bounds__(kBlock) k_link_rows(LinkParams P)
                 uint64_t j = s_beg[lo] + (e - s_off[lo]);
                 uint32_t u = __ldg(P.col + j);
                 if (u < P.n)
-                    cc_link(P.parent, (uint32_t)(t0 + lo), u);
+                    cc_union<LAZY>(P.parent, (uint32_t)(t0 + lo), u);
             }
             __syncthreads();
         }
@@ -343,14 +400,15 @@ __global__ void __launch_bounds__(kBlock) k_link_rows(LinkParams P)
         my_edges += __shfl_xor_sync(0xffffffffu, my_edges, o);
     }
     if (lane == 0 && rows) {
-        atomicAdd(P.finish, rows);
-        atomicAdd(P.finish + 1, my_edges);
+        atomicAdd(&P.cnt->finish_rows, rows);
+        atomicAdd(&P.cnt->finish_edges, my_edges);
     }
 }
 
+template <bool LAZY>
 __global__ void __launch_bounds__(kBlock) k_link_heavy(LinkParams P)
 {
-    uint32_t cnt = *P.heavy_count;
+    uint32_t cnt = P.cnt->heavy_count;
     if (cnt > P.heavy_cap)
         cnt = P.heavy_cap;
     for (uint32_t h = 0; h < cnt; ++h) {
@@ -366,7 +424,7 @@ __global__ void __launch_bounds__(kBlock) k_link_heavy(LinkParams P)
             for (uint64_t j = sb + threadIdx.x; j < se; j += kBlock) {
                 uint32_t u = __ldg(P.col + j);
                 if (u < P.n)
-                    cc_link(P.parent, v, u);
+                    cc_union<LAZY>(P.parent, v, u);
             }
         }
     }
@@ -414,36 +472,48 @@ __global__ void __launch_bounds__(kBlock) k_check_labels(const uint64_t *__restr
         atomicAdd(bad, (unsigned long long)local_bad);
 }
 
-/* Device scratch of one local-CC call. */
-struct Scratch {
-    unsigned long long *grab;
-    uint32_t *heavy_count;
-    uint32_t *giant;
-    unsigned long long *finish;
-    uint32_t *heavy_list;
-    uint32_t heavy_cap;
+struct Geometry {
+    unsigned stream_blocks; /* grid for the streaming kernels      */
+    unsigned link_blocks;   /* resident grid for k_link_rows        */
 };
 
-constexpr int kCounterWords = 8; /* grab (2 words), heavy_count, giant, finish (4) */
-
-size_t carve_scratch(cc_carve *c, Scratch *s, uint32_t n, uint64_t m, uint32_t heavy_deg)
+int geometry(const ccgpu_ctx *ctx, Geometry *g)
 {
-    uint64_t cap = m / (heavy_deg ? heavy_deg : 1) + 1;
-    if (cap > n)
-        cap = n;
-    if (cap == 0)
-        cap = 1;
-    uint32_t *counters = (uint32_t *)cc_take(c, kCounterWords * sizeof(uint32_t));
-    s->heavy_list = (uint32_t *)cc_take(c, cap * sizeof(uint32_t));
-    s->heavy_cap = (uint32_t)cap;
-    s->grab = (unsigned long long *)counters;
-    s->heavy_count = counters + 2;
-    s->giant = counters + 3;
-    s->finish = (unsigned long long *)(counters + 4);
-    return c->off;
+    static thread_local int occ_rows = 0;
+    if (!occ_rows) {
+        CC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_rows, k_link_rows<false>,
+                                                              kBlock, 0));
+        if (occ_rows < 1)
+            occ_rows = 1;
+    }
+    g->stream_blocks = (unsigned)ctx->sm_count * 8;
+    g->link_blocks = (unsigned)ctx->sm_count * (unsigned)occ_rows;
+    return CCGPU_OK;
 }
 
-int resolve_opts(const ccgpu_cc_opts *in, ccgpu_cc_opts *o)
+template <bool LAZY>
+int launch_sample(ccgpu_ctx *ctx, const LocalCCArgs &a, uint32_t vlo, uint32_t vhi, int r0,
+                  int r1, cudaStream_t st, unsigned blocks)
+{
+    const int first_done = (a.o.hook_mode & CCGPU_HOOK_FIRST) != 0;
+    CC_KLAUNCH(ctx, CCK_SAMPLE, k_sample<LAZY>, blocks, kBlock, 0, st, a.row_ptr, a.col, a.n,
+               a.m, a.labels, vlo, vhi, r0, r1, first_done);
+    return CCGPU_OK;
+}
+
+template <bool LAZY>
+int launch_finish(ccgpu_ctx *ctx, const LinkParams &P, const Geometry &g, cudaStream_t st)
+{
+    CC_KLAUNCH(ctx, CCK_LINK_ROWS, k_link_rows<LAZY>, g.link_blocks, kBlock, 0, st, P);
+    CC_KLAUNCH(ctx, CCK_LINK_HEAVY, k_link_heavy<LAZY>, g.link_blocks, kBlock, 0, st, P);
+    return CCGPU_OK;
+}
+
+} // namespace
+
+/* ------------------------------------------------------ internal entry */
+
+int cc_local_resolve_opts(const ccgpu_cc_opts *in, ccgpu_cc_opts *o)
 {
     ccgpu_cc_opts_default(o);
     if (in) {
@@ -454,33 +524,116 @@ int resolve_opts(const ccgpu_cc_opts *in, ccgpu_cc_opts *o)
             o->heavy_degree = 8192;
         if (o->chunk_size <= 0)
             o->chunk_size = 4096;
+        if (o->hook_mode < 0)
+            o->hook_mode = CCGPU_HOOK_CADENCE;
     }
     if (o->sample_rounds > 8)
         return ccgpu_set_error(CCGPU_ERR_INVALID, "sample_rounds %d above 8", o->sample_rounds);
+    if (o->hook_mode > 7)
+        return ccgpu_set_error(CCGPU_ERR_INVALID, "hook_mode %d is not a mask of 1|2|4",
+                               o->hook_mode);
     if (o->heavy_degree < 32)
         o->heavy_degree = 32;
     return CCGPU_OK;
 }
 
-struct Geometry {
-    unsigned stream_blocks; /* grid for the streaming kernels      */
-    unsigned link_blocks;   /* resident grid for k_link_rows        */
-};
-
-int geometry(const ccgpu_ctx *ctx, Geometry *g)
+void cc_local_carve(cc_carve *c, LocalCCScratch *s, const LocalCCArgs &a)
 {
-    static thread_local int occ_rows = 0;
-    if (!occ_rows) {
-        CC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_rows, k_link_rows, kBlock, 0));
-        if (occ_rows < 1)
-            occ_rows = 1;
-    }
-    g->stream_blocks = (unsigned)ctx->sm_count * 8;
-    g->link_blocks = (unsigned)ctx->sm_count * (unsigned)occ_rows;
+    uint64_t cap = a.m / (uint64_t)(a.o.heavy_degree > 0 ? a.o.heavy_degree : 1) + 1;
+    if (cap > a.n)
+        cap = a.n;
+    if (cap == 0)
+        cap = 1;
+    s->counters = (LocalCCCounters *)cc_take(c, sizeof(LocalCCCounters));
+    s->giants = (uint32_t *)cc_take(c, (size_t)(a.nseg ? a.nseg : 1) * sizeof(uint32_t));
+    s->heavy_list = (uint32_t *)cc_take(c, cap * sizeof(uint32_t));
+    s->heavy_cap = (uint32_t)cap;
+}
+
+int cc_local_init(ccgpu_ctx *ctx, const LocalCCArgs &a, const LocalCCScratch &s, cudaStream_t st)
+{
+    Geometry g = {1, 1};
+    CC_TRY(geometry(ctx, &g));
+    const unsigned sb = cc_blocks(a.n, kBlock, g.stream_blocks);
+    const int first = (a.o.hook_mode & CCGPU_HOOK_FIRST) && a.o.sample_rounds > 0;
+    CC_KLAUNCH(ctx, CCK_INIT, k_init, sb, kBlock, 0, st, a.labels, a.n, s.counters,
+               ((uintptr_t)a.labels & 15) == 0, a.row_ptr, a.col, a.m, first);
     return CCGPU_OK;
 }
 
-} // namespace
+int cc_local_sample_range(ccgpu_ctx *ctx, const LocalCCArgs &a, uint32_t v_lo, uint32_t v_hi,
+                          cudaStream_t st)
+{
+    if (a.o.sample_rounds <= 0 || v_hi <= v_lo)
+        return CCGPU_OK;
+    Geometry g = {1, 1};
+    CC_TRY(geometry(ctx, &g));
+    const unsigned sb = cc_blocks(v_hi - v_lo, kBlock, g.stream_blocks);
+    if (a.o.hook_mode & CCGPU_HOOK_LAZY)
+        return launch_sample<true>(ctx, a, v_lo, v_hi, 0, a.o.sample_rounds, st, sb);
+    return launch_sample<false>(ctx, a, v_lo, v_hi, 0, a.o.sample_rounds, st, sb);
+}
+
+int cc_local_run(ccgpu_ctx *ctx, const LocalCCArgs &a, const LocalCCScratch &s, cudaStream_t st,
+                 int init_done, int sampled)
+{
+    if (a.n == 0)
+        return CCGPU_OK;
+    Geometry g = {1, 1};
+    CC_TRY(geometry(ctx, &g));
+    const unsigned sb = cc_blocks(a.n, kBlock, g.stream_blocks);
+    const bool lazy = (a.o.hook_mode & CCGPU_HOOK_LAZY) != 0;
+    const int k = a.o.sample_rounds;
+    if (!init_done)
+        CC_TRY(cc_local_init(ctx, a, s, st));
+    const bool skip = k > 0 && a.o.skip_giant;
+    if (k > 0) {
+        if (!sampled) {
+            if (a.o.hook_mode & CCGPU_HOOK_CADENCE) {
+                for (int r = 0; r < k; ++r) {
+                    if (lazy)
+                        CC_TRY(launch_sample<true>(ctx, a, 0, a.n, r, r + 1, st, sb));
+                    else
+                        CC_TRY(launch_sample<false>(ctx, a, 0, a.n, r, r + 1, st, sb));
+                    if (r + 1 < k)
+                        CC_KLAUNCH(ctx, CCK_COMPRESS, k_compress, sb, kBlock, 0, st, a.labels,
+                                   a.n);
+                }
+            } else if (lazy) {
+                CC_TRY(launch_sample<true>(ctx, a, 0, a.n, 0, k, st, sb));
+            } else {
+                CC_TRY(launch_sample<false>(ctx, a, 0, a.n, 0, k, st, sb));
+            }
+        }
+        if (skip) {
+            CC_KLAUNCH(ctx, CCK_COMPRESS, k_compress, sb, kBlock, 0, st, a.labels, a.n);
+            CC_KLAUNCH(ctx, CCK_GIANT, k_giant, a.nseg, kGiantSamples, 0, st, a.labels, a.n,
+                       a.seg, 0x5eed1234u, s.giants);
+        }
+    }
+    LinkParams P;
+    P.row_ptr = a.row_ptr;
+    P.col = a.col;
+    P.n = a.n;
+    P.m = a.m;
+    P.parent = a.labels;
+    P.skip_from = (uint32_t)k;
+    P.giants = skip ? s.giants : nullptr;
+    P.seg = a.seg;
+    P.nseg = a.seg ? a.nseg : 1;
+    P.chunk = a.o.chunk_size == 1 ? 0u : (uint32_t)a.o.chunk_size;
+    P.cnt = s.counters;
+    P.heavy_list = s.heavy_list;
+    P.heavy_cap = s.heavy_cap;
+    P.heavy_deg = (uint32_t)a.o.heavy_degree;
+    P.vec = ((uintptr_t)a.col & 15) == 0;
+    if (lazy)
+        CC_TRY(launch_finish<true>(ctx, P, g, st));
+    else
+        CC_TRY(launch_finish<false>(ctx, P, g, st));
+    CC_KLAUNCH(ctx, CCK_FINAL_COMPRESS, k_compress, sb, kBlock, 0, st, a.labels, a.n);
+    return CCGPU_OK;
+}
 
 /* ------------------------------------------------------------------ API */
 
@@ -492,75 +645,25 @@ extern "C" void ccgpu_cc_opts_default(ccgpu_cc_opts *o)
     o->sample_rounds = 2;
     o->heavy_degree = 8192;
     o->skip_giant = 1;
+    o->hook_mode = CCGPU_HOOK_CADENCE;
 }
 
-/* The solve itself, on scratch already carved.  `sample_hi` bounds the
- * vertices k_sample covers (the host pipeline samples ranges itself and
- * passes sampled = 1). */
-static int local_cc_launch(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d_col,
-                           uint32_t n, uint64_t m, uint32_t *d_labels, const ccgpu_cc_opts *o,
-                           const Scratch &s, cudaStream_t st, int init_done, int sampled,
-                           uint32_t *kernels)
-{
-    Geometry g = {1, 1};
-    CC_TRY(geometry(ctx, &g));
-    const unsigned sb = cc_blocks(n, kBlock, g.stream_blocks);
-    const unsigned long long before = ctx->launches;
-    if (!init_done)
-        CC_KLAUNCH(ctx, CCK_INIT, k_init, sb, kBlock, 0, st, d_labels, n, (uint32_t *)s.grab,
-                   kCounterWords, ((uintptr_t)d_labels & 15) == 0);
-    const int k = o->sample_rounds;
-    const bool skip = k > 0 && o->skip_giant;
-    if (k > 0) {
-        if (!sampled)
-            CC_KLAUNCH(ctx, CCK_SAMPLE, k_sample, sb, kBlock, 0, st, d_row_ptr, d_col, n, m,
-                       d_labels, 0u, n, 0, k);
-        if (skip) {
-            CC_KLAUNCH(ctx, CCK_COMPRESS, k_compress, sb, kBlock, 0, st, d_labels, n);
-            CC_KLAUNCH(ctx, CCK_GIANT, k_giant, 1, kGiantSamples, 0, st, d_labels, n,
-                       0x5eed1234u, s.giant);
-        }
-    }
-    LinkParams P;
-    P.row_ptr = d_row_ptr;
-    P.col = d_col;
-    P.n = n;
-    P.m = m;
-    P.parent = d_labels;
-    P.skip_from = (uint32_t)k;
-    P.giant = skip ? s.giant : nullptr;
-    P.chunk = o->chunk_size == 1 ? 0u : (uint32_t)o->chunk_size;
-    P.grab = s.grab;
-    P.heavy_list = s.heavy_list;
-    P.heavy_count = s.heavy_count;
-    P.heavy_cap = s.heavy_cap;
-    P.heavy_deg = (uint32_t)o->heavy_degree;
-    P.vec = ((uintptr_t)d_col & 15) == 0;
-    P.finish = s.finish;
-    CC_KLAUNCH(ctx, CCK_LINK_ROWS, k_link_rows, g.link_blocks, kBlock, 0, st, P);
-    CC_KLAUNCH(ctx, CCK_LINK_HEAVY, k_link_heavy, g.link_blocks, kBlock, 0, st, P);
-    CC_KLAUNCH(ctx, CCK_FINAL_COMPRESS, k_compress, sb, kBlock, 0, st, d_labels, n);
-    const uint32_t launches = (uint32_t)(ctx->launches - before);
-    if (kernels)
-        *kernels = launches;
-    return CCGPU_OK;
-}
-
-static int fill_stats(ccgpu_ctx *ctx, const Scratch &s, const uint32_t *d_labels, uint32_t n,
-                      const ccgpu_cc_opts *o, uint32_t kernels, ccgpu_cc_stats *stats,
-                      cudaStream_t st)
+static int fill_stats(ccgpu_ctx *ctx, const LocalCCArgs &a, const LocalCCScratch &s,
+                      uint32_t kernels, ccgpu_cc_stats *stats, cudaStream_t st)
 {
     uint64_t roots = 0;
-    CC_TRY(ccgpu_count_roots(ctx, d_labels, n, &roots, st));
-    uint32_t h[6] = {0, 0, 0, 0, 0, 0};
-    CC_CUDA(cudaMemcpyAsync(h, s.heavy_count, 6 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    CC_TRY(ccgpu_count_roots(ctx, a.labels, a.n, &roots, st));
+    LocalCCCounters h;
+    uint32_t giant = 0xffffffffu;
+    CC_CUDA(cudaMemcpyAsync(&h, s.counters, sizeof(h), cudaMemcpyDeviceToHost, st));
+    CC_CUDA(cudaMemcpyAsync(&giant, s.giants, sizeof(giant), cudaMemcpyDeviceToHost, st));
     CC_CUDA(cudaStreamSynchronize(st));
-    memcpy(&stats->finish_rows, h + 2, sizeof(uint64_t));
-    memcpy(&stats->finish_edges, h + 4, sizeof(uint64_t));
-    stats->heavy_rows = h[0] < s.heavy_cap ? h[0] : s.heavy_cap;
-    stats->giant_label = (o->sample_rounds > 0 && o->skip_giant) ? h[1] : 0xffffffffu;
+    stats->heavy_rows = h.heavy_count < s.heavy_cap ? h.heavy_count : s.heavy_cap;
+    stats->giant_label = (a.o.sample_rounds > 0 && a.o.skip_giant) ? giant : 0xffffffffu;
     stats->components = (uint32_t)roots;
     stats->kernels = kernels + 1;
+    stats->finish_rows = h.finish_rows;
+    stats->finish_edges = h.finish_edges;
     return CCGPU_OK;
 }
 
@@ -585,27 +688,28 @@ extern "C" int ccgpu_local_cc(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const u
         memset(stats, 0, sizeof(*stats));
     if (n == 0)
         return CCGPU_OK;
-    ccgpu_cc_opts o;
-    CC_TRY(resolve_opts(opts, &o));
+    LocalCCArgs a = {d_row_ptr, d_col_idx, n, m, d_labels, nullptr, 1, {}};
+    CC_TRY(cc_local_resolve_opts(opts, &a.o));
     CC_TRY(ccgpu_ctx_resolve(&ctx));
     cudaStream_t st = (cudaStream_t)stream;
-    Scratch s;
+    LocalCCScratch s;
     cc_carve c = {nullptr, 0};
-    size_t bytes = carve_scratch(&c, &s, n, m, (uint32_t)o.heavy_degree);
+    cc_local_carve(&c, &s, a);
     void *base = nullptr;
-    CC_TRY(ccgpu_ctx_reserve(ctx, bytes, &base));
+    CC_TRY(ccgpu_ctx_reserve(ctx, c.off, &base));
     c = {(char *)base, 0};
-    carve_scratch(&c, &s, n, m, (uint32_t)o.heavy_degree);
-    uint32_t kernels = 0;
-    CC_TRY(local_cc_launch(ctx, d_row_ptr, d_col_idx, n, m, d_labels, &o, s, st, 0, 0, &kernels));
+    cc_local_carve(&c, &s, a);
+    const unsigned long long before = ctx->launches;
+    CC_TRY(cc_local_run(ctx, a, s, st, 0, 0));
     if (stats)
-        CC_TRY(fill_stats(ctx, s, d_labels, n, &o, kernels, stats, st));
+        CC_TRY(fill_stats(ctx, a, s, (uint32_t)(ctx->launches - before), stats, st));
     return CCGPU_OK;
 }
 
 /* Host-buffer variant.  Device copies of the CSR and the labels live in
- * the context's scratch.  Column chunks are copied on a second stream and
- * each chunk's vertex range is sampled as soon as its columns landed. */
+ * the context's scratch.  Column chunks are copied on a second stream and,
+ * when the init pass needs no columns, each chunk's vertex range is sampled
+ * as soon as its columns landed. */
 extern "C" int ccgpu_local_cc_host(ccgpu_ctx *ctx, const uint64_t *h_row_ptr,
                                    const uint32_t *h_col_idx, uint32_t n, uint64_t m,
                                    uint32_t *h_labels, const ccgpu_cc_opts *opts,
@@ -619,30 +723,35 @@ extern "C" int ccgpu_local_cc_host(ccgpu_ctx *ctx, const uint64_t *h_row_ptr,
     if (h_row_ptr[n] != m)
         return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_local_cc_host: row_ptr[n]=%llu != m=%llu",
                                (unsigned long long)h_row_ptr[n], (unsigned long long)m);
-    ccgpu_cc_opts o;
-    CC_TRY(resolve_opts(opts, &o));
+    LocalCCArgs a = {nullptr, nullptr, n, m, nullptr, nullptr, 1, {}};
+    CC_TRY(cc_local_resolve_opts(opts, &a.o));
     CC_TRY(ccgpu_ctx_resolve(&ctx));
 
-    Scratch s;
-    cc_carve c = {nullptr, 0};
-    carve_scratch(&c, &s, n, m, (uint32_t)o.heavy_degree);
-    uint64_t *d_row = (uint64_t *)cc_take(&c, ((size_t)n + 1) * sizeof(uint64_t));
-    uint32_t *d_col = (uint32_t *)cc_take(&c, (size_t)(m ? m : 1) * sizeof(uint32_t));
-    uint32_t *d_lab = (uint32_t *)cc_take(&c, (size_t)n * sizeof(uint32_t));
+    LocalCCScratch s;
+    uint64_t *d_row = nullptr;
+    uint32_t *d_col = nullptr, *d_lab = nullptr;
     void *base = nullptr;
-    CC_TRY(ccgpu_ctx_reserve(ctx, c.off, &base));
-    c = {(char *)base, 0};
-    carve_scratch(&c, &s, n, m, (uint32_t)o.heavy_degree);
-    d_row = (uint64_t *)cc_take(&c, ((size_t)n + 1) * sizeof(uint64_t));
-    d_col = (uint32_t *)cc_take(&c, (size_t)(m ? m : 1) * sizeof(uint32_t));
-    d_lab = (uint32_t *)cc_take(&c, (size_t)n * sizeof(uint32_t));
+    for (int pass = 0; pass < 2; ++pass) {
+        cc_carve c = {(char *)base, 0};
+        cc_local_carve(&c, &s, a);
+        d_row = (uint64_t *)cc_take(&c, ((size_t)n + 1) * sizeof(uint64_t));
+        d_col = (uint32_t *)cc_take(&c, (size_t)(m ? m : 1) * sizeof(uint32_t));
+        d_lab = (uint32_t *)cc_take(&c, (size_t)n * sizeof(uint32_t));
+        if (pass == 0)
+            CC_TRY(ccgpu_ctx_reserve(ctx, c.off, &base));
+    }
+    a.row_ptr = d_row;
+    a.col = d_col;
+    a.labels = d_lab;
 
     cudaStream_t st = nullptr, cp = nullptr;
     int rc = CCGPU_OK;
     const int kPieces = 8;
     cudaEvent_t ev[kPieces] = {};
-    Geometry g = {1, 1};
-    CC_TRY(geometry(ctx, &g));
+    const unsigned long long before = ctx->launches;
+    /* the init pass reads first neighbours when the first hook is on, so
+     * it then waits for all columns; otherwise sampling overlaps the copy */
+    const bool init_reads_cols = (a.o.hook_mode & CCGPU_HOOK_FIRST) && a.o.sample_rounds > 0;
 #define HOST_TRY(call)                                                         \
     do {                                                                       \
         cudaError_t e_ = (call);                                               \
@@ -651,20 +760,20 @@ extern "C" int ccgpu_local_cc_host(ccgpu_ctx *ctx, const uint64_t *h_row_ptr,
             goto done;                                                         \
         }                                                                      \
     } while (0)
+#define HOST_ST(call)                                                          \
+    do {                                                                       \
+        rc = (call);                                                           \
+        if (rc != CCGPU_OK)                                                    \
+            goto done;                                                         \
+    } while (0)
     HOST_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     HOST_TRY(cudaStreamCreateWithFlags(&cp, cudaStreamNonBlocking));
     for (int i = 0; i < kPieces; ++i)
         HOST_TRY(cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming));
     HOST_TRY(cudaMemcpyAsync(d_row, h_row_ptr, ((size_t)n + 1) * sizeof(uint64_t),
                              cudaMemcpyHostToDevice, st));
-    if (ctx->prof)
-        cc_prof_mark(ctx, CCK_INIT, 0, st);
-    k_init<<<cc_blocks(n, kBlock, g.stream_blocks), kBlock, 0, st>>>(
-        d_lab, n, (uint32_t *)s.grab, kCounterWords, 1);
-    HOST_TRY(cudaGetLastError());
-    ctx->launches++;
-    if (ctx->prof)
-        cc_prof_mark(ctx, CCK_INIT, 1, st);
+    if (!init_reads_cols)
+        HOST_ST(cc_local_init(ctx, a, s, st));
     HOST_TRY(cudaEventRecord(ev[0], st));
     HOST_TRY(cudaStreamWaitEvent(cp, ev[0], 0));
     for (int i = 0; i < kPieces; ++i) {
@@ -675,35 +784,28 @@ extern "C" int ccgpu_local_cc_host(ccgpu_ctx *ctx, const uint64_t *h_row_ptr,
             HOST_TRY(cudaMemcpyAsync(d_col + elo, h_col_idx + elo, (ehi - elo) * sizeof(uint32_t),
                                      cudaMemcpyHostToDevice, cp));
         HOST_TRY(cudaEventRecord(ev[i], cp));
-        if (o.sample_rounds > 0) {
+        if (!init_reads_cols) {
             HOST_TRY(cudaStreamWaitEvent(st, ev[i], 0));
-            if (ctx->prof)
-                cc_prof_mark(ctx, CCK_SAMPLE, 0, st);
-            k_sample<<<cc_blocks(vhi - vlo, kBlock, g.stream_blocks), kBlock, 0, st>>>(
-                d_row, d_col, n, m, d_lab, vlo, vhi, 0, o.sample_rounds);
-            HOST_TRY(cudaGetLastError());
-            ctx->launches++;
-            if (ctx->prof)
-                cc_prof_mark(ctx, CCK_SAMPLE, 1, st);
+            HOST_ST(cc_local_sample_range(ctx, a, vlo, vhi, st));
         }
     }
     HOST_TRY(cudaStreamWaitEvent(st, ev[kPieces - 1], 0));
-    {
-        uint32_t kernels = 0;
-        rc = local_cc_launch(ctx, d_row, d_col, n, m, d_lab, &o, s, st, 1, 1, &kernels);
-        if (rc != CCGPU_OK)
-            goto done;
-        HOST_TRY(cudaMemcpyAsync(h_labels, d_lab, (size_t)n * sizeof(uint32_t),
-                                 cudaMemcpyDeviceToHost, st));
-        if (stats) {
-            rc = fill_stats(ctx, s, d_lab, n, &o, kernels + 1 + kPieces, stats, st);
-            if (rc != CCGPU_OK)
-                goto done;
-        }
-        HOST_TRY(cudaStreamSynchronize(st));
-    }
+    if (init_reads_cols)
+        HOST_ST(cc_local_run(ctx, a, s, st, 0, 0));
+    else
+        HOST_ST(cc_local_run(ctx, a, s, st, 1, 1));
+    HOST_TRY(cudaMemcpyAsync(h_labels, d_lab, (size_t)n * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                             st));
+    if (stats)
+        HOST_ST(fill_stats(ctx, a, s, (uint32_t)(ctx->launches - before), stats, st));
+    HOST_TRY(cudaStreamSynchronize(st));
 done:
 #undef HOST_TRY
+#undef HOST_ST
+    if (rc != CCGPU_OK && st)
+        cudaStreamSynchronize(st);
+    if (rc != CCGPU_OK && cp)
+        cudaStreamSynchronize(cp);
     for (int i = 0; i < kPieces; ++i)
         if (ev[i])
             cudaEventDestroy(ev[i]);
@@ -729,10 +831,10 @@ extern "C" int ccgpu_count_roots(ccgpu_ctx *ctx, const uint32_t *d_labels, uint3
     unsigned long long *cell = nullptr;
     CC_TRY(ccgpu_ctx_cell(ctx, &cell));
     CC_CUDA(cudaMemsetAsync(cell, 0, sizeof(unsigned long long), st));
-    CC_KLAUNCH(ctx, CCK_COUNT_ROOTS, k_count_roots, cc_blocks(n, kBlock, (unsigned)ctx->sm_count * 8),
-               kBlock, 0, st, d_labels, n, cell);
-    CC_CUDA(cudaMemcpyAsync(host, cell, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
-                            st));
+    CC_KLAUNCH(ctx, CCK_COUNT_ROOTS, k_count_roots,
+               cc_blocks(n, kBlock, (unsigned)ctx->sm_count * 8), kBlock, 0, st, d_labels, n,
+               cell);
+    CC_CUDA(cudaMemcpyAsync(host, cell, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     CC_CUDA(cudaStreamSynchronize(st));
     *count = *(unsigned long long *)host;
     return CCGPU_OK;
@@ -759,7 +861,6 @@ extern "C" int ccgpu_check_labels(ccgpu_ctx *ctx, const uint64_t *d_row_ptr,
                d_row_ptr, d_col_idx, n, m, d_labels, d_bad);
     CC_CUDA(cudaMemcpyAsync(host, d_bad, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     CC_CUDA(cudaStreamSynchronize(st));
-    unsigned long long h = *(unsigned long long *)host;
-    *violations = h;
+    *violations = *(unsigned long long *)host;
     return CCGPU_OK;
 }

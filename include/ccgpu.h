@@ -104,7 +104,19 @@ typedef struct {
                          * <= 0 = default (8192)                              */
     int skip_giant;     /* 1 (default) = step 4 skips the giant tree;
                          * 0 = link every remaining neighbour               */
+    int hook_mode;      /* bit mask, < 0 = default (CADENCE):
+                         *  1 FIRST: the init pass hooks v under its first
+                         *    neighbour when that is smaller (plain store,
+                         *    no walk); step 1 links the rest
+                         *  2 LAZY: a root is hooked under the smaller
+                         *    endpoint itself instead of walking to its root
+                         *  4 CADENCE: one launch per sampled neighbour with a
+                         *    shortcut pass after each                        */
 } ccgpu_cc_opts;
+
+#define CCGPU_HOOK_FIRST 1
+#define CCGPU_HOOK_LAZY 2
+#define CCGPU_HOOK_CADENCE 4
 
 typedef struct {
     uint32_t giant_label;   /* root found in step 3 (UINT32_MAX if off)      */

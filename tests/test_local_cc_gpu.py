@@ -18,6 +18,9 @@ OPTION_GRID = [
     dict(chunk_size=100, sample_rounds=4, heavy_degree=33, skip_giant=0),      # odd chunk
     dict(chunk_size=8192, sample_rounds=8, heavy_degree=100000, skip_giant=1),
 ]
+# every hook mode (first hook / lazy hook / cadence) on two schedules
+OPTION_GRID += [dict(chunk_size=c, sample_rounds=r, heavy_degree=64, skip_giant=1, hook_mode=h)
+                for h in range(8) for c, r in ((4096, 2), (1, 3))]
 
 
 @pytest.fixture(scope="module")
@@ -162,3 +165,19 @@ def test_profiler_and_launch_counter(torch):
     got = {names[i]: cnt[i] for i in range(k) if cnt[i]}
     assert got.get("sample") == 1 and got.get("link_rows") == 1
     assert L.ccgpu_ctx_launches(None) - before == sum(cnt)
+
+
+def test_final_shortcut_race_regression(torch):
+    """Long paths and tile-boundary vertices under every hook mode and
+    schedule, repeated: a plain halving store once put an intermediate
+    ancestor back over a root pointer written in the final shortcut pass."""
+    cases = [graphs.csr_from_edges(20000, np.arange(19999), np.arange(1, 20000)),
+             graphs.small_cases()["zigzag"], graphs.small_cases()["long_path"]]
+    for rp, col in cases:
+        uf = oracle.uf_labels(rp, col)
+        for hm in range(8):
+            for ch, sr in ((1, 0), (256, 0), (2048, 2), (4096, 1)):
+                for _ in range(3):
+                    lab = solve_dev(torch, rp, col, _lib.opts(chunk_size=ch, sample_rounds=sr,
+                                                               hook_mode=hm))
+                    assert (lab == uf).all(), (hm, ch, sr)
