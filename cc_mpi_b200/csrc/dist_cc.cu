@@ -1,0 +1,1154 @@
+/*
+ * Partitioned connected components with every partition resident in HBM.
+ *
+ * Restates the reference's distributed path on one device:
+ *   src/graph_dist.c:22-92      partition bounds           -> k_bounds
+ *   src/cc_mpi.c:252-323        local subgraph + local CC  -> segmented
+ *                               union-find with a same-partition edge filter
+ *   src/cc_mpi.c:326-362        reps, comp_label init      -> k_reps
+ *   src/cc_mpi.c:364-394        boundary pairs             -> k_emit*
+ *   src/boundary_sort.c         sort + dedup               -> radix sort,
+ *                                                             k_dedup_*
+ *   src/cc_mpi.c:425-461        ghosts                     -> k_dedup_write
+ *   src/exchange_plan.c:48-225  exchange plan              -> k_plan
+ *   src/cc_mpi.c:541-710        merge rounds               -> k_hook_init,
+ *                                                             k_upd
+ *   src/exchange_plan.c:242-425 delta exchange             -> k_pack,
+ *                                                             k_scatter
+ *   src/cc_mpi.c:730-742        roots / labels             -> k_final
+ *
+ * Layout in HBM: all per-vertex arrays are indexed by global vertex id (a
+ * partition is a contiguous slice), so a partition's comp_label/comp_of of
+ * the reference are slices of cur[] and label[].  Boundary keys pack
+ * (partition, remote, rep) so one sort orders every partition's pairs at
+ * once; after dedup, partition p's ghosts are the contiguous range
+ * [gh_off[p], gh_off[p+1]) and the ghosts it needs from partition q are the
+ * sub-range [seg[p][q], seg[p][q+1]) - the reference's need_from lists.
+ *
+ * The reference's HOOK (comp_min = min over cut pairs of the ghost labels)
+ * only changes when ghost labels change, i.e. at exchanges; hook[] keeps that
+ * minimum per rep and is lowered by the exchange scatter for the pairs of
+ * each ghost that received a label, which gives the same comp_min every
+ * round without re-reading every pair.
+ */
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "local_cc.h"
+#include "primitives.h"
+
+namespace {
+
+constexpr int kB = 256;
+constexpr int kW = kB / 32;
+constexpr int kEmitBuf = 512;           /* keys per warp buffer           */
+constexpr uint64_t kHeavyChunk = 1024;  /* entries per warp in heavy rows */
+constexpr int kDedupItems = 16;
+constexpr uint64_t kDedupTile = kB * kDedupItems;
+
+__device__ __forceinline__ int part_of(const uint32_t *__restrict__ b, int parts, uint32_t v)
+{
+    int lo = 0, hi = parts;
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (b[mid] <= v)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+/* ------------------------------------------------------------- bounds */
+
+/* One thread replays the reference's cursor loop (src/graph_dist.c:70-89)
+ * with a binary search per cut: the running weight after advancing the
+ * cursor from (v, cum) to v' is cum + row_ptr[v'] - row_ptr[v] + (v' - v),
+ * strictly increasing in v'.  The clamp moves the cursor but not the
+ * running weight, exactly as in the reference. */
+__global__ void k_bounds(const uint64_t *__restrict__ row_ptr, uint32_t n, int parts, int kind,
+                         uint32_t *bounds, uint64_t *seg)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0)
+        return;
+    if (kind == 0) {
+        uint32_t base = n / (uint32_t)parts, rem = n % (uint32_t)parts;
+        for (int r = 0; r < parts; ++r) {
+            uint32_t ru = (uint32_t)r;
+            bounds[r] = ru < rem ? ru * (base + 1u) : rem * (base + 1u) + (ru - rem) * base;
+        }
+        bounds[parts] = n;
+    } else {
+        const uint64_t rp0 = row_ptr[0];
+        const uint64_t total_w = (row_ptr[n] - rp0) + (uint64_t)n;
+        bounds[0] = 0;
+        uint32_t v = 0;
+        uint64_t cum = 0;
+        for (int r = 1; r < parts; ++r) {
+            uint64_t target = total_w * (uint64_t)r / (uint64_t)parts;
+            if (v < n && cum < target) {
+                const uint32_t v0 = v;
+                const uint64_t base = cum - (row_ptr[v0] - rp0) - v0;
+                /* smallest v' in (v0, n] with base + (row_ptr[v'] - rp0) + v' >= target */
+                uint32_t lo = v0 + 1, hi = n;
+                while (lo < hi) {
+                    uint32_t mid = lo + (hi - lo) / 2;
+                    if (base + (row_ptr[mid] - rp0) + mid >= target)
+                        hi = mid;
+                    else
+                        lo = mid + 1;
+                }
+                v = lo;
+                cum = base + (row_ptr[v] - rp0) + v;
+            }
+            uint32_t min_v = bounds[r - 1] + 1u;
+            uint32_t max_v = n - (uint32_t)(parts - r);
+            if (v < min_v)
+                v = min_v;
+            if (v > max_v)
+                v = max_v;
+            bounds[r] = v;
+        }
+        bounds[parts] = n;
+    }
+    for (int r = 0; r <= parts; ++r)
+        seg[r] = bounds[r];
+}
+
+/* ---------------------------------------------------- boundary emission */
+
+struct EmitParams {
+    const uint64_t *row_ptr;
+    const uint32_t *col;
+    const uint32_t *label;   /* local CC labels (global min ids)          */
+    const uint32_t *bounds;  /* [parts+1]                                  */
+    uint32_t n;
+    uint64_t m;
+    int parts;
+    int rb, gb;              /* key bit widths of rep and remote          */
+    uint64_t *out;           /* keys, capacity m                          */
+    unsigned long long *count;
+    uint32_t *heavy_list;
+    uint32_t *heavy_count;
+    uint32_t heavy_cap;
+    uint32_t heavy_deg;
+};
+
+struct WarpBuf {
+    uint64_t *buf;
+    uint32_t cnt;
+};
+
+__device__ __forceinline__ void wb_flush(WarpBuf &w, const EmitParams &E, int lane)
+{
+    __syncwarp();
+    unsigned long long base = 0;
+    if (lane == 0 && w.cnt)
+        base = atomicAdd(E.count, (unsigned long long)w.cnt);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    for (uint32_t i = lane; i < w.cnt; i += 32)
+        E.out[base + i] = w.buf[i];
+    w.cnt = 0;
+    __syncwarp();
+}
+
+__device__ __forceinline__ void wb_append(WarpBuf &w, const EmitParams &E, int lane, bool pred,
+                                          uint64_t key)
+{
+    unsigned mask = __ballot_sync(0xffffffffu, pred);
+    if (!mask)
+        return;
+    if (w.cnt + 32 > kEmitBuf)
+        wb_flush(w, E, lane);
+    if (pred)
+        w.buf[w.cnt + __popc(mask & ((1u << lane) - 1u))] = key;
+    w.cnt += __popc(mask);
+}
+
+__device__ __forceinline__ uint64_t make_key(const EmitParams &E, int p, uint32_t u, uint32_t rep)
+{
+    return ((uint64_t)p << (E.gb + E.rb)) | ((uint64_t)u << E.rb) | rep;
+}
+
+__global__ void __launch_bounds__(kB) k_emit(EmitParams E)
+{
+    __shared__ uint64_t s_buf[kW][kEmitBuf];
+    __shared__ uint32_t s_b[CCGPU_MAX_PARTS + 1];
+    for (int i = threadIdx.x; i <= E.parts; i += kB)
+        s_b[i] = E.bounds[i];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    WarpBuf w = {s_buf[warp], 0};
+    const uint64_t wstride = (uint64_t)gridDim.x * kW * 32;
+    for (uint64_t w0 = ((uint64_t)blockIdx.x * kW + warp) * 32; w0 < E.n; w0 += wstride) {
+        const uint64_t v64 = w0 + lane;
+        const bool valid = v64 < E.n;
+        const uint32_t v = valid ? (uint32_t)v64 : 0u;
+        int p = part_of(s_b, E.parts, v);
+        uint32_t lo = s_b[p], hi = s_b[p + 1];
+        uint32_t rep = valid ? __ldg(E.label + v) - lo : 0u;
+        uint64_t beg = 0, end = 0;
+        if (valid) {
+            beg = __ldg(E.row_ptr + v);
+            end = __ldg(E.row_ptr + v + 1);
+            if (end > E.m)
+                end = E.m;
+            if (beg > end)
+                beg = end;
+        }
+        uint64_t deg = end - beg;
+        if (deg > E.heavy_deg) {
+            uint32_t slot = atomicAdd(E.heavy_count, 1u);
+            if (slot < E.heavy_cap) {
+                E.heavy_list[slot] = v;
+                deg = 0;
+            }
+        }
+        unsigned big = __ballot_sync(0xffffffffu, deg >= 32);
+        while (big) {
+            int src = __ffs(big) - 1;
+            big &= big - 1;
+            uint64_t bb = __shfl_sync(0xffffffffu, beg, src);
+            uint64_t ee = __shfl_sync(0xffffffffu, end, src);
+            int pp = __shfl_sync(0xffffffffu, p, src);
+            uint32_t ll = __shfl_sync(0xffffffffu, lo, src);
+            uint32_t hh = __shfl_sync(0xffffffffu, hi, src);
+            uint32_t rr = __shfl_sync(0xffffffffu, rep, src);
+            for (uint64_t j0 = bb; j0 < ee; j0 += 32) {
+                uint64_t j = j0 + lane;
+                uint32_t u = j < ee ? __ldg(E.col + j) : E.n;
+                bool bnd = u < E.n && (u < ll || u >= hh);
+                wb_append(w, E, lane, bnd, make_key(E, pp, u, rr));
+            }
+        }
+        uint32_t sdeg = deg < 32 ? (uint32_t)deg : 0u;
+        uint32_t maxd = __reduce_max_sync(0xffffffffu, sdeg);
+        for (uint32_t it = 0; it < maxd; ++it) {
+            uint32_t u = it < sdeg ? __ldg(E.col + beg + it) : E.n;
+            bool bnd = u < E.n && (u < lo || u >= hi);
+            wb_append(w, E, lane, bnd, make_key(E, p, u, rep));
+        }
+    }
+    wb_flush(w, E, lane);
+}
+
+__global__ void __launch_bounds__(kB) k_emit_heavy(EmitParams E)
+{
+    __shared__ uint64_t s_buf[kW][kEmitBuf];
+    __shared__ uint32_t s_b[CCGPU_MAX_PARTS + 1];
+    for (int i = threadIdx.x; i <= E.parts; i += kB)
+        s_b[i] = E.bounds[i];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    WarpBuf w = {s_buf[warp], 0};
+    uint32_t cnt = *E.heavy_count;
+    if (cnt > E.heavy_cap)
+        cnt = E.heavy_cap;
+    const uint64_t gw = (uint64_t)blockIdx.x * kW + warp, nw = (uint64_t)gridDim.x * kW;
+    for (uint32_t h = 0; h < cnt; ++h) {
+        uint32_t v = E.heavy_list[h];
+        int p = part_of(s_b, E.parts, v);
+        uint32_t lo = s_b[p], hi = s_b[p + 1];
+        uint32_t rep = __ldg(E.label + v) - lo;
+        uint64_t beg = __ldg(E.row_ptr + v), end = __ldg(E.row_ptr + v + 1);
+        if (end > E.m)
+            end = E.m;
+        if (beg > end)
+            beg = end;
+        uint64_t chunks = (end - beg + kHeavyChunk - 1) / kHeavyChunk;
+        for (uint64_t c = gw; c < chunks; c += nw) {
+            uint64_t cb = beg + c * kHeavyChunk;
+            uint64_t ce = cb + kHeavyChunk < end ? cb + kHeavyChunk : end;
+            for (uint64_t j0 = cb; j0 < ce; j0 += 32) {
+                uint64_t j = j0 + lane;
+                uint32_t u = j < ce ? __ldg(E.col + j) : E.n;
+                bool bnd = u < E.n && (u < lo || u >= hi);
+                wb_append(w, E, lane, bnd, make_key(E, p, u, rep));
+            }
+        }
+    }
+    wb_flush(w, E, lane);
+}
+
+/* --------------------------------------------------------------- reps */
+
+__global__ void __launch_bounds__(kB) k_reps(const uint32_t *__restrict__ label, uint32_t n,
+                                             uint32_t *rep_list, unsigned long long *rep_count,
+                                             uint32_t *cur, uint32_t *hook)
+{
+    const int lane = threadIdx.x & 31;
+    const uint64_t stride = (uint64_t)gridDim.x * kB;
+    for (uint64_t base = (uint64_t)blockIdx.x * kB; base < n; base += stride) {
+        uint64_t v = base + threadIdx.x;
+        bool is_rep = v < n && __ldg(label + v) == (uint32_t)v;
+        unsigned mask = __ballot_sync(0xffffffffu, is_rep);
+        unsigned long long slot = 0;
+        if (lane == 0 && mask)
+            slot = atomicAdd(rep_count, (unsigned long long)__popc(mask));
+        slot = __shfl_sync(0xffffffffu, slot, 0);
+        if (is_rep) {
+            rep_list[slot + __popc(mask & ((1u << lane) - 1u))] = (uint32_t)v;
+            cur[v] = (uint32_t)v; /* comp_label[i] = v_start + i, src/cc_mpi.c:361-362 */
+            hook[v] = 0xffffffffu;
+        }
+    }
+}
+
+/* -------------------------------------------------------------- dedup */
+
+struct DedupParams {
+    const uint64_t *keys;   /* sorted */
+    uint64_t count;
+    int rb, gb;
+    const uint32_t *bounds;
+    int parts;
+    uint32_t *tile_u, *tile_g;         /* per tile counts   */
+    const uint64_t *u_off, *g_off;     /* scanned, [T+1]    */
+    uint32_t *pair_rep, *pair_g;       /* [U]               */
+    uint32_t *ghost_v;                 /* [G]               */
+    uint64_t *ghost_pairs;             /* [G+1] first pair  */
+    uint32_t *ghost_labels, *prev_sent;
+    unsigned long long *gcount;        /* [parts]           */
+};
+
+__device__ __forceinline__ void dedup_flags(const DedupParams &D, uint64_t i, uint64_t k,
+                                            bool &uniq, bool &gst)
+{
+    if (i == 0) {
+        uniq = gst = true;
+        return;
+    }
+    uint64_t prev = D.keys[i - 1];
+    uniq = k != prev;
+    gst = (k >> D.rb) != (prev >> D.rb);
+}
+
+__global__ void __launch_bounds__(kB) k_dedup_count(DedupParams D)
+{
+    __shared__ uint32_t s_w[2][kW];
+    const uint64_t base = (uint64_t)blockIdx.x * kDedupTile + (uint64_t)threadIdx.x * kDedupItems;
+    uint32_t cu = 0, cg = 0;
+    for (int j = 0; j < kDedupItems; ++j) {
+        uint64_t i = base + j;
+        if (i < D.count) {
+            bool u, g;
+            dedup_flags(D, i, D.keys[i], u, g);
+            cu += u;
+            cg += g;
+        }
+    }
+    cu = __reduce_add_sync(0xffffffffu, cu);
+    cg = __reduce_add_sync(0xffffffffu, cg);
+    if ((threadIdx.x & 31) == 0) {
+        s_w[0][threadIdx.x >> 5] = cu;
+        s_w[1][threadIdx.x >> 5] = cg;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t a = 0, b = 0;
+        for (int w = 0; w < kW; ++w) {
+            a += s_w[0][w];
+            b += s_w[1][w];
+        }
+        D.tile_u[blockIdx.x] = a;
+        D.tile_g[blockIdx.x] = b;
+    }
+}
+
+__global__ void __launch_bounds__(kB) k_dedup_write(DedupParams D)
+{
+    __shared__ uint32_t s_wu[kW], s_wg[kW];
+    __shared__ uint32_t s_b[CCGPU_MAX_PARTS + 1];
+    for (int i = threadIdx.x; i <= D.parts; i += kB)
+        s_b[i] = D.bounds[i];
+    const uint64_t base = (uint64_t)blockIdx.x * kDedupTile + (uint64_t)threadIdx.x * kDedupItems;
+    uint32_t cu = 0, cg = 0;
+    for (int j = 0; j < kDedupItems; ++j) {
+        uint64_t i = base + j;
+        if (i < D.count) {
+            bool u, g;
+            dedup_flags(D, i, D.keys[i], u, g);
+            cu += u;
+            cg += g;
+        }
+    }
+    uint32_t iu = cc_block_incl_scan256<uint32_t>(cu, s_wu, nullptr);
+    uint32_t ig = cc_block_incl_scan256<uint32_t>(cg, s_wg, nullptr);
+    uint64_t up = D.u_off[blockIdx.x] + iu - cu; /* first unique index of this thread */
+    uint64_t gp = D.g_off[blockIdx.x] + ig - cg; /* ghosts started before this thread */
+    const uint64_t pmask = (1ull << D.gb) - 1ull;
+    const uint64_t rmask = (1ull << D.rb) - 1ull;
+    for (int j = 0; j < kDedupItems; ++j) {
+        uint64_t i = base + j;
+        if (i >= D.count)
+            break;
+        uint64_t k = D.keys[i];
+        bool u, g;
+        dedup_flags(D, i, k, u, g);
+        if (g) {
+            uint32_t remote = (uint32_t)((k >> D.rb) & pmask);
+            int p = (int)(k >> (D.rb + D.gb));
+            D.ghost_v[gp] = remote;
+            D.ghost_pairs[gp] = up;
+            D.ghost_labels[gp] = remote;   /* src/cc_mpi.c:456-457 */
+            D.prev_sent[gp] = 0xffffffffu; /* src/cc_mpi.c:480-487 */
+            atomicAdd(D.gcount + p, 1ull);
+            gp++;
+        }
+        if (u) {
+            int p = (int)(k >> (D.rb + D.gb));
+            D.pair_rep[up] = s_b[p] + (uint32_t)(k & rmask);
+            D.pair_g[up] = (uint32_t)(gp - 1);
+            up++;
+        }
+    }
+}
+
+/* --------------------------------------------------------------- plan */
+
+/* seg[p*(parts+1)+q] = first ghost of partition p owned by partition >= q
+ * (src/exchange_plan.c:74-83: need_from lists grouped by owner). */
+__global__ void k_plan(const uint32_t *__restrict__ ghost_v, const uint64_t *__restrict__ gh_off,
+                       const uint32_t *__restrict__ bounds, int parts, uint64_t *seg)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= parts * (parts + 1))
+        return;
+    int p = t / (parts + 1), q = t % (parts + 1);
+    uint64_t lo = gh_off[p], hi = gh_off[p + 1];
+    uint32_t key = bounds[q];
+    if (q == parts) {
+        seg[t] = hi;
+        return;
+    }
+    while (lo < hi) {
+        uint64_t mid = lo + (hi - lo) / 2;
+        if (ghost_v[mid] < key)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    seg[t] = lo;
+}
+
+/* ------------------------------------------------------------- merge */
+
+struct MergeParams {
+    const uint32_t *label;        /* comp_of as global rep ids          */
+    const uint32_t *bounds;
+    int parts;
+    const uint32_t *rep_list;
+    uint64_t rep_count;
+    const uint32_t *cur;
+    uint32_t *next;
+    uint32_t *hook;
+    const uint32_t *pair_rep, *pair_g;
+    uint64_t pairs;
+    const uint32_t *ghost_v;
+    const uint64_t *ghost_pairs;
+    uint32_t *ghost_labels;
+    uint32_t *prev_sent;
+    uint64_t ghosts;
+    const uint64_t *gh_off;       /* [parts+1] */
+    const uint64_t *seg;          /* [parts*(parts+1)] */
+    uint64_t *msg;                /* [ghosts] */
+    uint32_t *msg_count;          /* [parts*parts], [q*parts+p] */
+    int *changed;                 /* [parts] */
+    unsigned long long *sent;
+};
+
+/* hook[rep] = min over the rep's cut pairs of the ghost labels. */
+__global__ void __launch_bounds__(kB) k_hook_init(MergeParams M)
+{
+    const int lane = threadIdx.x & 31;
+    const uint64_t stride = (uint64_t)gridDim.x * kB;
+    for (uint64_t base = (uint64_t)blockIdx.x * kB; base < M.pairs; base += stride) {
+        uint64_t k = base + threadIdx.x;
+        bool ok = k < M.pairs;
+        uint32_t r = ok ? M.pair_rep[k] : 0xffffffffu;
+        uint32_t l = ok ? M.ghost_labels[M.pair_g[k]] : 0xffffffffu;
+        unsigned peers = __match_any_sync(0xffffffffu, r);
+        uint32_t mn = __reduce_min_sync(peers, l);
+        if (ok && (__ffs(peers) - 1) == lane)
+            atomicMin(M.hook + r, mn);
+    }
+}
+
+__device__ __forceinline__ bool label_of(const MergeParams &M, const uint32_t *s_b, int p,
+                                         uint32_t x, uint32_t &y)
+{
+    if (x >= s_b[p] && x < s_b[p + 1]) {
+        y = M.cur[__ldg(M.label + x)];
+        return true;
+    }
+    uint64_t lo = M.gh_off[p], hi = M.gh_off[p + 1];
+    while (lo < hi) {
+        uint64_t mid = lo + (hi - lo) / 2;
+        if (__ldg(M.ghost_v + mid) < x)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    if (lo < M.gh_off[p + 1] && __ldg(M.ghost_v + lo) == x) {
+        y = M.ghost_labels[lo];
+        return true;
+    }
+    return false;
+}
+
+/* One merge round over every rep (src/cc_mpi.c:547-622, MAX_JUMPS = 4),
+ * reading cur and writing next. */
+__global__ void __launch_bounds__(kB) k_upd(MergeParams M)
+{
+    __shared__ uint32_t s_b[CCGPU_MAX_PARTS + 1];
+    for (int i = threadIdx.x; i <= M.parts; i += kB)
+        s_b[i] = M.bounds[i];
+    __syncthreads();
+    const uint64_t stride = (uint64_t)gridDim.x * kB;
+    for (uint64_t i = (uint64_t)blockIdx.x * kB + threadIdx.x; i < M.rep_count; i += stride) {
+        uint32_t r = M.rep_list[i];
+        int p = part_of(s_b, M.parts, r);
+        uint32_t c = M.cur[r], h = M.hook[r];
+        uint32_t x = h < c ? h : c;
+        for (int t = 0; t < 4; ++t) {
+            uint32_t y;
+            if (!label_of(M, s_b, p, x, y) || y >= x)
+                break;
+            x = y;
+        }
+        M.next[r] = x;
+        if (x < c)
+            M.changed[p] = 1;
+    }
+}
+
+/* Delta exchange, sender side (src/exchange_plan.c:325-357): for every
+ * ghost g of partition p owned by q, q's current label of the ghost vertex
+ * goes out when it fell below what q sent last time; it is written as
+ * (position in the need-from range, label) into the (q -> p) region. */
+__global__ void __launch_bounds__(kB) k_pack(MergeParams M)
+{
+    __shared__ uint32_t s_b[CCGPU_MAX_PARTS + 1];
+    for (int i = threadIdx.x; i <= M.parts; i += kB)
+        s_b[i] = M.bounds[i];
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const uint64_t stride = (uint64_t)gridDim.x * kB;
+    for (uint64_t base = (uint64_t)blockIdx.x * kB; base < M.ghosts; base += stride) {
+        uint64_t g = base + threadIdx.x;
+        bool send = false;
+        uint32_t lbl = 0, region = 0xffffffffu;
+        uint64_t rstart = 0;
+        if (g < M.ghosts) {
+            uint32_t u = __ldg(M.ghost_v + g);
+            int q = part_of(s_b, M.parts, u);
+            int lo = 0, hi = M.parts; /* partition p whose ghost range holds g */
+            while (hi - lo > 1) {
+                int mid = (lo + hi) >> 1;
+                if (M.gh_off[mid] <= g)
+                    lo = mid;
+                else
+                    hi = mid;
+            }
+            int p = lo;
+            lbl = M.cur[__ldg(M.label + u)];
+            if (lbl < M.prev_sent[g]) {
+                M.prev_sent[g] = lbl;
+                send = true;
+                region = (uint32_t)(q * M.parts + p);
+                rstart = M.seg[(uint64_t)p * (M.parts + 1) + q];
+            }
+        }
+        unsigned peers = __match_any_sync(0xffffffffu, region);
+        uint32_t slot = 0;
+        if (send && (__ffs(peers) - 1) == lane)
+            slot = atomicAdd(M.msg_count + region, (uint32_t)__popc(peers));
+        slot = __shfl_sync(peers, slot, __ffs(peers) - 1);
+        if (send) {
+            slot += __popc(peers & ((1u << lane) - 1u));
+            M.msg[rstart + slot] = ((uint64_t)(g - rstart) << 32) | lbl;
+        }
+    }
+}
+
+/* Receiver side (src/exchange_plan.c:390-413): ghost_labels[pos] = label,
+ * and the hook minimum of every rep paired with that ghost is lowered. */
+__global__ void __launch_bounds__(kB) k_scatter(MergeParams M)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * kB;
+    const int regions = M.parts * M.parts;
+    for (uint64_t s = (uint64_t)blockIdx.x * kB + threadIdx.x; s < M.ghosts; s += stride) {
+        /* region (p, q) holding slot s: seg is ascending in p-major order */
+        int lo = 0, hi = regions;
+        while (hi - lo > 1) {
+            int mid = (lo + hi) >> 1;
+            int p = mid / M.parts, q = mid % M.parts;
+            if (M.seg[(uint64_t)p * (M.parts + 1) + q] <= s)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        int p = lo / M.parts, q = lo % M.parts;
+        uint64_t rstart = M.seg[(uint64_t)p * (M.parts + 1) + q];
+        if (s - rstart >= M.msg_count[q * M.parts + p])
+            continue;
+        uint64_t pr = M.msg[s];
+        uint64_t g = rstart + (pr >> 32);
+        uint32_t lbl = (uint32_t)pr;
+        M.ghost_labels[g] = lbl;
+        for (uint64_t k = M.ghost_pairs[g]; k < M.ghost_pairs[g + 1]; ++k)
+            atomicMin(M.hook + M.pair_rep[k], lbl);
+        atomicAdd(M.sent, 1ull);
+    }
+}
+
+__global__ void __launch_bounds__(kB) k_final(const uint32_t *__restrict__ label,
+                                              const uint32_t *__restrict__ cur, uint32_t n,
+                                              uint32_t *out, unsigned long long *roots)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * kB;
+    uint32_t c = 0;
+    for (uint64_t v = (uint64_t)blockIdx.x * kB + threadIdx.x; v < n; v += stride) {
+        uint32_t l = cur[__ldg(label + v)];
+        if (out)
+            out[v] = l;
+        c += (l == (uint32_t)v);
+    }
+    c = __reduce_add_sync(0xffffffffu, c);
+    if ((threadIdx.x & 31) == 0 && c)
+        atomicAdd(roots, (unsigned long long)c);
+}
+
+int bits_for(uint64_t max_value)
+{
+    int b = 0;
+    while (b < 64 && (max_value >> b) != 0)
+        ++b;
+    return b < 1 ? 1 : b;
+}
+
+struct PhaseClock {
+    cudaEvent_t ev[8];
+    int n = 0;
+    bool on = false;
+};
+
+int clock_mark(PhaseClock &c, cudaStream_t st)
+{
+    if (!c.on)
+        return CCGPU_OK;
+    CC_CUDA(cudaEventRecord(c.ev[c.n++], st));
+    return CCGPU_OK;
+}
+
+} // namespace
+
+/* ------------------------------------------------------------------ API */
+
+extern "C" void ccgpu_dist_opts_default(ccgpu_dist_opts *o)
+{
+    if (!o)
+        return;
+    o->parts = 1;
+    o->use_edge = 1;
+    o->chunk_size = 2048; /* the reference CLI's default -c, src/mpi_cc_benchmark.c:40 */
+    o->exchange_interval = 1;
+    o->verbose = 0;
+}
+
+extern "C" int ccgpu_partition_bounds(const uint64_t *d_row_ptr, uint32_t n, int parts,
+                                      int use_edge, uint32_t *h_bounds, void *stream)
+{
+    if (!d_row_ptr || !h_bounds || parts < 1 || parts > CCGPU_MAX_PARTS)
+        return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_partition_bounds: bad arguments");
+    if ((uint32_t)parts > n && n > 0)
+        return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_partition_bounds: %d parts > %u vertices",
+                               parts, n);
+    cudaStream_t st = (cudaStream_t)stream;
+    DevBufs b;
+    CC_TRY(cc_bufs_init(&b, st));
+    uint32_t *d_b = nullptr;
+    uint64_t *d_s = nullptr;
+    int rc = cc_bufs_get(&b, (void **)&d_b, (parts + 1) * sizeof(uint32_t));
+    if (rc == CCGPU_OK)
+        rc = cc_bufs_get(&b, (void **)&d_s, (parts + 1) * sizeof(uint64_t));
+    if (rc == CCGPU_OK) {
+        k_bounds<<<1, 32, 0, st>>>(d_row_ptr, n, parts, (use_edge && parts > 1) ? 1 : 0, d_b, d_s);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(h_bounds, d_b, (parts + 1) * sizeof(uint32_t),
+                                cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess)
+            e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess)
+            rc = ccgpu_cuda_fail(e, "partition bounds", __FILE__, __LINE__);
+    }
+    cc_bufs_release(&b);
+    return rc;
+}
+
+static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d_col, uint32_t n,
+                    uint64_t m, const ccgpu_dist_opts &o, uint32_t *d_labels, uint32_t *h_bounds,
+                    ccgpu_dist_stats *st_out, cudaStream_t st, DevBufs &B)
+{
+    const int P = o.parts;
+    const int interval = o.exchange_interval < 1 ? 1 : o.exchange_interval;
+    ccgpu_dist_stats S;
+    memset(&S, 0, sizeof(S));
+    PhaseClock clk;
+    clk.on = st_out != nullptr || o.verbose;
+    for (int i = 0; clk.on && i < 8; ++i)
+        CC_CUDA(cudaEventCreate(&clk.ev[i]));
+    struct EvGuard {
+        PhaseClock &c;
+        ~EvGuard()
+        {
+            for (int i = 0; c.on && i < 8; ++i)
+                cudaEventDestroy(c.ev[i]);
+        }
+    } guard{clk};
+    CC_TRY(clock_mark(clk, st)); /* 0 */
+
+    /* 1. bounds */
+    uint32_t *bounds = nullptr;
+    uint64_t *seg64 = nullptr;
+    CC_TRY(cc_bufs_get(&B, (void **)&bounds, (P + 1) * sizeof(uint32_t)));
+    CC_TRY(cc_bufs_get(&B, (void **)&seg64, (P + 1) * sizeof(uint64_t)));
+    const int kind = (o.use_edge && P > 1) ? 1 : 0;
+    CC_KLAUNCH(ctx, CCK_DIST_BOUNDS, k_bounds, 1, 32, 0, st, d_row_ptr, n, P, kind, bounds, seg64);
+    std::vector<uint32_t> hb(P + 1);
+    CC_CUDA(cudaMemcpyAsync(hb.data(), bounds, (P + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                            st));
+    CC_CUDA(cudaStreamSynchronize(st));
+    if (h_bounds)
+        memcpy(h_bounds, hb.data(), (P + 1) * sizeof(uint32_t));
+    uint32_t max_local = 1;
+    for (int p = 0; p < P; ++p)
+        if (hb[p + 1] - hb[p] > max_local)
+            max_local = hb[p + 1] - hb[p];
+    CC_TRY(clock_mark(clk, st)); /* 1 */
+
+    /* 2. local CC of every partition's local subgraph */
+    uint32_t *label = nullptr;
+    CC_TRY(cc_bufs_get(&B, (void **)&label, (size_t)n * sizeof(uint32_t)));
+    LocalCCArgs a = {d_row_ptr, d_col, n, m, label, seg64, (uint32_t)P, {}, 1};
+    ccgpu_cc_opts lo;
+    ccgpu_cc_opts_default(&lo);
+    lo.chunk_size = o.chunk_size;
+    CC_TRY(cc_local_resolve_opts(&lo, &a.o));
+    LocalCCScratch ls;
+    {
+        cc_carve c = {nullptr, 0};
+        cc_local_carve(&c, &ls, a);
+        void *base = nullptr;
+        CC_TRY(cc_bufs_get(&B, &base, c.off));
+        c = {(char *)base, 0};
+        cc_local_carve(&c, &ls, a);
+    }
+    CC_TRY(cc_local_run(ctx, a, ls, st, 0, 0));
+    CC_TRY(clock_mark(clk, st)); /* 2 */
+
+    /* 3. reps and boundary keys */
+    const int rb = bits_for(max_local - 1 ? max_local - 1 : 1);
+    const int gb = bits_for(n - 1 ? n - 1 : 1);
+    const int pb = P > 1 ? bits_for((uint64_t)P - 1) : 0;
+    if (rb + gb + pb > 64)
+        return ccgpu_set_error(CCGPU_ERR_LIMIT, "boundary key needs %d bits", rb + gb + pb);
+    uint32_t *rep_list = nullptr, *cur = nullptr, *nxt = nullptr, *hook = nullptr;
+    unsigned long long *counters = nullptr; /* [0] keys [1] reps [2] roots [3] sent */
+    CC_TRY(cc_bufs_get(&B, (void **)&rep_list, (size_t)n * sizeof(uint32_t)));
+    CC_TRY(cc_bufs_get(&B, (void **)&cur, (size_t)n * sizeof(uint32_t)));
+    CC_TRY(cc_bufs_get(&B, (void **)&nxt, (size_t)n * sizeof(uint32_t)));
+    CC_TRY(cc_bufs_get(&B, (void **)&hook, (size_t)n * sizeof(uint32_t)));
+    CC_TRY(cc_bufs_get(&B, (void **)&counters, 8 * sizeof(unsigned long long)));
+    CC_CUDA(cudaMemsetAsync(counters, 0, 8 * sizeof(unsigned long long), st));
+    const unsigned sb = cc_blocks(n, kB, (unsigned)ctx->sm_count * 8);
+    CC_KLAUNCH(ctx, CCK_DIST_REPS, k_reps, sb, kB, 0, st, label, n, rep_list, counters + 1, cur,
+               hook);
+    uint64_t *keys = nullptr, *alt = nullptr;
+    CC_TRY(cc_bufs_get(&B, (void **)&keys, (size_t)(m ? m : 1) * sizeof(uint64_t)));
+    EmitParams E;
+    E.row_ptr = d_row_ptr;
+    E.col = d_col;
+    E.label = label;
+    E.bounds = bounds;
+    E.n = n;
+    E.m = m;
+    E.parts = P;
+    E.rb = rb;
+    E.gb = gb;
+    E.out = keys;
+    E.count = counters;
+    E.heavy_deg = 16384;
+    E.heavy_cap = (uint32_t)(m / E.heavy_deg + 1);
+    CC_TRY(cc_bufs_get(&B, (void **)&E.heavy_list, (size_t)E.heavy_cap * sizeof(uint32_t)));
+    CC_TRY(cc_bufs_get(&B, (void **)&E.heavy_count, 256));
+    CC_CUDA(cudaMemsetAsync(E.heavy_count, 0, sizeof(uint32_t), st));
+    if (P > 1) {
+        const unsigned eb = (unsigned)ctx->sm_count * 4;
+        CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit, eb, kB, 0, st, E);
+        CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit_heavy, eb, kB, 0, st, E);
+    }
+    unsigned long long hc[2];
+    CC_CUDA(cudaMemcpyAsync(hc, counters, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                            st));
+    CC_CUDA(cudaStreamSynchronize(st));
+    const uint64_t R = hc[0];
+    S.boundary_raw = R;
+    S.rep_count = hc[1];
+    CC_TRY(clock_mark(clk, st)); /* 3 */
+
+    /* 4. sort */
+    uint64_t *sorted = keys;
+    if (R > 1) {
+        CC_TRY(cc_bufs_get(&B, (void **)&alt, (size_t)R * sizeof(uint64_t)));
+        CC_TRY(cc_radix_sort_u64(ctx, keys, alt, R, rb + gb + pb, &sorted, &S.sort_passes, &B,
+                                 st));
+    }
+    CC_TRY(clock_mark(clk, st)); /* 4 */
+
+    /* 5. dedup, ghosts, plan */
+    DedupParams D;
+    memset(&D, 0, sizeof(D));
+    D.keys = sorted;
+    D.count = R;
+    D.rb = rb;
+    D.gb = gb;
+    D.bounds = bounds;
+    D.parts = P;
+    uint64_t U = 0, G = 0;
+    std::vector<unsigned long long> gcount(P, 0);
+    const uint64_t T = (R + kDedupTile - 1) / kDedupTile;
+    uint64_t *gh_off = nullptr, *segs = nullptr;
+    CC_TRY(cc_bufs_get(&B, (void **)&gh_off, (P + 1) * sizeof(uint64_t)));
+    CC_TRY(cc_bufs_get(&B, (void **)&segs, (size_t)P * (P + 1) * sizeof(uint64_t)));
+    CC_TRY(cc_bufs_get(&B, (void **)&D.gcount, P * sizeof(unsigned long long)));
+    CC_CUDA(cudaMemsetAsync(D.gcount, 0, P * sizeof(unsigned long long), st));
+    if (R > 0) {
+        uint64_t *u_off = nullptr, *g_off = nullptr;
+        CC_TRY(cc_bufs_get(&B, (void **)&D.tile_u, T * sizeof(uint32_t)));
+        CC_TRY(cc_bufs_get(&B, (void **)&D.tile_g, T * sizeof(uint32_t)));
+        CC_TRY(cc_bufs_get(&B, (void **)&u_off, (T + 1) * sizeof(uint64_t)));
+        CC_TRY(cc_bufs_get(&B, (void **)&g_off, (T + 1) * sizeof(uint64_t)));
+        CC_KLAUNCH(ctx, CCK_DIST_DEDUP, k_dedup_count, (unsigned)T, kB, 0, st, D);
+        CC_TRY(cc_scan_u32(ctx, D.tile_u, u_off, T, &B, st));
+        CC_TRY(cc_scan_u32(ctx, D.tile_g, g_off, T, &B, st));
+        uint64_t tot[2];
+        CC_CUDA(cudaMemcpyAsync(&tot[0], u_off + T, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+        CC_CUDA(cudaMemcpyAsync(&tot[1], g_off + T, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+        CC_CUDA(cudaStreamSynchronize(st));
+        U = tot[0];
+        G = tot[1];
+        D.u_off = u_off;
+        D.g_off = g_off;
+    }
+    S.pair_count = U;
+    S.ghost_count = G;
+    CC_TRY(cc_bufs_get(&B, (void **)&D.pair_rep, (size_t)(U ? U : 1) * sizeof(uint32_t)));
+    CC_TRY(cc_bufs_get(&B, (void **)&D.pair_g, (size_t)(U ? U : 1) * sizeof(uint32_t)));
+    CC_TRY(cc_bufs_get(&B, (void **)&D.ghost_v, (size_t)(G ? G : 1) * sizeof(uint32_t)));
+    CC_TRY(cc_bufs_get(&B, (void **)&D.ghost_pairs, (size_t)(G + 1) * sizeof(uint64_t)));
+    CC_TRY(cc_bufs_get(&B, (void **)&D.ghost_labels, (size_t)(G ? G : 1) * sizeof(uint32_t)));
+    CC_TRY(cc_bufs_get(&B, (void **)&D.prev_sent, (size_t)(G ? G : 1) * sizeof(uint32_t)));
+    if (R > 0) {
+        CC_KLAUNCH(ctx, CCK_DIST_GHOSTS, k_dedup_write, (unsigned)T, kB, 0, st, D);
+        CC_CUDA(cudaMemcpyAsync(D.ghost_pairs + G, &U, sizeof(uint64_t), cudaMemcpyHostToDevice,
+                                st));
+    }
+    CC_CUDA(cudaMemcpyAsync(gcount.data(), D.gcount, P * sizeof(unsigned long long),
+                            cudaMemcpyDeviceToHost, st));
+    CC_CUDA(cudaStreamSynchronize(st));
+    std::vector<uint64_t> hoff(P + 1, 0);
+    for (int p = 0; p < P; ++p)
+        hoff[p + 1] = hoff[p] + gcount[p];
+    CC_CUDA(cudaMemcpyAsync(gh_off, hoff.data(), (P + 1) * sizeof(uint64_t),
+                            cudaMemcpyHostToDevice, st));
+    {
+        int tot = P * (P + 1);
+        CC_KLAUNCH(ctx, CCK_DIST_PLAN, k_plan, (tot + kB - 1) / kB, kB, 0, st, D.ghost_v, gh_off,
+                   bounds, P, segs);
+    }
+    CC_TRY(clock_mark(clk, st)); /* 5 */
+    if (o.verbose) {
+        for (int p = 0; p < P; ++p)
+            printf("[part %d] ghost_count=%llu\n", p, (unsigned long long)gcount[p]);
+        printf("[all] boundary_edges raw=%llu dedup=%llu reps=%llu sort_passes=%d\n",
+               (unsigned long long)R, (unsigned long long)U, (unsigned long long)S.rep_count,
+               S.sort_passes);
+    }
+
+    /* 6. merge rounds */
+    MergeParams M;
+    M.label = label;
+    M.bounds = bounds;
+    M.parts = P;
+    M.rep_list = rep_list;
+    M.rep_count = S.rep_count;
+    M.hook = hook;
+    M.pair_rep = D.pair_rep;
+    M.pair_g = D.pair_g;
+    M.pairs = U;
+    M.ghost_v = D.ghost_v;
+    M.ghost_pairs = D.ghost_pairs;
+    M.ghost_labels = D.ghost_labels;
+    M.prev_sent = D.prev_sent;
+    M.ghosts = G;
+    M.gh_off = gh_off;
+    M.seg = segs;
+    M.sent = counters + 3;
+    CC_TRY(cc_bufs_get(&B, (void **)&M.msg, (size_t)(G ? G : 1) * sizeof(uint64_t)));
+    CC_TRY(cc_bufs_get(&B, (void **)&M.msg_count, (size_t)P * P * sizeof(uint32_t)));
+    CC_TRY(cc_bufs_get(&B, (void **)&M.changed, P * sizeof(int)));
+    CC_CUDA(cudaMemsetAsync(M.msg_count, 0, (size_t)P * P * sizeof(uint32_t), st));
+    const unsigned gbk = (unsigned)ctx->sm_count * 8;
+    if (U > 0) {
+        M.cur = cur;
+        M.next = nxt;
+        CC_KLAUNCH(ctx, CCK_MERGE_HOOK, k_hook_init, cc_blocks(U, kB, gbk), kB, 0, st, M);
+    }
+    /* src/cc_mpi.c:538: merge only when some partition has ghosts, pairs
+     * and reps; a partition with none joins the rounds and exchanges
+     * without effect (the reference would stall there). */
+    std::vector<int> pending(P, 0), changed(P, 0);
+    int global_pending = (G > 0 && U > 0 && S.rep_count > 0) ? 1 : 0;
+    for (int p = 0; p < P; ++p)
+        pending[p] = global_pending;
+    int steps = 0;
+    uint32_t *pc = cur, *pn = nxt;
+    while (global_pending) {
+        M.cur = pc;
+        M.next = pn;
+        CC_CUDA(cudaMemsetAsync(M.changed, 0, P * sizeof(int), st));
+        CC_KLAUNCH(ctx, CCK_MERGE_UPD, k_upd, cc_blocks(S.rep_count, kB, gbk), kB, 0, st, M);
+        CC_CUDA(cudaMemcpyAsync(changed.data(), M.changed, P * sizeof(int),
+                                cudaMemcpyDeviceToHost, st));
+        CC_CUDA(cudaStreamSynchronize(st));
+        uint32_t *t = pc;
+        pc = pn;
+        pn = t;
+        int any_changed = 0;
+        global_pending = 0;
+        for (int p = 0; p < P; ++p) {
+            if (changed[p])
+                pending[p] = 1;
+            any_changed |= changed[p];
+            global_pending |= pending[p];
+        }
+        S.rounds++;
+        if (o.verbose && (S.rounds <= 3 || S.rounds % 10 == 0))
+            printf("[all] iter=%d pending=%d changed=%d\n", S.rounds, global_pending,
+                   any_changed);
+        if (!global_pending)
+            break;
+        steps++;
+        if (steps >= interval || !any_changed) {
+            M.cur = pc;
+            CC_KLAUNCH(ctx, CCK_MERGE_EXCH_PACK, k_pack, cc_blocks(G, kB, gbk), kB, 0, st, M);
+            CC_KLAUNCH(ctx, CCK_MERGE_EXCH_SCATTER, k_scatter, cc_blocks(G, kB, gbk), kB, 0, st,
+                       M);
+            CC_CUDA(cudaMemsetAsync(M.msg_count, 0, (size_t)P * P * sizeof(uint32_t), st));
+            S.exchanges++;
+            for (int p = 0; p < P; ++p)
+                pending[p] = 0;
+            steps = 0;
+        }
+    }
+    CC_TRY(clock_mark(clk, st)); /* 6 */
+
+    /* 7. labels and roots */
+    CC_KLAUNCH(ctx, CCK_DIST_LABELS, k_final, sb, kB, 0, st, label, pc, n, d_labels, counters + 2);
+    unsigned long long hr[2];
+    CC_CUDA(cudaMemcpyAsync(hr, counters + 2, 2 * sizeof(unsigned long long),
+                            cudaMemcpyDeviceToHost, st));
+    CC_TRY(clock_mark(clk, st)); /* 7 */
+    CC_CUDA(cudaStreamSynchronize(st));
+    S.roots = hr[0];
+    S.sent_pairs = hr[1];
+    if (clk.on) {
+        float t[7] = {0};
+        for (int i = 0; i < 7; ++i)
+            CC_CUDA(cudaEventElapsedTime(&t[i], clk.ev[i], clk.ev[i + 1]));
+        S.ms_bounds = t[0];
+        S.ms_local = t[1];
+        S.ms_pairs = t[2];
+        S.ms_sort = t[3];
+        S.ms_ghosts = t[4];
+        S.ms_merge = t[5];
+        float tot = 0;
+        CC_CUDA(cudaEventElapsedTime(&tot, clk.ev[0], clk.ev[7]));
+        S.ms_total = tot;
+    }
+    if (o.verbose) {
+        printf("CC merge converged in %d rounds\n", S.rounds);
+        printf("Number of connected components: %llu\n", (unsigned long long)S.roots);
+    }
+    if (st_out)
+        *st_out = S;
+    return CCGPU_OK;
+}
+
+extern "C" int ccgpu_dist_cc(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d_col_idx,
+                             uint32_t n, uint64_t m, const ccgpu_dist_opts *opts,
+                             uint32_t *d_labels, uint32_t *h_bounds, ccgpu_dist_stats *stats,
+                             void *stream)
+{
+    ccgpu_dist_opts o;
+    ccgpu_dist_opts_default(&o);
+    if (opts)
+        o = *opts;
+    if (stats)
+        memset(stats, 0, sizeof(*stats));
+    if (o.parts < 1 || o.parts > CCGPU_MAX_PARTS)
+        return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_dist_cc: parts %d outside [1, %d]",
+                               o.parts, CCGPU_MAX_PARTS);
+    if (n == 0)
+        return CCGPU_OK;
+    if (!d_row_ptr || (m && !d_col_idx))
+        return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_dist_cc: NULL row_ptr/col_idx");
+    if ((uint32_t)o.parts > n)
+        return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_dist_cc: %d parts > %u vertices",
+                               o.parts, n);
+    if (n == 0xffffffffu)
+        return ccgpu_set_error(CCGPU_ERR_LIMIT, "ccgpu_dist_cc: n must be below 2^32-1");
+    CC_TRY(ccgpu_ctx_resolve(&ctx));
+    cudaStream_t st = (cudaStream_t)stream;
+    DevBufs B;
+    CC_TRY(cc_bufs_init(&B, st));
+    int rc = dist_run(ctx, d_row_ptr, d_col_idx, n, m, o, d_labels, h_bounds, stats, st, B);
+    if (rc != CCGPU_OK)
+        cudaStreamSynchronize(st);
+    cc_bufs_release(&B);
+    return rc;
+}
+
+/* ----------------------------------------------------- pair sort / dedup */
+
+namespace {
+
+/* {rep, remote} as one little-endian u64 is remote << 32 | rep: the
+ * reference's key.  Compact it to (remote << rb | rep) for the sort and
+ * back afterwards. */
+__global__ void k_pairs_pack(uint64_t *p, uint64_t count, int rb)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {
+        uint64_t x = p[i];
+        p[i] = ((x >> 32) << rb) | (x & 0xffffffffull);
+    }
+}
+
+__global__ void k_pairs_unpack(const uint64_t *src, uint64_t *dst, uint64_t count, int rb)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t rmask = (1ull << rb) - 1ull;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {
+        uint64_t x = src[i];
+        dst[i] = ((x >> rb) << 32) | (x & rmask);
+    }
+}
+
+__global__ void k_flag_new(const uint64_t *p, uint64_t count, uint32_t *flag)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride)
+        flag[i] = (i == 0 || p[i] != p[i - 1]) ? 1u : 0u;
+}
+
+__global__ void k_compact(const uint64_t *src, const uint64_t *pos, uint64_t count, uint64_t *dst)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride)
+        if (pos[i + 1] != pos[i])
+            dst[pos[i]] = src[i];
+}
+
+} // namespace
+
+extern "C" int ccgpu_boundary_sort(ccgpu_ctx *ctx, uint32_t *d_pairs, uint64_t count,
+                                   uint32_t max_rep, uint32_t max_remote, void *stream)
+{
+    if (count <= 1)
+        return CCGPU_OK;
+    if (!d_pairs)
+        return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_boundary_sort: NULL pairs");
+    if (((uintptr_t)d_pairs & 7) != 0)
+        return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_boundary_sort: pairs not 8-byte aligned");
+    CC_TRY(ccgpu_ctx_resolve(&ctx));
+    cudaStream_t st = (cudaStream_t)stream;
+    const int rb = bits_for(max_rep), gb = bits_for(max_remote);
+    uint64_t *p = (uint64_t *)d_pairs;
+    DevBufs B;
+    CC_TRY(cc_bufs_init(&B, st));
+    int rc = CCGPU_OK;
+    do {
+        uint64_t *alt = nullptr, *sorted = nullptr;
+        if ((rc = cc_bufs_get(&B, (void **)&alt, count * sizeof(uint64_t))) != CCGPU_OK)
+            break;
+        const unsigned blocks = cc_blocks(count, 256, (unsigned)ctx->sm_count * 8);
+        k_pairs_pack<<<blocks, 256, 0, st>>>(p, count, rb);
+        ctx->launches++;
+        if ((rc = cc_radix_sort_u64(ctx, p, alt, count, rb + gb, &sorted, nullptr, &B, st)) !=
+            CCGPU_OK)
+            break;
+        k_pairs_unpack<<<blocks, 256, 0, st>>>(sorted, p, count, rb);
+        ctx->launches++;
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess)
+            e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess)
+            rc = ccgpu_cuda_fail(e, "boundary sort", __FILE__, __LINE__);
+    } while (0);
+    cc_bufs_release(&B);
+    return rc;
+}
+
+extern "C" int ccgpu_boundary_dedup(ccgpu_ctx *ctx, uint32_t *d_pairs, uint64_t count,
+                                    uint64_t *new_count, void *stream)
+{
+    if (!new_count)
+        return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_boundary_dedup: new_count is NULL");
+    *new_count = count;
+    if (count <= 1)
+        return CCGPU_OK;
+    if (!d_pairs)
+        return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_boundary_dedup: NULL pairs");
+    CC_TRY(ccgpu_ctx_resolve(&ctx));
+    cudaStream_t st = (cudaStream_t)stream;
+    uint64_t *p = (uint64_t *)d_pairs;
+    DevBufs B;
+    CC_TRY(cc_bufs_init(&B, st));
+    int rc = CCGPU_OK;
+    do {
+        uint32_t *flag = nullptr;
+        uint64_t *pos = nullptr, *tmp = nullptr;
+        if ((rc = cc_bufs_get(&B, (void **)&flag, count * sizeof(uint32_t))) != CCGPU_OK ||
+            (rc = cc_bufs_get(&B, (void **)&pos, (count + 1) * sizeof(uint64_t))) != CCGPU_OK ||
+            (rc = cc_bufs_get(&B, (void **)&tmp, count * sizeof(uint64_t))) != CCGPU_OK)
+            break;
+        const unsigned blocks = cc_blocks(count, 256, (unsigned)ctx->sm_count * 8);
+        k_flag_new<<<blocks, 256, 0, st>>>(p, count, flag);
+        ctx->launches++;
+        if ((rc = cc_scan_u32(ctx, flag, pos, count, &B, st)) != CCGPU_OK)
+            break;
+        k_compact<<<blocks, 256, 0, st>>>(p, pos, count, tmp);
+        ctx->launches++;
+        uint64_t kept = 0;
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(&kept, pos + count, sizeof(uint64_t), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess)
+            e = cudaStreamSynchronize(st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(p, tmp, kept * sizeof(uint64_t), cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess)
+            e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) {
+            rc = ccgpu_cuda_fail(e, "boundary dedup", __FILE__, __LINE__);
+            break;
+        }
+        *new_count = kept;
+    } while (0);
+    cc_bufs_release(&B);
+    return rc;
+}

@@ -78,11 +78,31 @@ __device__ __forceinline__ uint32_t seg_of(const uint64_t *__restrict__ seg, uin
     return lo;
 }
 
+/* [lo, hi) of v's segment when edges are filtered to segments, else [0, n). */
+struct Span {
+    uint32_t lo, hi;
+};
+
+__device__ __forceinline__ Span span_of(const uint64_t *__restrict__ fseg, uint32_t nseg,
+                                        uint32_t n, uint64_t v)
+{
+    if (!fseg)
+        return {0u, n};
+    uint32_t s = seg_of(fseg, nseg, v);
+    return {(uint32_t)__ldg(fseg + s), (uint32_t)__ldg(fseg + s + 1)};
+}
+
+__device__ __forceinline__ bool in_span(Span sp, uint32_t u)
+{
+    return u >= sp.lo && u < sp.hi;
+}
+
 __global__ void __launch_bounds__(kBlock) k_init(uint32_t *__restrict__ parent, uint32_t n,
                                                  LocalCCCounters *counters, int vec,
                                                  const uint64_t *__restrict__ row_ptr,
                                                  const uint32_t *__restrict__ col, uint64_t m,
-                                                 int first_hook)
+                                                 int first_hook, const uint64_t *__restrict__ fseg,
+                                                 uint32_t nseg)
 {
     const uint64_t stride = (uint64_t)gridDim.x * kBlock;
     const uint64_t tid = (uint64_t)blockIdx.x * kBlock + threadIdx.x;
@@ -96,7 +116,7 @@ __global__ void __launch_bounds__(kBlock) k_init(uint32_t *__restrict__ parent, 
             uint32_t p = (uint32_t)v;
             if (r.beg < r.end) {
                 uint32_t u = __ldg(col + r.beg);
-                if (u < p)
+                if (u < p && in_span(span_of(fseg, nseg, n, v), u))
                     p = u;
             }
             parent[v] = p;
@@ -123,18 +143,20 @@ template <bool LAZY>
 __global__ void __launch_bounds__(kBlock) k_sample(const uint64_t *__restrict__ row_ptr,
                                                    const uint32_t *__restrict__ col, uint32_t n,
                                                    uint64_t m, uint32_t *parent, uint32_t v_lo,
-                                                   uint32_t v_hi, int r0, int r1, int first_done)
+                                                   uint32_t v_hi, int r0, int r1, int first_done,
+                                                   const uint64_t *__restrict__ fseg, uint32_t nseg)
 {
     const uint64_t stride = (uint64_t)gridDim.x * kBlock;
     for (uint64_t v = (uint64_t)v_lo + (uint64_t)blockIdx.x * kBlock + threadIdx.x; v < v_hi;
          v += stride) {
         Rows r = row_of(row_ptr, (uint32_t)v, m);
+        const Span sp = span_of(fseg, nseg, n, v);
         for (int k = r0; k < r1; ++k) {
             uint64_t j = r.beg + (uint64_t)k;
             if (j >= r.end)
                 break;
             uint32_t u = __ldg(col + j);
-            if (u >= n || (k == 0 && first_done && u < (uint32_t)v))
+            if (!in_span(sp, u) || (k == 0 && first_done && u < (uint32_t)v))
                 continue;
             cc_union<LAZY>(parent, (uint32_t)v, u);
         }
@@ -233,13 +255,14 @@ struct LinkParams {
     uint32_t heavy_cap;
     uint32_t heavy_deg;
     int vec;                   /* col is 16-byte aligned                    */
+    const uint64_t *fseg;      /* segment filter offsets, NULL = off        */
 };
 
-/* One warp links v with row entries [beg, end): 16-byte column loads for
- * the aligned body, scalar head and tail. */
+/* One warp links v with row entries [beg, end) that fall in sp: 16-byte
+ * column loads for the aligned body, scalar head and tail. */
 template <bool LAZY>
 __device__ __forceinline__ void warp_link_row(const LinkParams &P, uint32_t v, uint64_t beg,
-                                              uint64_t end, int lane)
+                                              uint64_t end, int lane, Span sp)
 {
     uint64_t body_end = beg;
     if (P.vec) {
@@ -251,35 +274,36 @@ __device__ __forceinline__ void warp_link_row(const LinkParams &P, uint32_t v, u
             body_end = a;
         if (beg + lane < a) {
             uint32_t u = __ldg(P.col + beg + lane);
-            if (u < P.n)
+            if (in_span(sp, u))
                 cc_union<LAZY>(P.parent, v, u);
         }
         const uint4 *c4 = reinterpret_cast<const uint4 *>(P.col);
         for (uint64_t q = a / 4 + lane; q < body_end / 4; q += 32) {
             uint4 x = __ldg(c4 + q);
-            if (x.x < P.n)
+            if (in_span(sp, x.x))
                 cc_union<LAZY>(P.parent, v, x.x);
-            if (x.y < P.n)
+            if (in_span(sp, x.y))
                 cc_union<LAZY>(P.parent, v, x.y);
-            if (x.z < P.n)
+            if (in_span(sp, x.z))
                 cc_union<LAZY>(P.parent, v, x.z);
-            if (x.w < P.n)
+            if (in_span(sp, x.w))
                 cc_union<LAZY>(P.parent, v, x.w);
         }
     }
     for (uint64_t j = body_end + lane; j < end; j += 32) {
         uint32_t u = __ldg(P.col + j);
-        if (u < P.n)
+        if (in_span(sp, u))
             cc_union<LAZY>(P.parent, v, u);
     }
 }
 
 template <bool LAZY>
-__global__ void __launch_bounds__(kBlock) k_link_rows(LinkParams P)
+__global__ void __launch_bounds__(kBlock, 4) k_link_rows(LinkParams P)
 {
     __shared__ uint32_t s_off[kBlock + 1];
     __shared__ uint64_t s_beg[kBlock];
     __shared__ uint32_t s_wsum[kWarps];
+    __shared__ Span s_span[kBlock];
     __shared__ unsigned long long s_base;
 
     const uint32_t giant0 = (P.giants && P.nseg == 1) ? P.giants[0] : kNoGiant;
@@ -322,6 +346,7 @@ __global__ void __launch_bounds__(kBlock) k_link_rows(LinkParams P)
             const uint64_t v64 = t0 + threadIdx.x;
             const uint32_t v = (uint32_t)v64;
             uint64_t beg = 0, end = 0;
+            const Span sp = span_of(P.fseg, P.nseg, P.n, v64 < cend ? v64 : t0);
             if (v64 < cend) {
                 uint32_t giant = giant0;
                 if (P.giants && P.nseg > 1)
@@ -352,7 +377,9 @@ __global__ void __launch_bounds__(kBlock) k_link_rows(LinkParams P)
                 uint32_t vv = __shfl_sync(0xffffffffu, v, src);
                 uint64_t bb = __shfl_sync(0xffffffffu, beg, src);
                 uint64_t ee = __shfl_sync(0xffffffffu, end, src);
-                warp_link_row<LAZY>(P, vv, bb, ee, lane);
+                Span ss = {__shfl_sync(0xffffffffu, sp.lo, src),
+                           __shfl_sync(0xffffffffu, sp.hi, src)};
+                warp_link_row<LAZY>(P, vv, bb, ee, lane, ss);
             }
             /* short rows: CTA-wide gather, walked edge-parallel */
             uint32_t small = deg < 32 ? (uint32_t)deg : 0u;
@@ -365,6 +392,7 @@ __global__ void __launch_bounds__(kBlock) k_link_rows(LinkParams P)
             if (lane == 31)
                 s_wsum[warp] = incl;
             s_beg[threadIdx.x] = beg;
+            s_span[threadIdx.x] = sp;
             __syncthreads();
             uint32_t wpre = 0, total = 0;
 #pragma unroll
@@ -388,7 +416,7 @@ __global__ void __launch_bounds__(kBlock) k_link_rows(LinkParams P)
                 }
                 uint64_t j = s_beg[lo] + (e - s_off[lo]);
                 uint32_t u = __ldg(P.col + j);
-                if (u < P.n)
+                if (in_span(s_span[lo], u))
                     cc_union<LAZY>(P.parent, (uint32_t)(t0 + lo), u);
             }
             __syncthreads();
@@ -414,6 +442,7 @@ __global__ void __launch_bounds__(kBlock) k_link_heavy(LinkParams P)
     for (uint32_t h = 0; h < cnt; ++h) {
         uint32_t v = P.heavy_list[h];
         Rows r = row_of(P.row_ptr, v, P.m);
+        const Span sp = span_of(P.fseg, P.nseg, P.n, v);
         uint64_t beg = r.beg + P.skip_from;
         if (beg > r.end)
             beg = r.end;
@@ -423,7 +452,7 @@ __global__ void __launch_bounds__(kBlock) k_link_heavy(LinkParams P)
             uint64_t se = sb + kHeavySeg < r.end ? sb + kHeavySeg : r.end;
             for (uint64_t j = sb + threadIdx.x; j < se; j += kBlock) {
                 uint32_t u = __ldg(P.col + j);
-                if (u < P.n)
+                if (in_span(sp, u))
                     cc_union<LAZY>(P.parent, v, u);
             }
         }
@@ -496,8 +525,9 @@ int launch_sample(ccgpu_ctx *ctx, const LocalCCArgs &a, uint32_t vlo, uint32_t v
                   int r1, cudaStream_t st, unsigned blocks)
 {
     const int first_done = (a.o.hook_mode & CCGPU_HOOK_FIRST) != 0;
+    const uint64_t *fseg = a.seg_filter ? a.seg : nullptr;
     CC_KLAUNCH(ctx, CCK_SAMPLE, k_sample<LAZY>, blocks, kBlock, 0, st, a.row_ptr, a.col, a.n,
-               a.m, a.labels, vlo, vhi, r0, r1, first_done);
+               a.m, a.labels, vlo, vhi, r0, r1, first_done, fseg, a.nseg);
     return CCGPU_OK;
 }
 
@@ -557,7 +587,8 @@ int cc_local_init(ccgpu_ctx *ctx, const LocalCCArgs &a, const LocalCCScratch &s,
     const unsigned sb = cc_blocks(a.n, kBlock, g.stream_blocks);
     const int first = (a.o.hook_mode & CCGPU_HOOK_FIRST) && a.o.sample_rounds > 0;
     CC_KLAUNCH(ctx, CCK_INIT, k_init, sb, kBlock, 0, st, a.labels, a.n, s.counters,
-               ((uintptr_t)a.labels & 15) == 0, a.row_ptr, a.col, a.m, first);
+               ((uintptr_t)a.labels & 15) == 0, a.row_ptr, a.col, a.m, first,
+               a.seg_filter ? a.seg : (const uint64_t *)nullptr, a.nseg);
     return CCGPU_OK;
 }
 
@@ -627,6 +658,7 @@ int cc_local_run(ccgpu_ctx *ctx, const LocalCCArgs &a, const LocalCCScratch &s, 
     P.heavy_cap = s.heavy_cap;
     P.heavy_deg = (uint32_t)a.o.heavy_degree;
     P.vec = ((uintptr_t)a.col & 15) == 0;
+    P.fseg = a.seg_filter ? a.seg : nullptr;
     if (lazy)
         CC_TRY(launch_finish<true>(ctx, P, g, st));
     else

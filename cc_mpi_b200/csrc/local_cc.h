@@ -22,6 +22,10 @@ struct LocalCCArgs {
     const uint64_t *seg;      /* [nseg+1] segment vertex offsets or NULL */
     uint32_t nseg;            /* 1 when seg is NULL                      */
     ccgpu_cc_opts o;          /* resolved options                        */
+    int seg_filter;           /* 1: ignore edges whose endpoints lie in
+                               * different segments (the local subgraph
+                               * of each partition, reference
+                               * src/cc_mpi.c:252-297)                  */
 };
 
 /* Device counters a solve leaves behind (for stats). */

@@ -145,6 +145,76 @@ int ccgpu_local_cc_host(ccgpu_ctx *ctx, const uint64_t *h_row_ptr, const uint32_
                         uint32_t n, uint64_t m, uint32_t *h_labels,
                         const ccgpu_cc_opts *opts, ccgpu_cc_stats *stats);
 
+/* ------------------------------------------------------------------------
+ * Partitioned CC (the kernels behind compute_connected_components_mpi_
+ * advanced, reference include/cc_mpi.h:29-33 and src/cc_mpi.c:221-763).
+ *
+ * The graph is cut into `parts` contiguous vertex ranges exactly as the
+ * reference cuts it over MPI ranks (src/graph_dist.c:22-92), and every range
+ * stays resident in HBM:
+ *   1. bounds   edge+vertex weighted cuts (or block ranges) on the device
+ *   2. local    union-find CC of each range's local subgraph
+ *   3. pairs    (rep, remote) for every cut edge, packed as sort keys
+ *   4. sort     LSD radix sort of the keys, dedup, ghost ids, plan ranges
+ *   5. merge    rounds of hook + pointer jumps; every `exchange_interval`
+ *               rounds, or when nothing changed, the labels owners changed
+ *               since the last exchange travel as (position, label) pairs
+ *               between the ranges (the reference's delta exchange,
+ *               src/exchange_plan.c:242-425)
+ *   6. labels   labels[v] = min vertex id of v's component
+ * The round and exchange schedule is the reference's (src/cc_mpi.c:535-710);
+ * each round reads the previous round's labels, so the round count is
+ * deterministic.
+ * ---------------------------------------------------------------------- */
+#define CCGPU_MAX_PARTS 256
+
+typedef struct {
+    int parts;              /* number of partitions (the reference's -np)   */
+    int use_edge;           /* 1: edge-balanced bounds (the reference's
+                             * benchmark), 0: block vertex ranges           */
+    int chunk_size;         /* passed to the local CC as in the reference   */
+    int exchange_interval;  /* merge rounds between exchanges (< 1 = 1)     */
+    int verbose;            /* 1: print the reference's phase lines         */
+} ccgpu_dist_opts;
+
+typedef struct {
+    int rounds;             /* merge rounds ("CC merge converged in N")     */
+    int exchanges;          /* delta exchanges performed                    */
+    int sort_passes;        /* radix passes over the boundary keys          */
+    int pad;
+    uint64_t boundary_raw;  /* cut edges (before dedup), all partitions     */
+    uint64_t pair_count;    /* distinct (rep, remote) pairs                 */
+    uint64_t ghost_count;   /* distinct remote vertices, summed             */
+    uint64_t rep_count;     /* local components, summed                     */
+    uint64_t roots;         /* components of the whole graph                */
+    uint64_t sent_pairs;    /* (position, label) pairs moved in exchanges   */
+    double ms_bounds, ms_local, ms_pairs, ms_sort, ms_ghosts, ms_merge, ms_total;
+} ccgpu_dist_stats;
+
+void ccgpu_dist_opts_default(ccgpu_dist_opts *opts);
+
+/* d_labels (may be NULL) receives the labels; h_bounds (may be NULL,
+ * parts+1 entries) the partition bounds.  Synchronous (the merge loop reads
+ * two flags per round).  Needs n >= parts. */
+int ccgpu_dist_cc(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d_col_idx,
+                  uint32_t n, uint64_t m, const ccgpu_dist_opts *opts, uint32_t *d_labels,
+                  uint32_t *h_bounds, ccgpu_dist_stats *stats, void *stream);
+
+/* Partition bounds only (step 1), into h_bounds[parts+1]. */
+int ccgpu_partition_bounds(const uint64_t *d_row_ptr, uint32_t n, int parts, int use_edge,
+                           uint32_t *h_bounds, void *stream);
+
+/* Sorts d_pairs[0..count) in place, ascending on (remote << 32 | rep) - the
+ * reference's boundary edge order (src/boundary_sort.c:5-8,93-98) - where
+ * each pair is {uint32 rep, uint32 remote}.  max_rep / max_remote bound the
+ * values (UINT32_MAX if unknown) so that only the needed digits are sorted. */
+int ccgpu_boundary_sort(ccgpu_ctx *ctx, uint32_t *d_pairs, uint64_t count, uint32_t max_rep,
+                        uint32_t max_remote, void *stream);
+/* Removes adjacent duplicates of a sorted pair array in place
+ * (src/boundary_sort.c:100-119); *new_count receives the kept count. */
+int ccgpu_boundary_dedup(ccgpu_ctx *ctx, uint32_t *d_pairs, uint64_t count, uint64_t *new_count,
+                         void *stream);
+
 /* Number of v with d_labels[v] == v (one root per component when the labels
  * are min-id labels).  Synchronous; result in *count. */
 int ccgpu_count_roots(ccgpu_ctx *ctx, const uint32_t *d_labels, uint32_t n,

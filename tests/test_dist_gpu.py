@@ -1,0 +1,150 @@
+"""Parity of the partitioned path (ccgpu_dist_cc and the boundary sort) with
+the oracle's restatement of the reference's distributed algorithm: labels
+bit-exact, and - because both use the same round semantics - the same
+round, exchange, pair, ghost and rep counts and the same bounds."""
+import numpy as np
+import pytest
+
+import oracle
+from cc_mpi_b200 import dist, graphs
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as t
+    t.cuda.set_device(0)
+    return t
+
+
+def dev(torch, rp, col):
+    d_rp = torch.from_numpy(rp.astype(np.int64)).cuda()
+    d_col = torch.from_numpy(col.astype(np.int32)).cuda() if len(col) else \
+        torch.zeros(1, dtype=torch.int32, device="cuda")
+    return d_rp, d_col
+
+
+def run(torch, rp, col, parts, kind, interval, chunk=2048):
+    n = len(rp) - 1
+    d_rp, d_col = dev(torch, rp, col)
+    lab = torch.empty(max(n, 1), dtype=torch.int32, device="cuda")
+    st, bounds = dist.dist_cc_device(d_rp, d_col, n, int(rp[-1]), parts, kind, chunk, interval,
+                                     d_labels=lab)
+    torch.cuda.synchronize()
+    return lab[:n].cpu().numpy().view(np.uint32), st, bounds
+
+
+def check_against_oracle(torch, rp, col, parts, kind, interval, chunk=2048):
+    got, st, bounds = run(torch, rp, col, parts, kind, interval, chunk)
+    want, obounds, ost = oracle.dist_cc(rp, col, parts, kind, interval)
+    assert (got == want).all()
+    assert (bounds == obounds).all()
+    assert st.roots == ost.roots
+    assert st.boundary_raw == ost.boundary_raw
+    assert st.pair_count == ost.pair_count
+    assert st.ghost_count == ost.ghost_count
+    assert st.rep_count == ost.rep_count
+    assert st.rounds == ost.rounds, (st.rounds, ost.rounds)
+    assert st.exchanges == ost.exchanges
+    assert st.sent_pairs == ost.sent_pairs
+    return st
+
+
+@pytest.mark.parametrize("parts", [1, 2, 3, 4, 7])
+@pytest.mark.parametrize("kind", [0, 1])
+def test_small_cases(torch, small_cases, parts, kind):
+    for name, (rp, col) in small_cases.items():
+        if len(rp) - 1 < parts:
+            continue
+        for interval in (1, 2, 4):
+            check_against_oracle(torch, rp, col, parts, kind, interval)
+
+
+def test_golden_graphs(torch, golden_labels):
+    for name, (rp, col, ref) in golden_labels.items():
+        if len(rp) - 1 < 4:
+            continue
+        got, st, _ = run(torch, rp, col, 4, 1, 1)
+        assert (got == ref).all(), name
+
+
+@pytest.mark.parametrize("chunk", [1, 2048, 8192, 32768])
+@pytest.mark.parametrize("interval", [1, 2, 4])
+def test_rmat_chunks_and_intervals(torch, chunk, interval):
+    rp, col = graphs.rmat_csr(14, 16, seed=31)
+    st = check_against_oracle(torch, rp, col, 4, 1, interval, chunk)
+    assert st.rounds >= 1
+
+
+def test_grid_partitions(torch):
+    rp, col = graphs.grid_csr(256, 256, 0.1, seed=9)
+    for parts in (2, 4, 8):
+        check_against_oracle(torch, rp, col, parts, 1, 2)
+
+
+def test_many_partitions_and_er(torch):
+    rp, col = graphs.er_csr(30000, 3.0, seed=4)
+    for parts in (16, 64):
+        check_against_oracle(torch, rp, col, parts, 1, 1)
+        check_against_oracle(torch, rp, col, parts, 0, 3)
+
+
+def test_bounds_match_reference_restatement(torch):
+    rp, col = graphs.rmat_csr(12, 8, seed=6)
+    d_rp, _ = dev(torch, rp, col)
+    for parts in (1, 2, 3, 5, 16):
+        for kind in (0, 1):
+            got = dist.partition_bounds_device(d_rp, len(rp) - 1, parts, kind)
+            if kind and parts > 1:
+                want = oracle.weighted_bounds(rp, parts)
+            else:
+                want = np.array([oracle.vertex_range(len(rp) - 1, parts, r)[0]
+                                 for r in range(parts)] + [len(rp) - 1], dtype=np.uint32)
+            assert (got == want).all(), (parts, kind)
+
+
+def test_large_rmat_properties(torch):
+    rp_d, col_d = graphs.rmat_csr_torch(torch, 20, 16, seed=5)
+    n, m = rp_d.numel() - 1, col_d.numel()
+    lab = torch.empty(n, dtype=torch.int32, device="cuda")
+    st, bounds = dist.dist_cc_device(rp_d, col_d, n, m, 4, 1, 8192, 2, d_labels=lab)
+    rp = rp_d.cpu().numpy().view(np.uint64)
+    col = col_d.cpu().numpy().view(np.uint32)
+    uf = oracle.uf_labels(rp, col)
+    assert (lab.cpu().numpy().view(np.uint32) == uf).all()
+    assert st.roots == oracle.count_components(uf)
+
+
+def test_boundary_sort_golden(torch):
+    import os
+    from conftest import GOLDEN
+    d = np.load(os.path.join(GOLDEN, "boundary_sort.npz"))
+    for name in d["names"]:
+        name = str(name)
+        inp = d[f"{name}__in"]
+        exp = d[f"{name}__out"]
+        if len(inp) == 0:
+            continue
+        t = torch.from_numpy(inp.view(np.int64).copy()).cuda()
+        dist.boundary_sort_device(t, len(inp))
+        k = dist.boundary_dedup_device(t, len(inp))
+        torch.cuda.synchronize()
+        got = t[:k].cpu().numpy().view(np.uint64)
+        assert k == len(exp), name
+        assert (got == exp).all(), name
+
+
+def test_boundary_sort_random_bits(torch):
+    rng = np.random.default_rng(3)
+    for n, rb, gb in [(100000, 20, 24), (70000, 32, 32), (5, 3, 3), (4097, 12, 1)]:
+        pairs = np.empty(n, dtype=oracle.PAIR_DTYPE)
+        pairs["rep"] = rng.integers(0, 1 << rb, n, dtype=np.uint64)
+        pairs["remote"] = rng.integers(0, 1 << gb, n, dtype=np.uint64)
+        want = oracle.boundary_sort_dedup(pairs)
+        t = torch.from_numpy(pairs.view(np.int64).copy()).cuda()
+        dist.boundary_sort_device(t, n, (1 << rb) - 1, (1 << gb) - 1)
+        k = dist.boundary_dedup_device(t, n)
+        torch.cuda.synchronize()
+        assert k == len(want)
+        assert (t[:k].cpu().numpy().view(np.uint64) == want.view(np.uint64)).all()
