@@ -870,7 +870,7 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
                    bounds, P, segs);
     }
     CC_TRY(clock_mark(clk, st)); /* 5 */
-    if (o.verbose) {
+    if (o.verbose >= 2) {
         for (int p = 0; p < P; ++p)
             printf("[part %d] ghost_count=%llu\n", p, (unsigned long long)gcount[p]);
         printf("[all] boundary_edges raw=%llu dedup=%llu reps=%llu sort_passes=%d\n",
@@ -936,7 +936,7 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
             global_pending |= pending[p];
         }
         S.rounds++;
-        if (o.verbose && (S.rounds <= 3 || S.rounds % 10 == 0))
+        if (o.verbose >= 2 && (S.rounds <= 3 || S.rounds % 10 == 0))
             printf("[all] iter=%d pending=%d changed=%d\n", S.rounds, global_pending,
                    any_changed);
         if (!global_pending)
@@ -979,9 +979,15 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
         CC_CUDA(cudaEventElapsedTime(&tot, clk.ev[0], clk.ev[7]));
         S.ms_total = tot;
     }
-    if (o.verbose) {
+    if (o.verbose >= 2)
+        printf("[all] phases ms: bounds=%.3f local=%.3f pairs=%.3f sort=%.3f ghosts=%.3f "
+               "merge=%.3f total=%.3f\n",
+               S.ms_bounds, S.ms_local, S.ms_pairs, S.ms_sort, S.ms_ghosts, S.ms_merge,
+               S.ms_total);
+    if (o.verbose >= 1) { /* src/cc_mpi.c:712-713,741-742 */
         printf("CC merge converged in %d rounds\n", S.rounds);
         printf("Number of connected components: %llu\n", (unsigned long long)S.roots);
+        fflush(stdout);
     }
     if (st_out)
         *st_out = S;

@@ -22,6 +22,11 @@ int ccb200_set_exit_on_error(int on)
     return prev;
 }
 
+int ccb200_exit_on_error(void)
+{
+    return g_exit_on_error;
+}
+
 void ccb200_fail(const char *where, int status)
 {
     fprintf(stderr, "%s: %s (status %d)\n", where, ccgpu_last_error(), status);

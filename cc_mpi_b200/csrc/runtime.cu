@@ -29,6 +29,16 @@ int ccgpu_set_error(int status, const char *fmt, ...)
     return status;
 }
 
+/* The same, with C linkage, for the host C sources. */
+extern "C" int ccb200_set_error(int status, const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return status;
+}
+
 int ccgpu_cuda_fail(cudaError_t e, const char *what, const char *file, int line)
 {
     const char *base = strrchr(file, '/');

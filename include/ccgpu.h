@@ -78,6 +78,24 @@ int ccgpu_prof_kernels(void);
 const char *ccgpu_prof_name(int kernel_id);
 
 /* ------------------------------------------------------------------------
+ * Device memory and device-resident graphs (used by the host C layer).
+ * ---------------------------------------------------------------------- */
+int ccgpu_alloc(void **d_ptr, size_t bytes);
+void ccgpu_free(void *d_ptr);
+int ccgpu_memcpy_h2d(void *d_dst, const void *h_src, size_t bytes);
+int ccgpu_memcpy_d2h(void *h_dst, const void *d_src, size_t bytes);
+
+/* A CSR copied to HBM once and reused by many solves. */
+typedef struct ccgpu_graph ccgpu_graph;
+int ccgpu_graph_upload(const uint64_t *h_row_ptr, const uint32_t *h_col_idx, uint32_t n,
+                       uint64_t m, ccgpu_graph **out);
+void ccgpu_graph_free(ccgpu_graph *g);
+const uint64_t *ccgpu_graph_row_ptr(const ccgpu_graph *g);
+const uint32_t *ccgpu_graph_col_idx(const ccgpu_graph *g);
+uint32_t ccgpu_graph_n(const ccgpu_graph *g);
+uint64_t ccgpu_graph_m(const ccgpu_graph *g);
+
+/* ------------------------------------------------------------------------
  * Local CC (the kernel behind compute_connected_components_pthreads,
  * include/cc.h:27-28 of the reference).
  *

@@ -163,7 +163,8 @@ def test_profiler_and_launch_counter(torch):
     _lib.check(L.ccgpu_prof_enable(None, 0))
     names = [L.ccgpu_prof_name(i).decode() for i in range(k)]
     got = {names[i]: cnt[i] for i in range(k) if cnt[i]}
-    assert got.get("sample") == 1 and got.get("link_rows") == 1
+    # default schedule: one sampling launch per sampled neighbour (cadence)
+    assert got.get("sample") == 2 and got.get("link_rows") == 1
     assert L.ccgpu_ctx_launches(None) - before == sum(cnt)
 
 
