@@ -233,6 +233,26 @@ int ccgpu_boundary_sort(ccgpu_ctx *ctx, uint32_t *d_pairs, uint64_t count, uint3
 int ccgpu_boundary_dedup(ccgpu_ctx *ctx, uint32_t *d_pairs, uint64_t count, uint64_t *new_count,
                          void *stream);
 
+/* ccgpu_local_cc without any device allocation.  No counterpart in the
+ * reference: it exists for callers that cannot allocate device memory (code
+ * running inside another library's stream capture, where allocation calls
+ * are not capturable; processes whose allocator reserved all of HBM up
+ * front; loops that must not take the device-wide synchronisation of
+ * cudaMalloc/cudaFree).  Scratch lives in a fixed file-scope device array of
+ * ccgpu_local_cc_noalloc_capacity() bytes (1 MiB), held by every GPU that
+ * loads the library until the process exits; a solve needs
+ * ccgpu_local_cc_noalloc_required(n, m, opts) bytes (about 4 bytes per
+ * m/heavy_degree row of the heavy queue) and larger graphs are rejected
+ * with CCGPU_ERR_LIMIT.  The first call on a device looks up the array with
+ * cudaGetSymbolAddress; make it before any stream capture.  Calls share the
+ * array: calls whose kernels overlap on the GPU race.  Asynchronous on
+ * `stream`; no stats. */
+int ccgpu_local_cc_noalloc(const uint64_t *d_row_ptr, const uint32_t *d_col_idx, uint32_t n,
+                           uint64_t m, uint32_t *d_labels, const ccgpu_cc_opts *opts,
+                           void *stream);
+size_t ccgpu_local_cc_noalloc_capacity(void);
+size_t ccgpu_local_cc_noalloc_required(uint32_t n, uint64_t m, const ccgpu_cc_opts *opts);
+
 /* Number of v with d_labels[v] == v (one root per component when the labels
  * are min-id labels).  Synchronous; result in *count. */
 int ccgpu_count_roots(ccgpu_ctx *ctx, const uint32_t *d_labels, uint32_t n,
