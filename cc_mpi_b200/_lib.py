@@ -80,6 +80,11 @@ _SIGS = {
     "ccgpu_local_cc_host": (_INT, [_VP, _VP, _VP, _U32, _U64, _VP, C.POINTER(CCOpts),
                                    C.POINTER(CCStats)]),
     "ccgpu_count_roots": (_INT, [_VP, _VP, _U32, C.POINTER(_U64), _VP]),
+    "ccgpu_local_cc_plan": (_INT, [_VP, _VP, _U32, _U64, _VP, C.POINTER(CCOpts),
+                                   C.POINTER(_VP)]),
+    "ccgpu_plan_launch": (_INT, [_VP, _VP]),
+    "ccgpu_plan_kernels": (_INT, [_VP]),
+    "ccgpu_plan_destroy": (None, [_VP]),
     "ccgpu_check_labels": (_INT, [_VP, _VP, _VP, _U32, _U64, _VP, C.POINTER(_U64), _VP]),
 }
 
@@ -122,5 +127,5 @@ HOOK_FIRST, HOOK_LAZY, HOOK_CADENCE = 1, 2, 4
 
 
 def opts(chunk_size=4096, sample_rounds=2, heavy_degree=8192, skip_giant=1,
-         hook_mode=HOOK_CADENCE):
+         hook_mode=HOOK_CADENCE | 8):
     return CCOpts(chunk_size, sample_rounds, heavy_degree, skip_giant, hook_mode)

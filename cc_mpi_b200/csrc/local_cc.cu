@@ -163,6 +163,39 @@ __global__ void __launch_bounds__(kBlock) k_sample(const uint64_t *__restrict__ 
     }
 }
 
+/* Sampling that only has to leave a valid forest (MINHOOK): the larger of
+ * the two roots is lowered to the smaller with a fire-and-forget atomicMin.
+ * If that root was hooked elsewhere meanwhile, its subtree moves to the new
+ * parent and one earlier link is lost; the forest stays valid (parent < self,
+ * every link inside one component) and the finish pass re-links every row
+ * outside the giant tree from its first entry, which restores anything
+ * lost. */
+__global__ void __launch_bounds__(kBlock) k_sample_min(const uint64_t *__restrict__ row_ptr,
+                                                       const uint32_t *__restrict__ col,
+                                                       uint32_t n, uint64_t m, uint32_t *parent,
+                                                       uint32_t v_lo, uint32_t v_hi, int r0,
+                                                       int r1, const uint64_t *__restrict__ fseg,
+                                                       uint32_t nseg)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * kBlock;
+    for (uint64_t v = (uint64_t)v_lo + (uint64_t)blockIdx.x * kBlock + threadIdx.x; v < v_hi;
+         v += stride) {
+        Rows r = row_of(row_ptr, (uint32_t)v, m);
+        const Span sp = span_of(fseg, nseg, n, v);
+        for (int k = r0; k < r1; ++k) {
+            uint64_t j = r.beg + (uint64_t)k;
+            if (j >= r.end)
+                break;
+            uint32_t u = __ldg(col + j);
+            if (!in_span(sp, u))
+                continue;
+            uint32_t rv = cc_find(parent, (uint32_t)v), ru = cc_find(parent, u);
+            if (rv != ru)
+                atomicMin(parent + (rv > ru ? rv : ru), rv < ru ? rv : ru);
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kBlock) k_compress(uint32_t *parent, uint32_t n)
 {
     const uint64_t stride = (uint64_t)gridDim.x * kBlock;
@@ -531,6 +564,22 @@ int launch_sample(ccgpu_ctx *ctx, const LocalCCArgs &a, uint32_t vlo, uint32_t v
     return CCGPU_OK;
 }
 
+/* Step 1 over [vlo, vhi) for row entries [r0, r1), in the kernel the hook
+ * mode asks for. */
+int launch_sample_any(ccgpu_ctx *ctx, const LocalCCArgs &a, uint32_t vlo, uint32_t vhi, int r0,
+                      int r1, cudaStream_t st, unsigned blocks)
+{
+    if (a.o.hook_mode & CCGPU_HOOK_MINHOOK) {
+        const uint64_t *fseg = a.seg_filter ? a.seg : nullptr;
+        CC_KLAUNCH(ctx, CCK_SAMPLE, k_sample_min, blocks, kBlock, 0, st, a.row_ptr, a.col, a.n,
+                   a.m, a.labels, vlo, vhi, r0, r1, fseg, a.nseg);
+        return CCGPU_OK;
+    }
+    if (a.o.hook_mode & CCGPU_HOOK_LAZY)
+        return launch_sample<true>(ctx, a, vlo, vhi, r0, r1, st, blocks);
+    return launch_sample<false>(ctx, a, vlo, vhi, r0, r1, st, blocks);
+}
+
 template <bool LAZY>
 int launch_finish(ccgpu_ctx *ctx, const LinkParams &P, const Geometry &g, cudaStream_t st)
 {
@@ -555,12 +604,12 @@ int cc_local_resolve_opts(const ccgpu_cc_opts *in, ccgpu_cc_opts *o)
         if (o->chunk_size <= 0)
             o->chunk_size = 4096;
         if (o->hook_mode < 0)
-            o->hook_mode = CCGPU_HOOK_CADENCE;
+            o->hook_mode = CCGPU_HOOK_CADENCE | CCGPU_HOOK_MINHOOK;
     }
     if (o->sample_rounds > 8)
         return ccgpu_set_error(CCGPU_ERR_INVALID, "sample_rounds %d above 8", o->sample_rounds);
-    if (o->hook_mode > 7)
-        return ccgpu_set_error(CCGPU_ERR_INVALID, "hook_mode %d is not a mask of 1|2|4",
+    if (o->hook_mode > 15)
+        return ccgpu_set_error(CCGPU_ERR_INVALID, "hook_mode %d is not a mask of 1|2|4|8",
                                o->hook_mode);
     if (o->heavy_degree < 32)
         o->heavy_degree = 32;
@@ -600,9 +649,7 @@ int cc_local_sample_range(ccgpu_ctx *ctx, const LocalCCArgs &a, uint32_t v_lo, u
     Geometry g = {1, 1};
     CC_TRY(geometry(ctx, &g));
     const unsigned sb = cc_blocks(v_hi - v_lo, kBlock, g.stream_blocks);
-    if (a.o.hook_mode & CCGPU_HOOK_LAZY)
-        return launch_sample<true>(ctx, a, v_lo, v_hi, 0, a.o.sample_rounds, st, sb);
-    return launch_sample<false>(ctx, a, v_lo, v_hi, 0, a.o.sample_rounds, st, sb);
+    return launch_sample_any(ctx, a, v_lo, v_hi, 0, a.o.sample_rounds, st, sb);
 }
 
 int cc_local_run(ccgpu_ctx *ctx, const LocalCCArgs &a, const LocalCCScratch &s, cudaStream_t st,
@@ -618,22 +665,23 @@ int cc_local_run(ccgpu_ctx *ctx, const LocalCCArgs &a, const LocalCCScratch &s, 
     if (!init_done)
         CC_TRY(cc_local_init(ctx, a, s, st));
     const bool skip = k > 0 && a.o.skip_giant;
+    const bool minhook = (a.o.hook_mode & CCGPU_HOOK_MINHOOK) != 0;
     if (k > 0) {
         if (!sampled) {
+            /* with MINHOOK the finish pass relinks entry 0, so the init
+             * pass's first hook is all round 0 needs */
+            const int r_start = (minhook && (a.o.hook_mode & CCGPU_HOOK_FIRST)) ? 1 : 0;
             if (a.o.hook_mode & CCGPU_HOOK_CADENCE) {
-                for (int r = 0; r < k; ++r) {
-                    if (lazy)
-                        CC_TRY(launch_sample<true>(ctx, a, 0, a.n, r, r + 1, st, sb));
-                    else
-                        CC_TRY(launch_sample<false>(ctx, a, 0, a.n, r, r + 1, st, sb));
+                if (r_start > 0 && r_start < k)
+                    CC_KLAUNCH(ctx, CCK_COMPRESS, k_compress, sb, kBlock, 0, st, a.labels, a.n);
+                for (int r = r_start; r < k; ++r) {
+                    CC_TRY(launch_sample_any(ctx, a, 0, a.n, r, r + 1, st, sb));
                     if (r + 1 < k)
                         CC_KLAUNCH(ctx, CCK_COMPRESS, k_compress, sb, kBlock, 0, st, a.labels,
                                    a.n);
                 }
-            } else if (lazy) {
-                CC_TRY(launch_sample<true>(ctx, a, 0, a.n, 0, k, st, sb));
-            } else {
-                CC_TRY(launch_sample<false>(ctx, a, 0, a.n, 0, k, st, sb));
+            } else if (r_start < k) {
+                CC_TRY(launch_sample_any(ctx, a, 0, a.n, r_start, k, st, sb));
             }
         }
         if (skip) {
@@ -648,7 +696,7 @@ int cc_local_run(ccgpu_ctx *ctx, const LocalCCArgs &a, const LocalCCScratch &s, 
     P.n = a.n;
     P.m = a.m;
     P.parent = a.labels;
-    P.skip_from = (uint32_t)k;
+    P.skip_from = minhook ? 0u : (uint32_t)k;
     P.giants = skip ? s.giants : nullptr;
     P.seg = a.seg;
     P.nseg = a.seg ? a.nseg : 1;
@@ -677,7 +725,7 @@ extern "C" void ccgpu_cc_opts_default(ccgpu_cc_opts *o)
     o->sample_rounds = 2;
     o->heavy_degree = 8192;
     o->skip_giant = 1;
-    o->hook_mode = CCGPU_HOOK_CADENCE;
+    o->hook_mode = CCGPU_HOOK_CADENCE | CCGPU_HOOK_MINHOOK;
 }
 
 static int fill_stats(ccgpu_ctx *ctx, const LocalCCArgs &a, const LocalCCScratch &s,

@@ -122,19 +122,25 @@ typedef struct {
                          * <= 0 = default (8192)                              */
     int skip_giant;     /* 1 (default) = step 4 skips the giant tree;
                          * 0 = link every remaining neighbour               */
-    int hook_mode;      /* bit mask, < 0 = default (CADENCE):
+    int hook_mode;      /* bit mask, < 0 = default (CADENCE | MINHOOK):
                          *  1 FIRST: the init pass hooks v under its first
                          *    neighbour when that is smaller (plain store,
                          *    no walk); step 1 links the rest
                          *  2 LAZY: a root is hooked under the smaller
                          *    endpoint itself instead of walking to its root
                          *  4 CADENCE: one launch per sampled neighbour with a
-                         *    shortcut pass after each                        */
+                         *    shortcut pass after each
+                         *  8 MINHOOK: sampling only builds a valid forest:
+                         *    roots are lowered with fire-and-forget atomicMin
+                         *    (no CAS retry), and step 4 links every entry of
+                         *    each row outside the giant tree, sampled ones
+                         *    included                                        */
 } ccgpu_cc_opts;
 
 #define CCGPU_HOOK_FIRST 1
 #define CCGPU_HOOK_LAZY 2
 #define CCGPU_HOOK_CADENCE 4
+#define CCGPU_HOOK_MINHOOK 8
 
 typedef struct {
     uint32_t giant_label;   /* root found in step 3 (UINT32_MAX if off)      */
@@ -232,6 +238,19 @@ int ccgpu_boundary_sort(ccgpu_ctx *ctx, uint32_t *d_pairs, uint64_t count, uint3
  * (src/boundary_sort.c:100-119); *new_count receives the kept count. */
 int ccgpu_boundary_dedup(ccgpu_ctx *ctx, uint32_t *d_pairs, uint64_t count, uint64_t *new_count,
                          void *stream);
+
+/* Plans: the whole local-CC launch sequence for fixed arguments captured
+ * once into a CUDA graph and replayed with one cudaGraphLaunch.  The plan
+ * owns a private context (its scratch), so it stays valid whatever else the
+ * caller runs; its arguments (pointers, sizes, options) are fixed at
+ * creation.  ccgpu_plan_kernels() is the number of kernels one launch runs. */
+typedef struct ccgpu_plan ccgpu_plan;
+int ccgpu_local_cc_plan(const uint64_t *d_row_ptr, const uint32_t *d_col_idx, uint32_t n,
+                        uint64_t m, uint32_t *d_labels, const ccgpu_cc_opts *opts,
+                        ccgpu_plan **out);
+int ccgpu_plan_launch(ccgpu_plan *plan, void *stream);
+int ccgpu_plan_kernels(const ccgpu_plan *plan);
+void ccgpu_plan_destroy(ccgpu_plan *plan);
 
 /* ccgpu_local_cc without any device allocation.  No counterpart in the
  * reference: it exists for callers that cannot allocate device memory (code

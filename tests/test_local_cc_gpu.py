@@ -20,7 +20,7 @@ OPTION_GRID = [
 ]
 # every hook mode (first hook / lazy hook / cadence) on two schedules
 OPTION_GRID += [dict(chunk_size=c, sample_rounds=r, heavy_degree=64, skip_giant=1, hook_mode=h)
-                for h in range(8) for c, r in ((4096, 2), (1, 3))]
+                for h in range(16) for c, r in ((4096, 2), (1, 3))]
 
 
 @pytest.fixture(scope="module")
@@ -176,9 +176,31 @@ def test_final_shortcut_race_regression(torch):
              graphs.small_cases()["zigzag"], graphs.small_cases()["long_path"]]
     for rp, col in cases:
         uf = oracle.uf_labels(rp, col)
-        for hm in range(8):
+        for hm in range(16):
             for ch, sr in ((1, 0), (256, 0), (2048, 2), (4096, 1)):
                 for _ in range(3):
                     lab = solve_dev(torch, rp, col, _lib.opts(chunk_size=ch, sample_rounds=sr,
                                                                hook_mode=hm))
                     assert (lab == uf).all(), (hm, ch, sr)
+
+
+def test_plan_replays_match(torch):
+    """The CUDA-graph plan gives the same labels on every replay."""
+    L = _lib.lib()
+    rp, col = graphs.rmat_csr(14, 16, seed=12)
+    n, m = len(rp) - 1, int(rp[-1])
+    d_rp, d_col = to_dev(torch, rp, col)
+    lab = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+    uf = oracle.uf_labels(rp, col)
+    for o in (None, _lib.opts(chunk_size=1, hook_mode=5)):
+        plan = C.c_void_p()
+        _lib.check(L.ccgpu_local_cc_plan(d_rp.data_ptr(), d_col.data_ptr(), n, m,
+                                         lab.data_ptr(), C.byref(o) if o else None,
+                                         C.byref(plan)))
+        assert L.ccgpu_plan_kernels(plan) >= 6
+        for _ in range(3):
+            lab.fill_(-1)
+            _lib.check(L.ccgpu_plan_launch(plan, torch.cuda.current_stream().cuda_stream))
+            torch.cuda.synchronize()
+            assert (lab.cpu().numpy().view(np.uint32) == uf).all()
+        L.ccgpu_plan_destroy(plan)
