@@ -39,6 +39,11 @@ WORKLOADS = {
     "rmat20": dict(kind="rmat", scale=20, ef=16),
     "grid8192": dict(kind="grid", rows=8192, cols=8192, p=0.1),
     "grid2048": dict(kind="grid", rows=2048, cols=2048, p=0.1),
+    # partitioned path (compute_connected_components_mpi_advanced)
+    "c3": dict(kind="rmat_big", scale=26, n=65_600_000, undirected=1_800_000_000, parts=4,
+               dist=True),
+    "rmat24p4": dict(kind="rmat", scale=24, ef=16, parts=4, dist=True),
+    "rmat22p4": dict(kind="rmat", scale=22, ef=16, parts=4, dist=True),
 }
 L2_BYTES = 126 * 1024 * 1024
 FALLBACK_HBM_GBS = 6650.0
@@ -53,6 +58,8 @@ def make_graph(torch, wl, seed):
     spec = WORKLOADS[wl]
     if spec["kind"] == "rmat":
         return graphs.rmat_csr_torch(torch, spec["scale"], spec["ef"], seed=seed)
+    if spec["kind"] == "rmat_big":
+        return graphs.rmat_csr_big(torch, spec["scale"], spec["n"], spec["undirected"], seed=seed)
     return graphs.grid_csr_torch(torch, spec["rows"], spec["cols"], spec["p"], seed=seed)
 
 
@@ -62,6 +69,10 @@ def workload_config(wl, n, m):
     if spec["kind"] == "rmat":
         cfg.update(graph=f"R-MAT scale {spec['scale']}, edge factor {spec['ef']}, "
                          "a/b/c/d=.57/.19/.19/.05, seeded id permutation")
+    elif spec["kind"] == "rmat_big":
+        cfg.update(graph=f"R-MAT over 2^{spec['scale']} ids, a/b/c/d=.57/.19/.19/.05, seeded "
+                         f"permutation truncated to {spec['n']} vertices, sampled for about "
+                         f"{spec['undirected']} distinct undirected edges")
     else:
         cfg.update(graph=f"{spec['rows']}x{spec['cols']} 4-neighbour grid, "
                          f"{int(spec['p'] * 100)}% of edges deleted")
@@ -217,6 +228,196 @@ def cpu_baseline(rp, col, budget_s=20.0):
             "sample": sample, "seconds_per_solve": t}
 
 
+def dist_bytes(n, m, st):
+    """Algorithmic bytes per launch of the partitioned path's kernels (the
+    local-CC kernels are counted as in algorithmic_bytes, without the
+    sampled-entry term)."""
+    R, U, G, reps = int(st.boundary_raw), int(st.pair_count), int(st.ghost_count), \
+        int(st.rep_count)
+    return {
+        "init": 4 * n, "sample": 8 * (n + 1) + 8 * n, "compress": 8 * n,
+        "final_compress": 8 * n, "link_rows": 4 * n + 8 * n, "giant": 4096,
+        "dist_reps": 4 * n + 12 * reps, "dist_pairs": 8 * (n + 1) + 4 * m + 4 * n + 8 * R,
+        "sort_hist": 8 * R, "sort_scatter": 16 * R, "dist_dedup": 8 * R,
+        "dist_ghosts": 8 * R + 8 * U + 24 * G, "merge_hook": 12 * U,
+        "merge_upd": 12 * reps, "merge_exch_pack": 16 * G, "merge_exch_scatter": 16 * G,
+        "dist_labels": 12 * n, "dist_plan": 0, "dist_bounds": 0, "scan": 0,
+        "dist_pairs_heavy": 0,
+    }
+
+
+def run_dist(args, torch, dist_mod, rank, world, dev):
+    """Partitioned workloads: a step is one ccgpu_dist_cc solve (all
+    partitions device-resident) - the timed region of the reference's
+    benchmark, one compute_connected_components_mpi_advanced call."""
+    import numpy as np
+    from cc_mpi_b200 import _lib, cc, dist
+    spec = WORKLOADS[args.workload]
+    L = _lib.lib()
+    parts = args.parts or spec["parts"]
+    rp_d, col_d = make_graph(torch, args.workload, args.seed + rank)
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()  # hand the generator's cached blocks back for the solver's pool
+    n, m = rp_d.numel() - 1, col_d.numel()
+    lab = torch.empty(n, dtype=torch.int32, device=dev)
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+
+    def solve():
+        return dist.dist_cc_device(rp_d, col_d, n, m, parts, 1, args.chunk, args.exchange,
+                                   d_labels=lab, stream=sptr)
+
+    st, bounds = solve()
+    # verification: the unpartitioned union-find path, the device invariants,
+    # and (for graphs the CPU checks in seconds) the oracle
+    ref = torch.empty(n, dtype=torch.int32, device=dev)
+    cc.local_cc_device(rp_d, col_d, n, m, ref, stream=sptr)
+    torch.cuda.synchronize()
+    verified = bool(torch.equal(ref, lab)) and \
+        cc.check_labels_device(rp_d, col_d, n, m, lab) == 0
+    oracle_checked = False
+    if rank == 0 and not args.no_verify and m < 1_200_000_000:
+        import oracle
+        want, _, ost = oracle.dist_cc(rp_d.cpu().numpy().view(np.uint64),
+                                      col_d.cpu().numpy().view(np.uint32), parts, 1,
+                                      args.exchange)
+        verified = verified and bool((lab.cpu().numpy().view(np.uint32) == want).all()) and \
+            ost.rounds == st.rounds and ost.exchanges == st.exchanges
+        oracle_checked = True
+    del ref
+    torch.cuda.empty_cache()
+    for _ in range(args.warmup):
+        flush.fill_(1)
+        st, bounds = solve()  # the last warm solve's statistics are reported
+    torch.cuda.synchronize()
+
+    def timed_steps():
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(args.steps)]
+        torch.cuda.synchronize()
+        for i in range(args.steps):
+            flush.fill_(i)
+            ev[i][0].record(stream)
+            solve()
+            ev[i][1].record(stream)
+        torch.cuda.synchronize()
+        t = sum(a.elapsed_time(b) for a, b in ev) / args.steps
+        if world > 1:
+            tt = torch.tensor([t], device=dev)
+            dist_mod.all_reduce(tt, op=dist_mod.ReduceOp.MAX)
+            t = float(tt.item())
+        return t
+
+    if world > 1:
+        dist_mod.barrier()
+    launches0 = L.ccgpu_ctx_launches(None)
+    with ClockSampler(dev.index or 0) as clk:
+        t_ms = timed_steps()
+    launches = L.ccgpu_ctx_launches(None) - launches0
+    k = L.ccgpu_prof_kernels()
+    names = [L.ccgpu_prof_name(i).decode() for i in range(k)]
+    _lib.check(L.ccgpu_prof_enable(None, 1))
+    _lib.check(L.ccgpu_prof_collect(None, None, None))
+    t_prof_ms = timed_steps()
+    ms = (C.c_double * k)()
+    cnt = (C.c_uint64 * k)()
+    _lib.check(L.ccgpu_prof_collect(None, ms, cnt))
+    _lib.check(L.ccgpu_prof_enable(None, 0))
+    per = {names[i]: (ms[i] / cnt[i], int(cnt[i])) for i in range(k) if cnt[i]}
+    total_kernel_ms = {kk: v[0] * v[1] / args.steps for kk, v in per.items()}
+    dom = max(total_kernel_ms, key=total_kernel_ms.get)
+    bytes_per = dist_bytes(n, m, st)
+    peak, peak_kind = read_peaks()
+    achieved = bytes_per.get(dom, 0) / (per[dom][0] / 1e3) / 1e9
+    step_bytes = sum(bytes_per.get(kk, 0) * v[1] / args.steps for kk, v in per.items())
+    whole = step_bytes / (t_ms / 1e3) / 1e9
+    value = (m // 2) * world / (t_ms / 1e3) / 1e9
+
+    # e2e through the reference-facing calls with host buffers
+    rp_h = torch.empty(n + 1, dtype=torch.int64, pin_memory=True)
+    col_h = torch.empty(m, dtype=torch.int32, pin_memory=True)
+    rp_h.copy_(rp_d)
+    col_h.copy_(col_d)
+    lab_h = np.empty(n, dtype=np.uint32)
+    vp = C.c_void_p
+    L.cc_group_create.restype = vp
+    L.cc_group_create.argtypes = [C.c_int]
+    L.cc_group_set_verbose.argtypes = [vp, C.c_int]
+    L.cc_group_free.argtypes = [vp]
+    L.dist_csr_from_csr.argtypes = [C.POINTER(_lib.CSRGraph), C.c_int,
+                                    C.POINTER(_lib.DistCSRGraph), vp]
+    L.free_dist_csr_view.argtypes = [C.POINTER(_lib.DistCSRGraph)]
+    L.cc_mpi_solve.argtypes = [C.POINTER(_lib.DistCSRGraph), vp, C.c_int, C.c_int, vp, vp]
+    grp = L.cc_group_create(parts)
+    L.cc_group_set_verbose(grp, 0)
+    g = _lib.CSRGraph()
+    g.n, g.m = n, m
+    g.row_ptr = C.cast(rp_h.data_ptr(), C.POINTER(C.c_uint64))
+    g.col_idx = C.cast(col_h.data_ptr(), C.POINTER(C.c_uint32))
+    e2e_t = []
+    for _ in range(max(args.e2e_steps, 1) + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        Gd = _lib.DistCSRGraph()
+        if L.dist_csr_from_csr(C.byref(g), 1, C.byref(Gd), grp) != 0:
+            raise RuntimeError("dist_csr_from_csr failed: " + L.ccgpu_last_error().decode())
+        _lib.check(L.cc_mpi_solve(C.byref(Gd), lab_h.ctypes.data, args.chunk, args.exchange,
+                                  grp, None))
+        L.free_dist_csr_view(C.byref(Gd))
+        e2e_t.append(time.perf_counter() - t0)
+    e2e_s = sum(e2e_t[1:]) / len(e2e_t[1:])
+    e2e_ok = bool((lab_h == lab.cpu().numpy().view(np.uint32)).all())
+    L.cc_group_free(grp)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(rp_h.numpy().view(np.uint64), col_h.numpy().view(np.uint32),
+                           budget_s=30.0)
+    if rank == 0:
+        cfg = workload_config(args.workload, n, m)
+        cfg.update(partitions=parts, chunk_size=args.chunk, exchange_interval=args.exchange,
+                   bounds=[int(x) for x in bounds], components=int(st.roots),
+                   rounds=int(st.rounds), exchanges=int(st.exchanges),
+                   boundary_raw=int(st.boundary_raw), boundary_dedup=int(st.pair_count),
+                   ghosts=int(st.ghost_count), reps=int(st.rep_count),
+                   sent_pairs=int(st.sent_pairs), sort_passes=int(st.sort_passes),
+                   phases_ms={"bounds": st.ms_bounds, "local": st.ms_local,
+                              "pairs": st.ms_pairs, "sort": st.ms_sort,
+                              "ghosts": st.ms_ghosts, "merge": st.ms_merge},
+                   l2="2x L2 buffer written between timed steps; col_idx > L2",
+                   parallelism=f"{parts} partitions on one device" +
+                               (f", replicas{world}" if world > 1 else ""),
+                   verified=verified, verified_by_oracle=oracle_checked,
+                   e2e_labels_match=e2e_ok)
+        line = {
+            "metric": "CC GTEPS", "value": value, "unit": "GTEPS", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic", "config": cfg,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                         "traffic": None, "bytes_per_launch": bytes_per.get(dom, 0),
+                         "ms_per_launch": per[dom][0],
+                         "whole_solve": {"algorithmic_bytes": step_bytes, "achieved": whole,
+                                         "frac": whole / peak}},
+            "kernels": {kk: {"ms": round(v[0], 5), "launches": v[1],
+                             "gbs": round(bytes_per.get(kk, 0) / (v[0] / 1e3) / 1e9, 1)}
+                        for kk, v in per.items()},
+            "ms_per_step_kernel_by_kernel": t_prof_ms,
+            "cpu_baseline": cpu,
+            "e2e": {"value": (m // 2) * world / e2e_s / 1e9, "unit": "GTEPS",
+                    "h2d_bytes_per_step": 8 * (n + 1) + 4 * m, "d2h_bytes_per_step": 4 * n,
+                    "ms_per_step": e2e_s * 1e3,
+                    "api": "dist_csr_from_csr + compute_connected_components_mpi_advanced "
+                           "(pinned host CSR, labels to host)"},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -230,6 +431,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--hook-mode", type=int, default=-1, help="ccgpu_cc_opts.hook_mode")
     ap.add_argument("--sample-rounds", type=int, default=-1)
+    ap.add_argument("--parts", type=int, default=0, help="partitions (partitioned workloads)")
+    ap.add_argument("--chunk", type=int, default=8192, help="-c of the partitioned workloads")
+    ap.add_argument("--exchange", type=int, default=1, help="-e of the partitioned workloads")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -256,6 +460,12 @@ def main():
     L = _lib.lib()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    if WORKLOADS[args.workload].get("dist"):
+        rc = run_dist(args, torch, dist, rank, world, dev)
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return rc
 
     rp_d, col_d = make_graph(torch, args.workload, args.seed + rank)
     torch.cuda.synchronize()

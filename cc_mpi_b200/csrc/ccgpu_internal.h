@@ -82,6 +82,7 @@ enum {
     CCK_SCAN,
     CCK_BATCH,
     CCK_MISC,
+    CCK_DIST_PAIRS_HEAVY,
     CCK_NUM
 };
 
@@ -245,6 +246,78 @@ __device__ __forceinline__ void cc_union(uint32_t *parent, uint32_t a, uint32_t 
 __device__ __forceinline__ uint32_t cc_warp_min(uint32_t v)
 {
     return __reduce_min_sync(0xffffffffu, v);
+}
+
+/* Spreads the rows of a heavy-row list over every warp of the grid in
+ * pieces of `chunk` entries: rows are taken 256 at a time, the block scans
+ * their piece counts in shared memory, and piece g of the batch goes to
+ * warp g mod (all warps).  fn(v, jb, je) is called by all 32 lanes of a
+ * warp together.  Rows are [row_ptr[v] + skip, row_ptr[v+1]) clamped to m.
+ * Must be called by every thread of a 256-thread block. */
+template <typename Fn>
+__device__ __forceinline__ void cc_for_heavy_pieces(const uint32_t *list, uint32_t count,
+                                                    const uint64_t *row_ptr, uint64_t m,
+                                                    uint32_t skip, uint64_t chunk, Fn fn)
+{
+    __shared__ uint64_t s_pre[257];
+    __shared__ uint64_t s_beg[256], s_end[256];
+    __shared__ uint32_t s_v[256];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t gwarp = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp;
+    const uint64_t nwarps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+    for (uint32_t b0 = 0; b0 < count; b0 += 256) {
+        const uint32_t h = b0 + threadIdx.x;
+        uint64_t pieces = 0;
+        if (h < count) {
+            uint32_t v = list[h];
+            uint64_t e = row_ptr[v + 1], b = row_ptr[v];
+            if (e > m)
+                e = m;
+            if (b > e)
+                b = e;
+            b = b + skip < e ? b + skip : e;
+            s_v[threadIdx.x] = v;
+            s_beg[threadIdx.x] = b;
+            s_end[threadIdx.x] = e;
+            pieces = (e - b + chunk - 1) / chunk;
+        }
+        /* block-wide exclusive scan of the piece counts (256 threads) */
+        uint64_t incl = pieces;
+        for (int o = 1; o < 32; o <<= 1) {
+            uint64_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o)
+                incl += y;
+        }
+        __shared__ uint64_t s_w[8];
+        if (lane == 31)
+            s_w[warp] = incl;
+        __syncthreads();
+        uint64_t pre = 0, total = 0;
+        for (int w = 0; w < 8; ++w) {
+            pre += (w < warp) ? s_w[w] : 0ull;
+            total += s_w[w];
+        }
+        s_pre[threadIdx.x] = pre + incl - pieces;
+        if (threadIdx.x == 0)
+            s_pre[256] = total;
+        __syncthreads();
+        const int rows = count - b0 < 256u ? (int)(count - b0) : 256;
+        for (uint64_t g = gwarp; g < total; g += nwarps) {
+            int lo = 0, hi = rows; /* last row whose first piece is <= g */
+            while (hi - lo > 1) {
+                int mid = (lo + hi) >> 1;
+                if (s_pre[mid] <= g)
+                    lo = mid;
+                else
+                    hi = mid;
+            }
+            uint64_t jb = s_beg[lo] + (g - s_pre[lo]) * chunk;
+            uint64_t je = jb + chunk < s_end[lo] ? jb + chunk : s_end[lo];
+            fn(s_v[lo], jb, je);
+        }
+        __syncthreads();
+    }
+    (void)lane;
 }
 
 #endif /* __CUDACC__ */

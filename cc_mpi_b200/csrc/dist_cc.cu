@@ -309,31 +309,57 @@ struct DedupParams {
     uint32_t *ghost_v;                 /* [G]               */
     uint64_t *ghost_pairs;             /* [G+1] first pair  */
     uint32_t *ghost_labels, *prev_sent;
-    unsigned long long *gcount;        /* [parts]           */
+    uint64_t *gh_first;                /* [parts] first ghost of each partition, ~0 if none */
 };
 
-__device__ __forceinline__ void dedup_flags(const DedupParams &D, uint64_t i, uint64_t k,
+/* A tile of sorted keys staged in shared memory with one pad slot per 16
+ * keys, so that thread t's 16 consecutive keys sit in distinct banks. */
+#define DD_PAD(i) ((i) + ((i) >> 4))
+constexpr int kDedupSmem = kDedupTile + kDedupTile / 16;
+
+__device__ __forceinline__ void dedup_stage(const DedupParams &D, uint64_t *s_keys,
+                                            uint64_t *s_prev)
+{
+    const uint64_t tile = (uint64_t)blockIdx.x * kDedupTile;
+    for (int i = threadIdx.x; i < (int)kDedupTile; i += kB) {
+        uint64_t gi = tile + i;
+        s_keys[DD_PAD(i)] = gi < D.count ? D.keys[gi] : 0ull;
+    }
+    if (threadIdx.x == 0)
+        *s_prev = tile > 0 ? D.keys[tile - 1] : 0ull;
+    __syncthreads();
+}
+
+/* Flags of the key at tile position li (global index gi): a new pair
+ * (unique) and a new ghost (partition or remote changed). */
+__device__ __forceinline__ void dedup_flags(const DedupParams &D, const uint64_t *s_keys,
+                                            uint64_t s_prev, int li, uint64_t gi, uint64_t &k,
                                             bool &uniq, bool &gst)
 {
-    if (i == 0) {
+    k = s_keys[DD_PAD(li)];
+    if (gi == 0) {
         uniq = gst = true;
         return;
     }
-    uint64_t prev = D.keys[i - 1];
+    uint64_t prev = li > 0 ? s_keys[DD_PAD(li - 1)] : s_prev;
     uniq = k != prev;
     gst = (k >> D.rb) != (prev >> D.rb);
 }
 
 __global__ void __launch_bounds__(kB) k_dedup_count(DedupParams D)
 {
+    __shared__ uint64_t s_keys[kDedupSmem];
+    __shared__ uint64_t s_prev;
     __shared__ uint32_t s_w[2][kW];
-    const uint64_t base = (uint64_t)blockIdx.x * kDedupTile + (uint64_t)threadIdx.x * kDedupItems;
+    dedup_stage(D, s_keys, &s_prev);
+    const uint64_t tile = (uint64_t)blockIdx.x * kDedupTile;
     uint32_t cu = 0, cg = 0;
     for (int j = 0; j < kDedupItems; ++j) {
-        uint64_t i = base + j;
-        if (i < D.count) {
+        int li = threadIdx.x * kDedupItems + j;
+        if (tile + li < D.count) {
+            uint64_t k;
             bool u, g;
-            dedup_flags(D, i, D.keys[i], u, g);
+            dedup_flags(D, s_keys, s_prev, li, tile + li, k, u, g);
             cu += u;
             cg += g;
         }
@@ -358,17 +384,21 @@ __global__ void __launch_bounds__(kB) k_dedup_count(DedupParams D)
 
 __global__ void __launch_bounds__(kB) k_dedup_write(DedupParams D)
 {
+    __shared__ uint64_t s_keys[kDedupSmem];
+    __shared__ uint64_t s_prev;
     __shared__ uint32_t s_wu[kW], s_wg[kW];
     __shared__ uint32_t s_b[CCGPU_MAX_PARTS + 1];
     for (int i = threadIdx.x; i <= D.parts; i += kB)
         s_b[i] = D.bounds[i];
-    const uint64_t base = (uint64_t)blockIdx.x * kDedupTile + (uint64_t)threadIdx.x * kDedupItems;
+    dedup_stage(D, s_keys, &s_prev);
+    const uint64_t tile = (uint64_t)blockIdx.x * kDedupTile;
     uint32_t cu = 0, cg = 0;
     for (int j = 0; j < kDedupItems; ++j) {
-        uint64_t i = base + j;
-        if (i < D.count) {
+        int li = threadIdx.x * kDedupItems + j;
+        if (tile + li < D.count) {
+            uint64_t k;
             bool u, g;
-            dedup_flags(D, i, D.keys[i], u, g);
+            dedup_flags(D, s_keys, s_prev, li, tile + li, k, u, g);
             cu += u;
             cg += g;
         }
@@ -379,25 +409,28 @@ __global__ void __launch_bounds__(kB) k_dedup_write(DedupParams D)
     uint64_t gp = D.g_off[blockIdx.x] + ig - cg; /* ghosts started before this thread */
     const uint64_t pmask = (1ull << D.gb) - 1ull;
     const uint64_t rmask = (1ull << D.rb) - 1ull;
+    const int pshift = D.rb + D.gb;
     for (int j = 0; j < kDedupItems; ++j) {
-        uint64_t i = base + j;
-        if (i >= D.count)
+        int li = threadIdx.x * kDedupItems + j;
+        uint64_t gi = tile + li;
+        if (gi >= D.count)
             break;
-        uint64_t k = D.keys[i];
+        uint64_t k;
         bool u, g;
-        dedup_flags(D, i, k, u, g);
+        dedup_flags(D, s_keys, s_prev, li, gi, k, u, g);
+        const int p = (int)(k >> pshift);
         if (g) {
             uint32_t remote = (uint32_t)((k >> D.rb) & pmask);
-            int p = (int)(k >> (D.rb + D.gb));
+            uint64_t prev = gi == 0 ? ~0ull : (li > 0 ? s_keys[DD_PAD(li - 1)] : s_prev);
+            if (gi == 0 || (int)(prev >> pshift) != p)
+                D.gh_first[p] = gp; /* first ghost of partition p */
             D.ghost_v[gp] = remote;
             D.ghost_pairs[gp] = up;
             D.ghost_labels[gp] = remote;   /* src/cc_mpi.c:456-457 */
             D.prev_sent[gp] = 0xffffffffu; /* src/cc_mpi.c:480-487 */
-            atomicAdd(D.gcount + p, 1ull);
             gp++;
         }
         if (u) {
-            int p = (int)(k >> (D.rb + D.gb));
             D.pair_rep[up] = s_b[p] + (uint32_t)(k & rmask);
             D.pair_g[up] = (uint32_t)(gp - 1);
             up++;
@@ -470,7 +503,7 @@ __global__ void __launch_bounds__(kB) k_hook_init(MergeParams M)
         uint32_t l = ok ? M.ghost_labels[M.pair_g[k]] : 0xffffffffu;
         unsigned peers = __match_any_sync(0xffffffffu, r);
         uint32_t mn = __reduce_min_sync(peers, l);
-        if (ok && (__ffs(peers) - 1) == lane)
+        if (ok && (__ffs(peers) - 1) == lane && mn < M.hook[r])
             atomicMin(M.hook + r, mn);
     }
 }
@@ -576,30 +609,47 @@ __global__ void __launch_bounds__(kB) k_pack(MergeParams M)
  * and the hook minimum of every rep paired with that ghost is lowered. */
 __global__ void __launch_bounds__(kB) k_scatter(MergeParams M)
 {
+    const int lane = threadIdx.x & 31;
     const uint64_t stride = (uint64_t)gridDim.x * kB;
     const int regions = M.parts * M.parts;
-    for (uint64_t s = (uint64_t)blockIdx.x * kB + threadIdx.x; s < M.ghosts; s += stride) {
-        /* region (p, q) holding slot s: seg is ascending in p-major order */
-        int lo = 0, hi = regions;
-        while (hi - lo > 1) {
-            int mid = (lo + hi) >> 1;
-            int p = mid / M.parts, q = mid % M.parts;
-            if (M.seg[(uint64_t)p * (M.parts + 1) + q] <= s)
-                lo = mid;
-            else
-                hi = mid;
+    for (uint64_t base = (uint64_t)blockIdx.x * kB; base < M.ghosts; base += stride) {
+        const uint64_t s = base + threadIdx.x;
+        bool has = false;
+        uint64_t g = 0;
+        uint32_t lbl = 0;
+        if (s < M.ghosts) {
+            /* region (p, q) holding slot s: seg is ascending in p-major order */
+            int lo = 0, hi = regions;
+            while (hi - lo > 1) {
+                int mid = (lo + hi) >> 1;
+                int p = mid / M.parts, q = mid % M.parts;
+                if (M.seg[(uint64_t)p * (M.parts + 1) + q] <= s)
+                    lo = mid;
+                else
+                    hi = mid;
+            }
+            int p = lo / M.parts, q = lo % M.parts;
+            uint64_t rstart = M.seg[(uint64_t)p * (M.parts + 1) + q];
+            if (s - rstart < M.msg_count[q * M.parts + p]) {
+                uint64_t pr = M.msg[s];
+                g = rstart + (pr >> 32);
+                lbl = (uint32_t)pr;
+                M.ghost_labels[g] = lbl;
+                has = true;
+            }
         }
-        int p = lo / M.parts, q = lo % M.parts;
-        uint64_t rstart = M.seg[(uint64_t)p * (M.parts + 1) + q];
-        if (s - rstart >= M.msg_count[q * M.parts + p])
+        unsigned got = __popc(__ballot_sync(0xffffffffu, has));
+        if (lane == 0 && got)
+            atomicAdd(M.sent, (unsigned long long)got);
+        if (!has)
             continue;
-        uint64_t pr = M.msg[s];
-        uint64_t g = rstart + (pr >> 32);
-        uint32_t lbl = (uint32_t)pr;
-        M.ghost_labels[g] = lbl;
-        for (uint64_t k = M.ghost_pairs[g]; k < M.ghost_pairs[g + 1]; ++k)
-            atomicMin(M.hook + M.pair_rep[k], lbl);
-        atomicAdd(M.sent, 1ull);
+        /* hook values only decrease: a plain read, even a stale one, that is
+         * already <= lbl means the atomicMin would change nothing */
+        for (uint64_t k = M.ghost_pairs[g]; k < M.ghost_pairs[g + 1]; ++k) {
+            uint32_t r = M.pair_rep[k];
+            if (lbl < M.hook[r])
+                atomicMin(M.hook + r, lbl);
+        }
     }
 }
 
@@ -788,7 +838,7 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
     if (P > 1) {
         const unsigned eb = (unsigned)ctx->sm_count * 4;
         CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit, eb, kB, 0, st, E);
-        CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit_heavy, eb, kB, 0, st, E);
+        CC_KLAUNCH(ctx, CCK_DIST_PAIRS_HEAVY, k_emit_heavy, eb, kB, 0, st, E);
     }
     unsigned long long hc[2];
     CC_CUDA(cudaMemcpyAsync(hc, counters, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
@@ -818,13 +868,13 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
     D.bounds = bounds;
     D.parts = P;
     uint64_t U = 0, G = 0;
-    std::vector<unsigned long long> gcount(P, 0);
+    std::vector<uint64_t> gfirst(P, ~0ull);
     const uint64_t T = (R + kDedupTile - 1) / kDedupTile;
     uint64_t *gh_off = nullptr, *segs = nullptr;
     CC_TRY(cc_bufs_get(&B, (void **)&gh_off, (P + 1) * sizeof(uint64_t)));
     CC_TRY(cc_bufs_get(&B, (void **)&segs, (size_t)P * (P + 1) * sizeof(uint64_t)));
-    CC_TRY(cc_bufs_get(&B, (void **)&D.gcount, P * sizeof(unsigned long long)));
-    CC_CUDA(cudaMemsetAsync(D.gcount, 0, P * sizeof(unsigned long long), st));
+    CC_TRY(cc_bufs_get(&B, (void **)&D.gh_first, P * sizeof(uint64_t)));
+    CC_CUDA(cudaMemsetAsync(D.gh_first, 0xff, P * sizeof(uint64_t), st));
     if (R > 0) {
         uint64_t *u_off = nullptr, *g_off = nullptr;
         CC_TRY(cc_bufs_get(&B, (void **)&D.tile_u, T * sizeof(uint32_t)));
@@ -856,12 +906,14 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
         CC_CUDA(cudaMemcpyAsync(D.ghost_pairs + G, &U, sizeof(uint64_t), cudaMemcpyHostToDevice,
                                 st));
     }
-    CC_CUDA(cudaMemcpyAsync(gcount.data(), D.gcount, P * sizeof(unsigned long long),
+    CC_CUDA(cudaMemcpyAsync(gfirst.data(), D.gh_first, P * sizeof(uint64_t),
                             cudaMemcpyDeviceToHost, st));
     CC_CUDA(cudaStreamSynchronize(st));
-    std::vector<uint64_t> hoff(P + 1, 0);
-    for (int p = 0; p < P; ++p)
-        hoff[p + 1] = hoff[p] + gcount[p];
+    /* partition p's ghosts: [first ghost of p, first ghost of the next
+     * partition that has any) */
+    std::vector<uint64_t> hoff(P + 1, G);
+    for (int p = P - 1; p >= 0; --p)
+        hoff[p] = gfirst[p] != ~0ull ? gfirst[p] : hoff[p + 1];
     CC_CUDA(cudaMemcpyAsync(gh_off, hoff.data(), (P + 1) * sizeof(uint64_t),
                             cudaMemcpyHostToDevice, st));
     {
@@ -872,7 +924,7 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
     CC_TRY(clock_mark(clk, st)); /* 5 */
     if (o.verbose >= 2) {
         for (int p = 0; p < P; ++p)
-            printf("[part %d] ghost_count=%llu\n", p, (unsigned long long)gcount[p]);
+            printf("[part %d] ghost_count=%llu\n", p, (unsigned long long)(hoff[p + 1] - hoff[p]));
         printf("[all] boundary_edges raw=%llu dedup=%llu reps=%llu sort_passes=%d\n",
                (unsigned long long)R, (unsigned long long)U, (unsigned long long)S.rep_count,
                S.sort_passes);
@@ -1104,6 +1156,68 @@ extern "C" int ccgpu_boundary_sort(ccgpu_ctx *ctx, uint32_t *d_pairs, uint64_t c
             e = cudaStreamSynchronize(st);
         if (e != cudaSuccess)
             rc = ccgpu_cuda_fail(e, "boundary sort", __FILE__, __LINE__);
+    } while (0);
+    cc_bufs_release(&B);
+    return rc;
+}
+
+extern "C" int ccgpu_sort_keys(ccgpu_ctx *ctx, uint64_t *d_keys, uint64_t *d_alt, uint64_t count,
+                               int bits, int *in_alt, void *stream)
+{
+    if (in_alt)
+        *in_alt = 0;
+    if (count <= 1)
+        return CCGPU_OK;
+    if (!d_keys || !d_alt)
+        return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_sort_keys: NULL buffer");
+    CC_TRY(ccgpu_ctx_resolve(&ctx));
+    cudaStream_t st = (cudaStream_t)stream;
+    DevBufs B;
+    CC_TRY(cc_bufs_init(&B, st));
+    uint64_t *sorted = d_keys;
+    int rc = cc_radix_sort_u64(ctx, d_keys, d_alt, count, bits, &sorted, nullptr, &B, st);
+    cc_bufs_release(&B);
+    if (in_alt)
+        *in_alt = sorted == d_alt;
+    return rc;
+}
+
+extern "C" int ccgpu_unique_keys(ccgpu_ctx *ctx, const uint64_t *d_keys, uint64_t count,
+                                 uint64_t *d_out, uint64_t *out_count, void *stream)
+{
+    if (!out_count)
+        return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_unique_keys: out_count is NULL");
+    *out_count = 0;
+    if (count == 0)
+        return CCGPU_OK;
+    if (!d_keys || !d_out)
+        return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_unique_keys: NULL buffer");
+    CC_TRY(ccgpu_ctx_resolve(&ctx));
+    cudaStream_t st = (cudaStream_t)stream;
+    DevBufs B;
+    CC_TRY(cc_bufs_init(&B, st));
+    int rc = CCGPU_OK;
+    do {
+        uint32_t *flag = nullptr;
+        uint64_t *pos = nullptr;
+        if ((rc = cc_bufs_get(&B, (void **)&flag, count * sizeof(uint32_t))) != CCGPU_OK ||
+            (rc = cc_bufs_get(&B, (void **)&pos, (count + 1) * sizeof(uint64_t))) != CCGPU_OK)
+            break;
+        const unsigned blocks = cc_blocks(count, 256, (unsigned)ctx->sm_count * 8);
+        k_flag_new<<<blocks, 256, 0, st>>>(d_keys, count, flag);
+        ctx->launches++;
+        if ((rc = cc_scan_u32(ctx, flag, pos, count, &B, st)) != CCGPU_OK)
+            break;
+        k_compact<<<blocks, 256, 0, st>>>(d_keys, pos, count, d_out);
+        ctx->launches++;
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(out_count, pos + count, sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                                st);
+        if (e == cudaSuccess)
+            e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess)
+            rc = ccgpu_cuda_fail(e, "ccgpu_unique_keys", __FILE__, __LINE__);
     } while (0);
     cc_bufs_release(&B);
     return rc;

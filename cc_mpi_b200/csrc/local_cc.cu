@@ -291,42 +291,83 @@ struct LinkParams {
     const uint64_t *fseg;      /* segment filter offsets, NULL = off        */
 };
 
+/* Warp-cooperative link of v with up to K entries per lane (all 32 lanes
+ * call it).  Hooking every entry's root under v's root one by one piles the
+ * CAS attempts of the whole row onto v's root (a herd: one wins per round,
+ * the rest retry).  Instead the warp first hooks v's tree under the
+ * smallest root among its entries; v's root is then no larger than any
+ * entry's root, so the remaining hooks go to each entry's own root. */
+template <int K>
+__device__ __forceinline__ void warp_link_min_first(uint32_t *parent, uint32_t v, const uint32_t *u,
+                                                    const bool *ok, int lane)
+{
+    uint32_t r[K];
+    uint32_t mn = 0xffffffffu;
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+        r[i] = ok[i] ? cc_find(parent, u[i]) : 0xffffffffu;
+        mn = r[i] < mn ? r[i] : mn;
+    }
+    mn = __reduce_min_sync(0xffffffffu, mn);
+    if (mn == 0xffffffffu)
+        return;
+    if (lane == 0) {
+        uint32_t rv = cc_find(parent, v);
+        if (rv != mn)
+            cc_link_roots(parent, rv, mn);
+    }
+    __syncwarp();
+    uint32_t rv = cc_find(parent, v);
+#pragma unroll
+    for (int i = 0; i < K; ++i)
+        if (ok[i] && r[i] != rv)
+            cc_link_roots(parent, r[i], rv);
+}
+
 /* One warp links v with row entries [beg, end) that fall in sp: 16-byte
- * column loads for the aligned body, scalar head and tail. */
+ * column loads for the aligned body, scalar loads for head and tail, every
+ * step taken by all 32 lanes together. */
 template <bool LAZY>
 __device__ __forceinline__ void warp_link_row(const LinkParams &P, uint32_t v, uint64_t beg,
                                               uint64_t end, int lane, Span sp)
 {
-    uint64_t body_end = beg;
+    uint64_t a = beg, body_end = beg;
     if (P.vec) {
-        uint64_t a = (beg + 3) & ~3ull;
+        a = (beg + 3) & ~3ull;
         if (a > end)
             a = end;
         body_end = end & ~3ull;
         if (body_end < a)
             body_end = a;
-        if (beg + lane < a) {
-            uint32_t u = __ldg(P.col + beg + lane);
-            if (in_span(sp, u))
-                cc_union<LAZY>(P.parent, v, u);
-        }
-        const uint4 *c4 = reinterpret_cast<const uint4 *>(P.col);
-        for (uint64_t q = a / 4 + lane; q < body_end / 4; q += 32) {
-            uint4 x = __ldg(c4 + q);
-            if (in_span(sp, x.x))
-                cc_union<LAZY>(P.parent, v, x.x);
-            if (in_span(sp, x.y))
-                cc_union<LAZY>(P.parent, v, x.y);
-            if (in_span(sp, x.z))
-                cc_union<LAZY>(P.parent, v, x.z);
-            if (in_span(sp, x.w))
-                cc_union<LAZY>(P.parent, v, x.w);
-        }
     }
-    for (uint64_t j = body_end + lane; j < end; j += 32) {
-        uint32_t u = __ldg(P.col + j);
-        if (in_span(sp, u))
-            cc_union<LAZY>(P.parent, v, u);
+    /* scalar entries: [beg, a) and [body_end, end) */
+    const uint64_t head = a - beg, scalars = head + (end - body_end);
+    for (uint64_t s0 = 0; s0 < scalars; s0 += 32) {
+        uint64_t s = s0 + lane;
+        uint32_t u[1] = {0};
+        bool ok[1] = {false};
+        if (s < scalars) {
+            u[0] = __ldg(P.col + (s < head ? beg + s : body_end + (s - head)));
+            ok[0] = in_span(sp, u[0]);
+        }
+        warp_link_min_first<1>(P.parent, v, u, ok, lane);
+    }
+    const uint4 *c4 = reinterpret_cast<const uint4 *>(P.col);
+    for (uint64_t q0 = a / 4; q0 < body_end / 4; q0 += 32) {
+        uint64_t q = q0 + lane;
+        uint32_t u[4] = {0, 0, 0, 0};
+        bool ok[4] = {false, false, false, false};
+        if (q < body_end / 4) {
+            uint4 x = __ldg(c4 + q);
+            u[0] = x.x;
+            u[1] = x.y;
+            u[2] = x.z;
+            u[3] = x.w;
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                ok[i] = in_span(sp, u[i]);
+        }
+        warp_link_min_first<4>(P.parent, v, u, ok, lane);
     }
 }
 
@@ -479,14 +520,24 @@ __global__ void __launch_bounds__(kBlock) k_link_heavy(LinkParams P)
         uint64_t beg = r.beg + P.skip_from;
         if (beg > r.end)
             beg = r.end;
+        /* 4096-entry pieces over the CTAs, 512 entries per warp, linked
+         * min-first like the warp rows */
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         uint64_t nseg = (r.end - beg + kHeavySeg - 1) / kHeavySeg;
         for (uint64_t s = blockIdx.x; s < nseg; s += gridDim.x) {
-            uint64_t sb = beg + s * kHeavySeg;
-            uint64_t se = sb + kHeavySeg < r.end ? sb + kHeavySeg : r.end;
-            for (uint64_t j = sb + threadIdx.x; j < se; j += kBlock) {
-                uint32_t u = __ldg(P.col + j);
-                if (in_span(sp, u))
-                    cc_union<LAZY>(P.parent, v, u);
+            uint64_t wb = beg + s * kHeavySeg + (uint64_t)warp * (kHeavySeg / kWarps);
+            uint64_t we = wb + kHeavySeg / kWarps;
+            if (we > r.end)
+                we = r.end;
+            for (uint64_t j0 = wb; j0 < we; j0 += 32) {
+                uint64_t j = j0 + lane;
+                uint32_t u[1] = {0};
+                bool ok[1] = {false};
+                if (j < we) {
+                    u[0] = __ldg(P.col + j);
+                    ok[0] = in_span(sp, u[0]);
+                }
+                warp_link_min_first<1>(P.parent, v, u, ok, lane);
             }
         }
     }

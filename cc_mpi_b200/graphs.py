@@ -172,6 +172,82 @@ def rmat_csr_torch(torch, scale, edge_factor=16, seed=1, device="cuda", abc=RMAT
     return symmetric_csr_torch(torch, nv, src, dst)
 
 
+def _sort_unique_keys(torch, keys, bits):
+    """Sorted distinct values of a device int64 tensor, through the library's
+    radix sort (ccgpu_sort_keys / ccgpu_unique_keys)."""
+    import ctypes as C
+    from . import _lib
+    L = _lib.lib()
+    L.ccgpu_sort_keys.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_int,
+                                  C.POINTER(C.c_int), C.c_void_p]
+    L.ccgpu_unique_keys.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p,
+                                    C.POINTER(C.c_uint64), C.c_void_p]
+    n = keys.numel()
+    alt = torch.empty_like(keys)
+    in_alt = C.c_int(0)
+    st = torch.cuda.current_stream().cuda_stream
+    _lib.check(L.ccgpu_sort_keys(None, keys.data_ptr(), alt.data_ptr(), n, bits, C.byref(in_alt),
+                                 st))
+    src, dst = (alt, keys) if in_alt.value else (keys, alt)
+    cnt = C.c_uint64(0)
+    _lib.check(L.ccgpu_unique_keys(None, src.data_ptr(), n, dst.data_ptr(), C.byref(cnt), st))
+    del src
+    return dst[:cnt.value]
+
+
+def rmat_csr_big(torch, scale, n, target_undirected, seed=1, device="cuda", abc=RMAT_ABC,
+                 chunk=1 << 27, keep_estimate=0.87):
+    """Large R-MAT graph built chunk by chunk on the device: ids over 2**scale
+    permuted by a seeded permutation and truncated to [0, n); enough samples
+    for about `target_undirected` distinct undirected edges (the exact count
+    is whatever remains after dropping self loops and duplicates).  Returns
+    (row_ptr int64[n+1], col int32[m]) with sorted rows."""
+    assert n <= (1 << scale) and n < (1 << 31)
+    bits = max(1, (n - 1).bit_length())
+    mask = (1 << bits) - 1
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    perm = torch.randperm(1 << scale, generator=g, device=device)
+    a, b, c = abc
+    samples = int(target_undirected / keep_estimate)
+    keys = torch.empty(samples, dtype=torch.int64, device=device)
+    w = 0
+    for start in range(0, samples, chunk):
+        cnt = min(chunk, samples - start)
+        src = torch.zeros(cnt, dtype=torch.int64, device=device)
+        dst = torch.zeros(cnt, dtype=torch.int64, device=device)
+        for lvl in range(scale):
+            r = torch.rand(cnt, generator=g, device=device)
+            src |= (r >= a + b).to(torch.int64) << lvl
+            dst |= (((r >= a) & (r < a + b)) | (r >= a + b + c)).to(torch.int64) << lvl
+            del r
+        src, dst = perm[src], perm[dst]
+        keep = (src < n) & (dst < n) & (src != dst)
+        lo = torch.minimum(src, dst)[keep]
+        hi = torch.maximum(src, dst)[keep]
+        del src, dst, keep
+        k = (lo << bits) | hi
+        keys[w:w + k.numel()] = k
+        w += k.numel()
+        del lo, hi, k
+    del perm
+    und = _sort_unique_keys(torch, keys[:w], 2 * bits).clone()
+    del keys
+    both = torch.empty(2 * und.numel(), dtype=torch.int64, device=device)
+    both[:und.numel()] = und
+    both[und.numel():] = ((und & mask) << bits) | (und >> bits)
+    del und
+    both = _sort_unique_keys(torch, both, 2 * bits)
+    col = (both & mask).to(torch.int32)
+    counts = torch.zeros(n, dtype=torch.int64, device=device)
+    for start in range(0, both.numel(), chunk):
+        counts += torch.bincount(both[start:start + chunk] >> bits, minlength=n)
+    del both
+    row_ptr = torch.zeros(n + 1, dtype=torch.int64, device=device)
+    torch.cumsum(counts, 0, out=row_ptr[1:])
+    return row_ptr, col
+
+
 def grid_csr_torch(torch, rows, cols, p_delete=0.1, seed=1, device="cuda"):
     g = torch.Generator(device=device)
     g.manual_seed(seed)

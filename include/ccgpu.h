@@ -228,6 +228,17 @@ int ccgpu_dist_cc(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d_c
 int ccgpu_partition_bounds(const uint64_t *d_row_ptr, uint32_t n, int parts, int use_edge,
                            uint32_t *h_bounds, void *stream);
 
+/* Generic u64 key sort (the LSD radix sort behind the boundary sort): sorts
+ * d_keys[0..count) ascending on bits [0, bits) (higher bits must be zero),
+ * using d_alt (same size) as the other buffer; *in_alt = 1 when the result
+ * ended in d_alt.  Asynchronous on `stream`. */
+int ccgpu_sort_keys(ccgpu_ctx *ctx, uint64_t *d_keys, uint64_t *d_alt, uint64_t count, int bits,
+                    int *in_alt, void *stream);
+/* Writes the distinct values of the sorted d_keys[0..count) to d_out
+ * (may not alias d_keys); *out_count receives their number.  Synchronous. */
+int ccgpu_unique_keys(ccgpu_ctx *ctx, const uint64_t *d_keys, uint64_t count, uint64_t *d_out,
+                      uint64_t *out_count, void *stream);
+
 /* Sorts d_pairs[0..count) in place, ascending on (remote << 32 | rep) - the
  * reference's boundary edge order (src/boundary_sort.c:5-8,93-98) - where
  * each pair is {uint32 rep, uint32 remote}.  max_rep / max_remote bound the
