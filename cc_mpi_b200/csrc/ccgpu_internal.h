@@ -83,6 +83,7 @@ enum {
     CCK_BATCH,
     CCK_MISC,
     CCK_DIST_PAIRS_HEAVY,
+    CCK_DIST_PAIRS_BITMAP,
     CCK_NUM
 };
 

@@ -133,6 +133,10 @@ struct EmitParams {
     uint32_t *heavy_count;
     uint32_t heavy_cap;
     uint32_t heavy_deg;
+    unsigned long long *raw; /* cut edges seen (the reference's raw count) */
+    uint32_t *bitmap;        /* [parts][bm_words] (p, remote) bits, giant rep */
+    uint64_t bm_words;
+    const uint32_t *giants;  /* [parts] giant root of each partition, NULL = no bitmap */
 };
 
 struct WarpBuf {
@@ -171,12 +175,52 @@ __device__ __forceinline__ uint64_t make_key(const EmitParams &E, int p, uint32_
     return ((uint64_t)p << (E.gb + E.rb)) | ((uint64_t)u << E.rb) | rep;
 }
 
+/* Cut edges into the giant local component of a partition all carry that
+ * partition's giant rep, so most raw pairs repeat the same (p, remote, giant)
+ * key.  Those edges set bit (p, remote) of a bitmap instead of emitting a
+ * key (read-before-set keeps repeated hits off the atomic unit; a stale read
+ * only costs one redundant atomicOr); k_bitmap_keys turns the bitmap into
+ * one key per set bit.  Every other cut edge emits its key as before, so the
+ * sorted, deduplicated pair list is the same set. */
+__device__ __forceinline__ void bitmap_set(const EmitParams &E, int p, uint32_t u)
+{
+    uint32_t *w = E.bitmap + (uint64_t)p * E.bm_words + (u >> 5);
+    const uint32_t bit = 1u << (u & 31);
+    uint32_t cur;
+    asm volatile("ld.global.ca.u32 %0, [%1];" : "=r"(cur) : "l"(w));
+    if (!(cur & bit))
+        atomicOr(w, bit);
+}
+
+/* Giant label (global min id) of every partition, ~0 when it has none or the
+ * bitmap path is off. */
+__device__ __forceinline__ void load_giant_labels(const EmitParams &E, uint32_t *s_gl)
+{
+    for (int i = threadIdx.x; i < E.parts; i += blockDim.x) {
+        uint32_t g = E.giants ? E.giants[i] : 0xffffffffu;
+        s_gl[i] = g < E.n ? __ldg(E.label + g) : 0xffffffffu;
+    }
+}
+
+/* Raw cut-edge count of the reference (src/cc_mpi.c:364-375), one atomic per
+ * warp at the end of the kernel. */
+__device__ __forceinline__ void add_raw(const EmitParams &E, unsigned long long raw, int lane)
+{
+    for (int o = 16; o > 0; o >>= 1)
+        raw += __shfl_xor_sync(0xffffffffu, raw, o);
+    if (lane == 0 && raw)
+        atomicAdd(E.raw, raw);
+}
+
 __global__ void __launch_bounds__(kB) k_emit(EmitParams E)
 {
     __shared__ uint64_t s_buf[kW][kEmitBuf];
     __shared__ uint32_t s_b[CCGPU_MAX_PARTS + 1];
+    __shared__ uint32_t s_gl[CCGPU_MAX_PARTS];
     for (int i = threadIdx.x; i <= E.parts; i += kB)
         s_b[i] = E.bounds[i];
+    load_giant_labels(E, s_gl);
+    unsigned long long raw = 0;
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     WarpBuf w = {s_buf[warp], 0};
@@ -219,7 +263,11 @@ __global__ void __launch_bounds__(kB) k_emit(EmitParams E)
                 uint64_t j = j0 + lane;
                 uint32_t u = j < ee ? __ldg(E.col + j) : E.n;
                 bool bnd = u < E.n && (u < ll || u >= hh);
-                wb_append(w, E, lane, bnd, make_key(E, pp, u, rr));
+                bool gnt = bnd && rr + ll == s_gl[pp];
+                if (gnt)
+                    bitmap_set(E, pp, u);
+                raw += bnd;
+                wb_append(w, E, lane, bnd && !gnt, make_key(E, pp, u, rr));
             }
         }
         uint32_t sdeg = deg < 32 ? (uint32_t)deg : 0u;
@@ -227,48 +275,91 @@ __global__ void __launch_bounds__(kB) k_emit(EmitParams E)
         for (uint32_t it = 0; it < maxd; ++it) {
             uint32_t u = it < sdeg ? __ldg(E.col + beg + it) : E.n;
             bool bnd = u < E.n && (u < lo || u >= hi);
-            wb_append(w, E, lane, bnd, make_key(E, p, u, rep));
+            bool gnt = bnd && rep + lo == s_gl[p];
+            if (gnt)
+                bitmap_set(E, p, u);
+            raw += bnd;
+            wb_append(w, E, lane, bnd && !gnt, make_key(E, p, u, rep));
         }
     }
     wb_flush(w, E, lane);
+    add_raw(E, raw, lane);
 }
 
 __global__ void __launch_bounds__(kB) k_emit_heavy(EmitParams E)
 {
     __shared__ uint64_t s_buf[kW][kEmitBuf];
     __shared__ uint32_t s_b[CCGPU_MAX_PARTS + 1];
+    __shared__ uint32_t s_gl[CCGPU_MAX_PARTS];
     for (int i = threadIdx.x; i <= E.parts; i += kB)
         s_b[i] = E.bounds[i];
+    load_giant_labels(E, s_gl);
+    unsigned long long raw = 0;
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     WarpBuf w = {s_buf[warp], 0};
     uint32_t cnt = *E.heavy_count;
     if (cnt > E.heavy_cap)
         cnt = E.heavy_cap;
-    const uint64_t gw = (uint64_t)blockIdx.x * kW + warp, nw = (uint64_t)gridDim.x * kW;
-    for (uint32_t h = 0; h < cnt; ++h) {
-        uint32_t v = E.heavy_list[h];
-        int p = part_of(s_b, E.parts, v);
-        uint32_t lo = s_b[p], hi = s_b[p + 1];
-        uint32_t rep = __ldg(E.label + v) - lo;
-        uint64_t beg = __ldg(E.row_ptr + v), end = __ldg(E.row_ptr + v + 1);
-        if (end > E.m)
-            end = E.m;
-        if (beg > end)
-            beg = end;
-        uint64_t chunks = (end - beg + kHeavyChunk - 1) / kHeavyChunk;
-        for (uint64_t c = gw; c < chunks; c += nw) {
-            uint64_t cb = beg + c * kHeavyChunk;
-            uint64_t ce = cb + kHeavyChunk < end ? cb + kHeavyChunk : end;
-            for (uint64_t j0 = cb; j0 < ce; j0 += 32) {
-                uint64_t j = j0 + lane;
-                uint32_t u = j < ce ? __ldg(E.col + j) : E.n;
-                bool bnd = u < E.n && (u < lo || u >= hi);
-                wb_append(w, E, lane, bnd, make_key(E, p, u, rep));
+    cc_for_heavy_pieces(E.heavy_list, cnt, E.row_ptr, E.m, 0, kHeavyChunk,
+                        [&](uint32_t v, uint64_t jb, uint64_t je) {
+                            const int p = part_of(s_b, E.parts, v);
+                            const uint32_t lo = s_b[p], hi = s_b[p + 1];
+                            const uint32_t rep = __ldg(E.label + v) - lo;
+                            for (uint64_t j0 = jb; j0 < je; j0 += 32) {
+                                uint64_t j = j0 + lane;
+                                uint32_t u = j < je ? __ldg(E.col + j) : E.n;
+                                bool bnd = u < E.n && (u < lo || u >= hi);
+                                bool gnt = bnd && rep + lo == s_gl[p];
+                                if (gnt)
+                                    bitmap_set(E, p, u);
+                                raw += bnd;
+                                wb_append(w, E, lane, bnd && !gnt, make_key(E, p, u, rep));
+                            }
+                        });
+    wb_flush(w, E, lane);
+    add_raw(E, raw, lane);
+}
+
+/* One key (p, remote, giant rep of p) per set bit of the giant bitmap,
+ * appended after the keys k_emit wrote (the sort orders them). */
+__global__ void __launch_bounds__(kB) k_bitmap_keys(EmitParams E)
+{
+    __shared__ uint32_t s_b[CCGPU_MAX_PARTS + 1];
+    __shared__ uint32_t s_gl[CCGPU_MAX_PARTS];
+    for (int i = threadIdx.x; i <= E.parts; i += kB)
+        s_b[i] = E.bounds[i];
+    load_giant_labels(E, s_gl);
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const uint64_t total = (uint64_t)E.parts * E.bm_words;
+    const uint64_t stride = (uint64_t)gridDim.x * kB;
+    for (uint64_t base = (uint64_t)blockIdx.x * kB; base < total; base += stride) {
+        const uint64_t i = base + threadIdx.x;
+        uint32_t word = i < total ? E.bitmap[i] : 0u;
+        uint32_t c = __popc(word);
+        uint32_t incl = c;
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o)
+                incl += y;
+        }
+        const uint32_t wtot = __shfl_sync(0xffffffffu, incl, 31);
+        unsigned long long at = 0;
+        if (lane == 31 && wtot)
+            at = atomicAdd(E.count, (unsigned long long)wtot);
+        at = __shfl_sync(0xffffffffu, at, 31) + (incl - c);
+        if (word) {
+            const int p = (int)(i / E.bm_words);
+            const uint32_t u0 = (uint32_t)((i - (uint64_t)p * E.bm_words) << 5);
+            const uint32_t rep = s_gl[p] - s_b[p];
+            while (word) {
+                const int b = __ffs(word) - 1;
+                word &= word - 1;
+                E.out[at++] = make_key(E, p, u0 + (uint32_t)b, rep);
             }
         }
     }
-    wb_flush(w, E, lane);
 }
 
 /* --------------------------------------------------------------- reps */
@@ -806,7 +897,7 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
     if (rb + gb + pb > 64)
         return ccgpu_set_error(CCGPU_ERR_LIMIT, "boundary key needs %d bits", rb + gb + pb);
     uint32_t *rep_list = nullptr, *cur = nullptr, *nxt = nullptr, *hook = nullptr;
-    unsigned long long *counters = nullptr; /* [0] keys [1] reps [2] roots [3] sent */
+    unsigned long long *counters = nullptr; /* [0] keys [1] reps [2] roots [3] sent [4] raw */
     CC_TRY(cc_bufs_get(&B, (void **)&rep_list, (size_t)n * sizeof(uint32_t)));
     CC_TRY(cc_bufs_get(&B, (void **)&cur, (size_t)n * sizeof(uint32_t)));
     CC_TRY(cc_bufs_get(&B, (void **)&nxt, (size_t)n * sizeof(uint32_t)));
@@ -835,17 +926,33 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
     CC_TRY(cc_bufs_get(&B, (void **)&E.heavy_list, (size_t)E.heavy_cap * sizeof(uint32_t)));
     CC_TRY(cc_bufs_get(&B, (void **)&E.heavy_count, 256));
     CC_CUDA(cudaMemsetAsync(E.heavy_count, 0, sizeof(uint32_t), st));
+    E.raw = counters + 4;
+    /* giant bitmap: P bits per vertex, used while it stays small */
+    E.bm_words = ((uint64_t)n + 31) / 32;
+    E.giants = nullptr;
+    E.bitmap = nullptr;
+    const bool use_bitmap = P > 1 && a.o.sample_rounds > 0 && a.o.skip_giant &&
+                            (uint64_t)P * E.bm_words * 4 <= (1ull << 31);
+    if (use_bitmap) {
+        CC_TRY(cc_bufs_get(&B, (void **)&E.bitmap, (size_t)P * E.bm_words * 4));
+        CC_CUDA(cudaMemsetAsync(E.bitmap, 0, (size_t)P * E.bm_words * 4, st));
+        E.giants = ls.giants;
+    }
     if (P > 1) {
         const unsigned eb = (unsigned)ctx->sm_count * 4;
         CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit, eb, kB, 0, st, E);
         CC_KLAUNCH(ctx, CCK_DIST_PAIRS_HEAVY, k_emit_heavy, eb, kB, 0, st, E);
+        if (use_bitmap)
+            CC_KLAUNCH(ctx, CCK_DIST_PAIRS_BITMAP, k_bitmap_keys,
+                       cc_blocks((uint64_t)P * E.bm_words, kB, (unsigned)ctx->sm_count * 8), kB,
+                       0, st, E);
     }
-    unsigned long long hc[2];
-    CC_CUDA(cudaMemcpyAsync(hc, counters, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+    unsigned long long hc[5];
+    CC_CUDA(cudaMemcpyAsync(hc, counters, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                             st));
     CC_CUDA(cudaStreamSynchronize(st));
     const uint64_t R = hc[0];
-    S.boundary_raw = R;
+    S.boundary_raw = hc[4];
     S.rep_count = hc[1];
     CC_TRY(clock_mark(clk, st)); /* 3 */
 

@@ -22,7 +22,7 @@
  *                walks them edge-parallel, a warp takes rows of >= 32 entries
  *                with 16-byte column loads, rows above the heavy threshold go
  *                to a queue
- *   k_link_heavy queued rows split in 4096-entry pieces over every CTA
+ *   k_link_heavy queued rows split in 512-entry pieces over every warp
  *   k_count_roots, k_check_labels   reductions for stats and tests
  */
 #include <cstdio>
@@ -36,7 +36,7 @@ constexpr int kBlock = 256;
 constexpr int kWarps = kBlock / 32;
 constexpr uint32_t kNoGiant = 0xffffffffu;
 constexpr int kGiantSamples = 1024;
-constexpr uint64_t kHeavySeg = 4096;
+constexpr uint64_t kHeavyPiece = 512; /* entries per warp piece of a queued row */
 
 struct Rows {
     uint64_t beg, end;
@@ -507,40 +507,30 @@ __global__ void __launch_bounds__(kBlock, 4) k_link_rows(LinkParams P)
     }
 }
 
+/* Queued rows in pieces of kHeavyPiece entries spread over every warp of
+ * the grid (piece g of the list goes to warp g mod all warps), each piece
+ * linked min-first like the warp rows. */
 template <bool LAZY>
 __global__ void __launch_bounds__(kBlock) k_link_heavy(LinkParams P)
 {
     uint32_t cnt = P.cnt->heavy_count;
     if (cnt > P.heavy_cap)
         cnt = P.heavy_cap;
-    for (uint32_t h = 0; h < cnt; ++h) {
-        uint32_t v = P.heavy_list[h];
-        Rows r = row_of(P.row_ptr, v, P.m);
-        const Span sp = span_of(P.fseg, P.nseg, P.n, v);
-        uint64_t beg = r.beg + P.skip_from;
-        if (beg > r.end)
-            beg = r.end;
-        /* 4096-entry pieces over the CTAs, 512 entries per warp, linked
-         * min-first like the warp rows */
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-        uint64_t nseg = (r.end - beg + kHeavySeg - 1) / kHeavySeg;
-        for (uint64_t s = blockIdx.x; s < nseg; s += gridDim.x) {
-            uint64_t wb = beg + s * kHeavySeg + (uint64_t)warp * (kHeavySeg / kWarps);
-            uint64_t we = wb + kHeavySeg / kWarps;
-            if (we > r.end)
-                we = r.end;
-            for (uint64_t j0 = wb; j0 < we; j0 += 32) {
-                uint64_t j = j0 + lane;
-                uint32_t u[1] = {0};
-                bool ok[1] = {false};
-                if (j < we) {
-                    u[0] = __ldg(P.col + j);
-                    ok[0] = in_span(sp, u[0]);
-                }
-                warp_link_min_first<1>(P.parent, v, u, ok, lane);
-            }
-        }
-    }
+    const int lane = threadIdx.x & 31;
+    cc_for_heavy_pieces(P.heavy_list, cnt, P.row_ptr, P.m, P.skip_from, kHeavyPiece,
+                        [&](uint32_t v, uint64_t jb, uint64_t je) {
+                            const Span sp = span_of(P.fseg, P.nseg, P.n, v);
+                            for (uint64_t j0 = jb; j0 < je; j0 += 32) {
+                                uint64_t j = j0 + lane;
+                                uint32_t u[1] = {0};
+                                bool ok[1] = {false};
+                                if (j < je) {
+                                    u[0] = __ldg(P.col + j);
+                                    ok[0] = in_span(sp, u[0]);
+                                }
+                                warp_link_min_first<1>(P.parent, v, u, ok, lane);
+                            }
+                        });
 }
 
 __global__ void __launch_bounds__(kBlock) k_count_roots(const uint32_t *__restrict__ labels,

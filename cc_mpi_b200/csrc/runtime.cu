@@ -188,7 +188,8 @@ static const char *const kKernelNames[CCK_NUM] = {
     "count_roots", "check_labels", "dist_split", "dist_fill", "dist_reps", "dist_pairs",
     "sort_hist", "sort_scan", "sort_scatter", "dist_dedup", "dist_ghosts", "dist_plan",
     "merge_init", "merge_hook", "merge_upd", "merge_exch_pack", "merge_exch_scatter",
-    "dist_labels", "dist_bounds", "scan", "batch", "misc", "dist_pairs_heavy"};
+    "dist_labels", "dist_bounds", "scan", "batch", "misc", "dist_pairs_heavy",
+    "dist_pairs_bitmap"};
 
 struct cc_prof {
     std::vector<cudaEvent_t> pool;
