@@ -44,6 +44,10 @@ WORKLOADS = {
                dist=True),
     "rmat24p4": dict(kind="rmat", scale=24, ef=16, parts=4, dist=True),
     "rmat22p4": dict(kind="rmat", scale=22, ef=16, parts=4, dist=True),
+    # batched path (ccgpu_batch_*): graphs of log-uniform size, a third each
+    # Erdos-Renyi (mean degree 8), R-MAT (edge factor 16), grid (10% deleted)
+    "batch4096": dict(kind="batch", graphs=4096, n_min=1_000, n_max=2_000_000, batch=True),
+    "batch1024": dict(kind="batch", graphs=1024, n_min=1_000, n_max=200_000, batch=True),
 }
 L2_BYTES = 126 * 1024 * 1024
 FALLBACK_HBM_GBS = 6650.0
@@ -418,6 +422,237 @@ def run_dist(args, torch, dist_mod, rank, world, dev):
     return 0
 
 
+def batch_bytes(vo, eo, rounds_by_class, kinds_sampled):
+    """Algorithmic bytes per launch of the batched kernels, summed over the
+    classes: init writes 4n; a sampling round reads 8(n+G) of row pointers,
+    one column entry per vertex with a long enough row and the own label
+    (4n); a shortcut reads and writes labels (8n); the finish pass reads the
+    own label (4n) and the row bounds of every vertex (8(n+G)) - rows it
+    walks are extra and not counted; the final pass reads and writes labels
+    (8n)."""
+    n, G = int(vo[-1]), len(vo) - 1
+    return {
+        "batch_init": 4 * n,
+        "batch_sample": 8 * (n + G) + 4 * kinds_sampled + 4 * n,
+        "batch_compress": 8 * n,
+        "batch_giant": 4096 * G,
+        "batch_link": 4 * n + 8 * (n + G),
+        "batch_heavy": 0,
+        "batch_final": 8 * n,
+    }
+
+
+def run_batch(args, torch, dist_mod, rank, world, dev):
+    """Batched workload: a step is one solve of the whole batch - one CUDA
+    graph replay of the autotuned plan.  The same graphs solved one by one
+    with the single-graph kernel (ccgpu_local_cc in a loop) are timed beside
+    it and give the reference labels every graph is compared with."""
+    import numpy as np
+    from cc_mpi_b200 import _lib, batch, cc
+    spec_w = WORKLOADS[args.workload]
+    L = _lib.lib()
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+    t0 = time.perf_counter()
+    spec = batch.mix_spec(spec_w["graphs"], spec_w["n_min"], spec_w["n_max"],
+                          seed=args.seed + rank)
+    vo, eo, d_rp, d_col, kinds = batch.build_batch_torch(torch, spec)
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    gen_s = time.perf_counter() - t0
+    G, N, M = len(spec), int(vo[-1]), int(eo[-1])
+    log(f"batch: {G} graphs, {N} vertices, {M} entries, built in {gen_s:.1f} s")
+    flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device=dev)
+
+    def plain_loop(out):
+        for g in range(G):
+            a, b = int(vo[g]), int(vo[g + 1])
+            n, m = b - a, int(eo[g + 1] - eo[g])
+            if n == 0:
+                continue
+            cc.local_cc_device(d_rp[a + g:], d_col[int(eo[g]):] if m else d_col, n, m,
+                               out[a:b], stream=sptr)
+
+    want = torch.empty(N, dtype=torch.int32, device=dev)
+    plain_loop(want)
+    d_lab = torch.full((N,), -1, dtype=torch.int32, device=dev)
+    plan = batch.BatchPlan(vo, eo, d_rp, d_col, d_lab)
+    t0 = time.perf_counter()
+    tuning = plan.autotune(stream=sptr)
+    tune_s = time.perf_counter() - t0
+    plan.launch(stream=sptr)
+    torch.cuda.synchronize()
+    comps, done = plan.results(stream=sptr)
+    verified = bool(torch.equal(d_lab, want)) and bool((done == 1).all())
+    oracle_checked = []
+    if rank == 0 and not args.no_verify:
+        import oracle
+        lab = d_lab.cpu().numpy().view(np.uint32)
+        order = np.argsort([n for _, n, _ in spec])
+        for g in sorted({int(order[0]), int(order[G // 2]), int(order[-1])} |
+                        {int(x) for x in range(0, G, max(1, G // 16))}):
+            a, n = int(vo[g]), int(vo[g + 1] - vo[g])
+            rp = d_rp[a + g:a + g + n + 1].cpu().numpy().view(np.uint64)
+            col = d_col[int(eo[g]):int(eo[g + 1])].cpu().numpy().view(np.uint32)
+            ref = oracle.uf_labels(rp, col)
+            ok = bool((batch.labels_of(lab, vo, g) == ref).all()) and \
+                int(comps[g]) == oracle.count_components(ref)
+            verified = verified and ok
+            oracle_checked.append(g)
+    for _ in range(args.warmup):
+        flush.fill_(1)
+        plan.launch(stream=sptr)
+    torch.cuda.synchronize()
+
+    def timed(step_fn, steps):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(steps)]
+        if world > 1:
+            dist_mod.barrier()
+        torch.cuda.synchronize()
+        for i in range(steps):
+            flush.fill_(i)
+            ev[i][0].record(stream)
+            step_fn()
+            ev[i][1].record(stream)
+        torch.cuda.synchronize()
+        t = sum(a.elapsed_time(b) for a, b in ev) / steps
+        if world > 1:
+            tt = torch.tensor([t], device=dev)
+            dist_mod.all_reduce(tt, op=dist_mod.ReduceOp.MAX)
+            t = float(tt.item())
+        return t
+
+    with ClockSampler(dev.index or 0) as clk:
+        t_ms = timed(lambda: plan.launch(stream=sptr), args.steps)
+    launches = plan.kernels() * args.steps
+    plain_steps = max(1, min(args.steps, 3))
+    t_plain_ms = timed(lambda: plain_loop(want), plain_steps)
+
+    k = L.ccgpu_prof_kernels()
+    names = [L.ccgpu_prof_name(i).decode() for i in range(k)]
+    _lib.check(L.ccgpu_prof_enable(None, 1))
+    _lib.check(L.ccgpu_prof_collect(None, None, None))
+    t_prof_ms = timed(lambda: plan.run(stream=sptr), args.steps)
+    ms = (C.c_double * k)()
+    cnt = (C.c_uint64 * k)()
+    _lib.check(L.ccgpu_prof_collect(None, ms, cnt))
+    _lib.check(L.ccgpu_prof_enable(None, 0))
+    per = {names[i]: (ms[i] / cnt[i], int(cnt[i])) for i in range(k) if cnt[i]}
+    tot = {kk: v[0] * v[1] / args.steps for kk, v in per.items()}
+    dom = max(tot, key=tot.get)
+    deg = (d_rp[1:] - d_rp[:-1])
+    sampled = int((deg > 0).sum().item())  # rows with at least one entry (an upper bound
+    del deg                                # of the entries one sampling round reads)
+    bytes_per = batch_bytes(vo, eo, None, sampled)
+    peak, peak_kind = read_peaks()
+    achieved = bytes_per.get(dom, 0) / (per[dom][0] / 1e3) / 1e9
+    step_bytes = sum(bytes_per.get(kk, 0) * v[1] / args.steps for kk, v in per.items())
+    whole = step_bytes / (t_ms / 1e3) / 1e9
+
+    # e2e: host buffers through the one-shot public call ccgpu_batch_cc
+    # (plan set-up included), copies in and labels out inside the timed region
+    e2e = None
+    in_bytes = 8 * (N + G) + 4 * M
+    if in_bytes <= (24 << 30):
+        rp_h = torch.empty(N + G, dtype=torch.int64, pin_memory=True)
+        col_h = torch.empty(max(M, 1), dtype=torch.int32, pin_memory=True)
+        lab_h = torch.empty(N, dtype=torch.int32, pin_memory=True)
+        rp_h.copy_(d_rp)
+        col_h.copy_(d_col[:max(M, 1)])
+        Lb = batch._bind()
+        b = batch.Batch()
+        b.graphs = G
+        b.h_vtx_off = vo.ctypes.data_as(C.POINTER(C.c_uint64))
+        b.h_edge_off = eo.ctypes.data_as(C.POINTER(C.c_uint64))
+        b.d_row_ptr, b.d_col, b.d_labels = d_rp.data_ptr(), d_col.data_ptr(), d_lab.data_ptr()
+        t_e2e = []
+        for it in range(max(args.e2e_steps, 1) + 1):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            d_rp.copy_(rp_h, non_blocking=True)
+            d_col[:max(M, 1)].copy_(col_h, non_blocking=True)
+            _lib.check(Lb.ccgpu_batch_cc(None, C.byref(b), C.byref(tuning), None, sptr))
+            lab_h.copy_(d_lab, non_blocking=True)
+            torch.cuda.synchronize()
+            t_e2e.append(time.perf_counter() - t0)
+        e2e_s = sum(t_e2e[1:]) / len(t_e2e[1:])
+        e2e = {"value": G * world / e2e_s, "unit": "graphs/s", "gteps": (M // 2) * world / e2e_s
+               / 1e9, "h2d_bytes_per_step": in_bytes, "d2h_bytes_per_step": 4 * N,
+               "ms_per_step": e2e_s * 1e3, "labels_match": bool(torch.equal(lab_h.to(dev), want)),
+               "api": "ccgpu_batch_cc (one-shot plan + solve) with pinned host buffers"}
+        del rp_h, col_h, lab_h
+    else:
+        e2e = {"value": None, "unit": "graphs/s", "h2d_bytes_per_step": in_bytes,
+               "d2h_bytes_per_step": 4 * N,
+               "skipped": "packed batch above 24 GB of pinned host memory"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+        threads = os.cpu_count() or 1
+        rng = np.random.default_rng(args.seed)
+        done_g, edges, t_cpu = 0, 0, 0.0
+        for g in rng.permutation(G):
+            a, n = int(vo[g]), int(vo[g + 1] - vo[g])
+            rp = d_rp[a + g:a + g + n + 1].cpu().numpy().view(np.uint64)
+            col = d_col[int(eo[g]):int(eo[g + 1])].cpu().numpy().view(np.uint32)
+            t0 = time.perf_counter()
+            if oracle.have_ref():
+                oracle.ref_pthreads_labels(rp, col, threads, 8192)
+            else:
+                oracle.lp_labels(rp, col)
+            t_cpu += time.perf_counter() - t0
+            done_g += 1
+            edges += len(col) // 2
+            if t_cpu > 20.0:
+                break
+        cpu = {"value": done_g / t_cpu, "unit": "graphs/s", "gteps": edges / t_cpu / 1e9,
+               "cores": threads if oracle.have_ref() else 1,
+               "kind": "reference" if oracle.have_ref() else "port",
+               "sample": f"{done_g} of {G} graphs in seeded random order, solved one by one "
+                         f"(compute_connected_components_pthreads, chunk 8192)"}
+
+    if rank == 0:
+        classes = plan.class_graphs()
+        cfg = {"workload": args.workload, "graphs": G, "vertices": N, "undirected_edges": M // 2,
+               "csr_entries": M, "n_range": [spec_w["n_min"], spec_w["n_max"]],
+               "mix": "log-uniform vertex counts; ER mean degree 8 / R-MAT ef 16 / grid 10% "
+                      "deleted, one third each",
+               "graphs_per_class": [int(x) for x in classes], "tuning": tuning.as_dict(),
+               "autotune_s": tune_s, "build_s": gen_s,
+               "l2": "2x L2 buffer written between timed steps; packed batch > L2",
+               "parallelism": f"replicas{world}" if world > 1 else "single",
+               "verified_vs_plain_kernel": verified, "oracle_checked_graphs": len(oracle_checked)}
+        line = {
+            "metric": "batched CC graphs/s", "value": G * world / (t_ms / 1e3),
+            "unit": "graphs/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic", "config": cfg,
+            "gteps": (M // 2) * world / (t_ms / 1e3) / 1e9,
+            "plain_loop": {"ms_per_step": t_plain_ms, "graphs_per_s": G / (t_plain_ms / 1e3),
+                           "speedup_of_batch": t_plain_ms / t_ms,
+                           "api": "ccgpu_local_cc once per graph"},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                         "traffic": None, "bytes_per_launch": bytes_per.get(dom, 0),
+                         "ms_per_launch": per[dom][0],
+                         "whole_solve": {"algorithmic_bytes": step_bytes, "achieved": whole,
+                                         "frac": whole / peak}},
+            "kernels": {kk: {"ms": round(v[0], 5), "launches": v[1],
+                             "gbs": round(bytes_per.get(kk, 0) / (v[0] / 1e3) / 1e9, 1)}
+                        for kk, v in per.items()},
+            "ms_per_step_kernel_by_kernel": t_prof_ms,
+            "timing": "value: K replays of the batch's CUDA graph; kernels: the same K solves "
+                      "launched kernel by kernel with events around every launch",
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    plan.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -460,6 +695,12 @@ def main():
     L = _lib.lib()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    if WORKLOADS[args.workload].get("batch"):
+        rc = run_batch(args, torch, dist, rank, world, dev)
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return rc
     if WORKLOADS[args.workload].get("dist"):
         rc = run_dist(args, torch, dist, rank, world, dev)
         if world > 1:

@@ -1,0 +1,901 @@
+/*
+ * Batched connected components: many independent graphs solved by one
+ * sequence of grid-wide kernels, replayed as one CUDA graph.
+ *
+ * The reference solves one graph per call (src/cc_pthreads.c:152-229); a
+ * batch keeps that result for every graph - labels[v] is the minimum local
+ * vertex id of v's component in its own graph - and removes the per-graph
+ * launch and synchronisation cost that dominates small graphs.
+ *
+ * Layout (packed CSR-of-CSRs in HBM):
+ *   vtx_off[G+1], edge_off[G+1]  prefix sums of vertex and entry counts
+ *   row_ptr   graph g's n_g + 1 local row pointers at row_ptr[vtx_off[g] + g]
+ *   col       graph g's local (int32) neighbour ids at col[edge_off[g]]
+ *   labels    graph g's labels at labels[vtx_off[g]]
+ *
+ * Work is cut into tiles - up to `tile` consecutive vertices of one graph -
+ * so a CTA reads its graph's bases once per tile and then runs exactly the
+ * single-graph union-find (roots hooked larger-id under smaller-id) on the
+ * graph's own slice of the label array in local ids.  Graphs are grouped
+ * into degree classes by their mean row length; each class has its own
+ * tile size, sampled neighbours, shortcut cadence and warp-row threshold
+ * (the autotuner picks them), its own tile list and counters, and its own
+ * branch of the CUDA graph, so classes run concurrently.
+ *
+ * Per class, one solve is:
+ *   kb_init      parent[v] = v
+ *   kb_sample    r = 0..k-1: link v with its r-th neighbour (atomicMin on
+ *                the larger root: the forest stays valid; anything lost is
+ *                relinked by the finish pass), kb_compress after each round
+ *                when the cadence is on, and always before kb_giant
+ *   kb_giant     one CTA per graph: most frequent root of 1024 samples
+ *   kb_link      finish pass over the rows of vertices outside their graph's
+ *                giant tree: short rows gathered per CTA and walked
+ *                edge-parallel, rows of >= warp_degree entries by a warp,
+ *                rows above heavy_degree queued
+ *   kb_heavy     queued rows in 512-entry pieces over every warp
+ *   kb_final     labels[v] = root(v); per-graph root count, and the graph's
+ *                done flag set by its last tile
+ */
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "ccgpu_internal.h"
+
+namespace {
+
+constexpr int kB = 256;
+constexpr int kWarpsB = kB / 32;
+constexpr uint64_t kPiece = 512;
+constexpr uint32_t kNone = 0xffffffffu;
+
+struct BatchK {
+    const uint64_t *vtx_off;  /* [G+1] */
+    const uint64_t *edge_off; /* [G+1] */
+    const uint64_t *row_ptr;
+    const uint32_t *col;
+    uint32_t *labels;
+    const uint32_t *tile_g;   /* [tiles] graph of each tile      */
+    const uint32_t *tile_v0;  /* [tiles] first local vertex      */
+    uint32_t tiles;
+    uint32_t tile;            /* vertices per tile               */
+    const uint32_t *graphs;   /* [ngraphs] graphs of this class  */
+    uint32_t ngraphs;
+    uint32_t *giants;         /* [G] giant root (local id)       */
+    uint32_t *comps;          /* [G] components                  */
+    uint32_t *tiles_done;     /* [G] finished tiles of kb_final  */
+    uint32_t *done;           /* [G] 1 once the graph is solved  */
+    unsigned long long *grab; /* tile counter of kb_link         */
+    uint32_t *heavy_count;
+    uint64_t *heavy_list;     /* (g << 32) | v                   */
+    uint32_t heavy_cap;
+    uint32_t heavy_deg;
+    uint32_t warp_deg;
+    int skip;                 /* finish pass skips giant trees   */
+};
+
+struct Tile {
+    uint32_t g, v0, v1, n;
+    uint64_t ebase, m;
+    const uint64_t *rp;
+    uint32_t *parent;
+    const uint32_t *col;
+};
+
+__device__ __forceinline__ Tile tile_of(const BatchK &K, uint32_t t)
+{
+    Tile T;
+    T.g = __ldg(K.tile_g + t);
+    T.v0 = __ldg(K.tile_v0 + t);
+    const uint64_t vb = __ldg(K.vtx_off + T.g);
+    T.n = (uint32_t)(__ldg(K.vtx_off + T.g + 1) - vb);
+    T.v1 = T.v0 + K.tile < T.n ? T.v0 + K.tile : T.n;
+    T.ebase = __ldg(K.edge_off + T.g);
+    T.m = __ldg(K.edge_off + T.g + 1) - T.ebase;
+    T.rp = K.row_ptr + vb + T.g;
+    T.parent = K.labels + vb;
+    T.col = K.col + T.ebase;
+    return T;
+}
+
+__device__ __forceinline__ void row_bounds(const Tile &T, uint32_t v, uint64_t &b, uint64_t &e)
+{
+    b = __ldg(T.rp + v);
+    e = __ldg(T.rp + v + 1);
+    if (e > T.m)
+        e = T.m;
+    if (b > e)
+        b = e;
+}
+
+__global__ void __launch_bounds__(kB) kb_init(BatchK K)
+{
+    for (uint32_t t = blockIdx.x; t < K.tiles; t += gridDim.x) {
+        const Tile T = tile_of(K, t);
+        for (uint32_t v = T.v0 + threadIdx.x; v < T.v1; v += kB)
+            T.parent[v] = v;
+    }
+}
+
+/* Links row entry r of every vertex (MINHOOK sampling). */
+__global__ void __launch_bounds__(kB) kb_sample(BatchK K, int r)
+{
+    for (uint32_t t = blockIdx.x; t < K.tiles; t += gridDim.x) {
+        const Tile T = tile_of(K, t);
+        for (uint32_t v = T.v0 + threadIdx.x; v < T.v1; v += kB) {
+            uint64_t b, e;
+            row_bounds(T, v, b, e);
+            if (b + (uint64_t)r >= e)
+                continue;
+            const uint32_t u = __ldg(T.col + b + r);
+            if (u >= T.n)
+                continue;
+            const uint32_t rv = cc_find(T.parent, v), ru = cc_find(T.parent, u);
+            if (rv != ru)
+                atomicMin(T.parent + (rv > ru ? rv : ru), rv < ru ? rv : ru);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kB) kb_compress(BatchK K)
+{
+    for (uint32_t t = blockIdx.x; t < K.tiles; t += gridDim.x) {
+        const Tile T = tile_of(K, t);
+        for (uint32_t v = T.v0 + threadIdx.x; v < T.v1; v += kB) {
+            const uint32_t r = cc_find(T.parent, v);
+            if (r != v)
+                T.parent[v] = r;
+        }
+    }
+}
+
+/* One CTA per graph of the class: most frequent root of 1024 samples. */
+__global__ void __launch_bounds__(1024) kb_giant(BatchK K, uint32_t seed)
+{
+    __shared__ uint32_t s[1024];
+    __shared__ unsigned long long s_best[32];
+    for (uint32_t i = blockIdx.x; i < K.ngraphs; i += gridDim.x) {
+        const uint32_t g = __ldg(K.graphs + i);
+        const uint64_t vb = __ldg(K.vtx_off + g);
+        const uint32_t n = (uint32_t)(__ldg(K.vtx_off + g + 1) - vb);
+        if (n == 0) {
+            if (threadIdx.x == 0)
+                K.giants[g] = kNone;
+            continue;
+        }
+        const uint32_t h = cc_mix32(threadIdx.x * 0x9e3779b9u + seed + g);
+        const uint32_t v = (uint32_t)(((uint64_t)h * n) >> 32);
+        const uint32_t mode = cc_block_mode1024(cc_find_ro(K.labels + vb, v), s, s_best);
+        if (threadIdx.x == 0)
+            K.giants[g] = mode;
+    }
+}
+
+/* A warp links v with entries [b, e) of its graph: 16-byte column loads on
+ * the aligned body when the graph's columns are 16-byte aligned. */
+__device__ __forceinline__ void warp_row(const Tile &T, uint32_t v, uint64_t b, uint64_t e,
+                                         int lane)
+{
+    uint64_t a = b, body_end = b; /* unaligned columns: every entry scalar */
+    if ((((uintptr_t)T.col) & 15) == 0) {
+        a = (b + 3) & ~3ull;
+        if (a > e)
+            a = e;
+        body_end = e & ~3ull;
+        if (body_end < a)
+            body_end = a;
+    }
+    const uint64_t head = a - b, scalars = head + (e - body_end);
+    for (uint64_t s0 = 0; s0 < scalars; s0 += 32) {
+        const uint64_t s = s0 + lane;
+        uint32_t u[1] = {0};
+        bool ok[1] = {false};
+        if (s < scalars) {
+            u[0] = __ldg(T.col + (s < head ? b + s : body_end + (s - head)));
+            ok[0] = u[0] < T.n;
+        }
+        cc_warp_link_min_first<1>(T.parent, v, u, ok, lane);
+    }
+    const uint4 *c4 = reinterpret_cast<const uint4 *>(T.col);
+    for (uint64_t q0 = a / 4; q0 < body_end / 4; q0 += 32) {
+        const uint64_t q = q0 + lane;
+        uint32_t u[4] = {0, 0, 0, 0};
+        bool ok[4] = {false, false, false, false};
+        if (q < body_end / 4) {
+            const uint4 x = __ldg(c4 + q);
+            u[0] = x.x;
+            u[1] = x.y;
+            u[2] = x.z;
+            u[3] = x.w;
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                ok[i] = u[i] < T.n;
+        }
+        cc_warp_link_min_first<4>(T.parent, v, u, ok, lane);
+    }
+}
+
+/* Finish pass: tiles grabbed with an atomic counter; rows of vertices in
+ * the graph's giant tree are skipped (valid for symmetric graphs: every
+ * edge leaving the tree is seen from its other end). */
+__global__ void __launch_bounds__(kB, 4) kb_link(BatchK K)
+{
+    __shared__ uint32_t s_off[kB + 1];
+    __shared__ uint64_t s_beg[kB];
+    __shared__ uint32_t s_wsum[kWarpsB];
+    __shared__ unsigned long long s_t;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (;;) {
+        if (threadIdx.x == 0)
+            s_t = atomicAdd(K.grab, 1ull);
+        __syncthreads();
+        const unsigned long long t = s_t;
+        __syncthreads();
+        if (t >= K.tiles)
+            break;
+        const Tile T = tile_of(K, (uint32_t)t);
+        const uint32_t giant = K.skip ? __ldg(K.giants + T.g) : kNone;
+        for (uint32_t t0 = T.v0; t0 < T.v1; t0 += kB) {
+            const uint32_t v = t0 + threadIdx.x;
+            uint64_t beg = 0, end = 0;
+            if (v < T.v1 && (giant == kNone || cc_ldp(T.parent, v) != giant))
+                row_bounds(T, v, beg, end);
+            uint64_t deg = end - beg;
+            if (deg > K.heavy_deg) {
+                const uint32_t slot = atomicAdd(K.heavy_count, 1u);
+                if (slot < K.heavy_cap) {
+                    K.heavy_list[slot] = ((uint64_t)T.g << 32) | v;
+                    deg = 0;
+                }
+            }
+            unsigned big = __ballot_sync(0xffffffffu, deg >= K.warp_deg);
+            while (big) {
+                const int src = __ffs(big) - 1;
+                big &= big - 1;
+                const uint32_t vv = __shfl_sync(0xffffffffu, v, src);
+                const uint64_t bb = __shfl_sync(0xffffffffu, beg, src);
+                const uint64_t ee = __shfl_sync(0xffffffffu, end, src);
+                warp_row(T, vv, bb, ee, lane);
+            }
+            const uint32_t small = deg < K.warp_deg ? (uint32_t)deg : 0u;
+            uint32_t incl = small;
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o)
+                    incl += y;
+            }
+            if (lane == 31)
+                s_wsum[warp] = incl;
+            s_beg[threadIdx.x] = beg;
+            __syncthreads();
+            uint32_t wpre = 0, total = 0;
+#pragma unroll
+            for (int w = 0; w < kWarpsB; ++w) {
+                const uint32_t x = s_wsum[w];
+                wpre += (w < warp) ? x : 0u;
+                total += x;
+            }
+            s_off[threadIdx.x] = wpre + incl - small;
+            if (threadIdx.x == 0)
+                s_off[kB] = total;
+            __syncthreads();
+            for (uint32_t e = threadIdx.x; e < total; e += kB) {
+                int lo = 0, hi = kB;
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) >> 1;
+                    if (s_off[mid] <= e)
+                        lo = mid;
+                    else
+                        hi = mid;
+                }
+                const uint32_t u = __ldg(T.col + s_beg[lo] + (e - s_off[lo]));
+                if (u < T.n)
+                    cc_link(T.parent, t0 + (uint32_t)lo, u);
+            }
+            __syncthreads();
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kB) kb_heavy(BatchK K)
+{
+    uint32_t cnt = *K.heavy_count;
+    if (cnt > K.heavy_cap)
+        cnt = K.heavy_cap;
+    const int lane = threadIdx.x & 31;
+    cc_for_pieces(
+        cnt, kPiece,
+        [&](uint32_t h, uint64_t &b, uint64_t &e) {
+            const uint64_t gv = K.heavy_list[h];
+            const uint32_t g = (uint32_t)(gv >> 32), v = (uint32_t)gv;
+            const uint64_t vb = __ldg(K.vtx_off + g);
+            const uint64_t m = __ldg(K.edge_off + g + 1) - __ldg(K.edge_off + g);
+            const uint64_t *rp = K.row_ptr + vb + g;
+            b = __ldg(rp + v);
+            e = __ldg(rp + v + 1);
+            if (e > m)
+                e = m;
+            if (b > e)
+                b = e;
+        },
+        [&](uint32_t h, uint64_t jb, uint64_t je) {
+            const uint64_t gv = K.heavy_list[h];
+            const uint32_t g = (uint32_t)(gv >> 32), v = (uint32_t)gv;
+            const uint64_t vb = __ldg(K.vtx_off + g);
+            const uint32_t n = (uint32_t)(__ldg(K.vtx_off + g + 1) - vb);
+            const uint32_t *col = K.col + __ldg(K.edge_off + g);
+            uint32_t *parent = K.labels + vb;
+            for (uint64_t j0 = jb; j0 < je; j0 += 32) {
+                const uint64_t j = j0 + lane;
+                uint32_t u[1] = {0};
+                bool ok[1] = {false};
+                if (j < je) {
+                    u[0] = __ldg(col + j);
+                    ok[0] = u[0] < n;
+                }
+                cc_warp_link_min_first<1>(parent, v, u, ok, lane);
+            }
+        });
+}
+
+__global__ void __launch_bounds__(kB) kb_final(BatchK K)
+{
+    __shared__ uint32_t s_c[kWarpsB];
+    for (uint32_t t = blockIdx.x; t < K.tiles; t += gridDim.x) {
+        const Tile T = tile_of(K, t);
+        uint32_t c = 0;
+        for (uint32_t v = T.v0 + threadIdx.x; v < T.v1; v += kB) {
+            const uint32_t r = cc_find(T.parent, v);
+            if (r != v)
+                T.parent[v] = r;
+            c += r == v;
+        }
+        c = __reduce_add_sync(0xffffffffu, c);
+        if ((threadIdx.x & 31) == 0)
+            s_c[threadIdx.x >> 5] = c;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t sum = 0;
+            for (int w = 0; w < kWarpsB; ++w)
+                sum += s_c[w];
+            if (sum)
+                atomicAdd(K.comps + T.g, sum);
+            const uint32_t ntiles = (T.n + K.tile - 1) / K.tile;
+            __threadfence();
+            if (atomicAdd(K.tiles_done + T.g, 1u) + 1 == ntiles)
+                atomicExch(K.done + T.g, 1u);
+        }
+        __syncthreads();
+    }
+}
+
+/* ------------------------------------------------------------------ host */
+
+struct ClassPlan {
+    ccgpu_batch_class_opts o;
+    std::vector<uint32_t> graphs;  /* host copy of the class's graph list */
+    uint64_t vertices = 0, entries = 0;
+    uint32_t *d_graphs = nullptr;
+    uint32_t *d_tile_g = nullptr, *d_tile_v0 = nullptr;
+    uint32_t tiles = 0;
+    uint32_t tiles_for = 0;        /* tile size the tile list was built for */
+    unsigned long long *d_cnt = nullptr; /* [0] grab, [1] heavy count */
+    uint64_t *d_heavy = nullptr;
+    uint32_t heavy_cap = 0;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev = nullptr;
+};
+
+} // namespace
+
+struct ccgpu_batch_plan {
+    ccgpu_ctx *ctx;
+    uint32_t G;
+    std::vector<uint64_t> vtx_off, edge_off;
+    ccgpu_batch_tuning tune;
+    uint64_t *d_vtx_off = nullptr, *d_edge_off = nullptr;
+    const uint64_t *d_row_ptr;
+    const uint32_t *d_col;
+    uint32_t *d_labels;
+    uint32_t *d_giants = nullptr, *d_comps = nullptr, *d_tiles_done = nullptr, *d_done = nullptr;
+    ClassPlan cls[CCGPU_BATCH_CLASSES];
+    cudaEvent_t fork = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int kernels = 0;
+    int sms = 148;
+};
+
+namespace {
+
+int class_of(const ccgpu_batch_tuning &t, uint64_t n, uint64_t m)
+{
+    const double avg = n ? (double)m / (double)n : 0.0;
+    int c = 0;
+    while (c < CCGPU_BATCH_CLASSES - 1 && avg >= t.class_bounds[c])
+        ++c;
+    return c;
+}
+
+int check_class_opts(const ccgpu_batch_class_opts &o)
+{
+    if (o.sample_rounds < 0 || o.sample_rounds > 4)
+        return ccgpu_set_error(CCGPU_ERR_INVALID, "batch: sample_rounds %d not in 0..4",
+                               o.sample_rounds);
+    if (o.tile < 256 || o.tile > (1 << 20) || (o.tile & (o.tile - 1)))
+        return ccgpu_set_error(CCGPU_ERR_INVALID,
+                               "batch: tile %d is not a power of two in 256..2^20", o.tile);
+    if (o.warp_degree < 2 || o.warp_degree > 1024)
+        return ccgpu_set_error(CCGPU_ERR_INVALID, "batch: warp_degree %d not in 2..1024",
+                               o.warp_degree);
+    return CCGPU_OK;
+}
+
+/* (Re)builds the tile list of class c for its current tile size. */
+int build_tiles(ccgpu_batch_plan *p, int c)
+{
+    ClassPlan &C = p->cls[c];
+    const uint32_t T = (uint32_t)C.o.tile;
+    if (T == 0)
+        return ccgpu_set_error(CCGPU_ERR_INVALID, "batch: tile size 0");
+    if (C.d_tile_g && C.tiles_for == T)
+        return CCGPU_OK;
+    std::vector<uint32_t> tg, tv;
+    for (uint32_t g : C.graphs) {
+        const uint64_t n = p->vtx_off[g + 1] - p->vtx_off[g];
+        for (uint64_t v0 = 0; v0 < n; v0 += T) {
+            tg.push_back(g);
+            tv.push_back((uint32_t)v0);
+        }
+    }
+    cudaFree(C.d_tile_g);
+    cudaFree(C.d_tile_v0);
+    C.d_tile_g = C.d_tile_v0 = nullptr;
+    C.tiles = (uint32_t)tg.size();
+    C.tiles_for = T;
+    const size_t bytes = (tg.size() ? tg.size() : 1) * sizeof(uint32_t);
+    CC_CUDA(cudaMalloc((void **)&C.d_tile_g, bytes));
+    CC_CUDA(cudaMalloc((void **)&C.d_tile_v0, bytes));
+    if (!tg.empty()) {
+        CC_CUDA(cudaMemcpy(C.d_tile_g, tg.data(), tg.size() * 4, cudaMemcpyHostToDevice));
+        CC_CUDA(cudaMemcpy(C.d_tile_v0, tv.data(), tv.size() * 4, cudaMemcpyHostToDevice));
+    }
+    return CCGPU_OK;
+}
+
+BatchK kargs(ccgpu_batch_plan *p, int c)
+{
+    ClassPlan &C = p->cls[c];
+    BatchK K;
+    K.vtx_off = p->d_vtx_off;
+    K.edge_off = p->d_edge_off;
+    K.row_ptr = p->d_row_ptr;
+    K.col = p->d_col;
+    K.labels = p->d_labels;
+    K.tile_g = C.d_tile_g;
+    K.tile_v0 = C.d_tile_v0;
+    K.tiles = C.tiles;
+    K.tile = (uint32_t)C.o.tile;
+    K.graphs = C.d_graphs;
+    K.ngraphs = (uint32_t)C.graphs.size();
+    K.giants = p->d_giants;
+    K.comps = p->d_comps;
+    K.tiles_done = p->d_tiles_done;
+    K.done = p->d_done;
+    K.grab = C.d_cnt;
+    K.heavy_count = (uint32_t *)(C.d_cnt + 1);
+    K.heavy_list = C.d_heavy;
+    K.heavy_cap = C.heavy_cap;
+    K.heavy_deg = (uint32_t)p->tune.heavy_degree;
+    K.warp_deg = (uint32_t)C.o.warp_degree;
+    K.skip = C.o.sample_rounds > 0;
+    return K;
+}
+
+/* Enqueues class c's whole solve on stream st. */
+int enqueue_class(ccgpu_batch_plan *p, int c, cudaStream_t st, int *kernels)
+{
+    ClassPlan &C = p->cls[c];
+    if (C.graphs.empty() || C.tiles == 0)
+        return CCGPU_OK;
+    ccgpu_ctx *ctx = p->ctx;
+    const BatchK K = kargs(p, c);
+    const unsigned tb = cc_blocks(C.tiles, 1, (unsigned)p->sms * 8);
+    int k = 0;
+    CC_CUDA(cudaMemsetAsync(C.d_cnt, 0, 2 * sizeof(unsigned long long), st));
+    CC_KLAUNCH(ctx, CCK_BATCH_INIT, kb_init, tb, kB, 0, st, K);
+    ++k;
+    const int rounds = C.o.sample_rounds;
+    for (int r = 0; r < rounds; ++r) {
+        CC_KLAUNCH(ctx, CCK_BATCH_SAMPLE, kb_sample, tb, kB, 0, st, K, r);
+        ++k;
+        if (C.o.cadence || r + 1 == rounds) {
+            CC_KLAUNCH(ctx, CCK_BATCH_COMPRESS, kb_compress, tb, kB, 0, st, K);
+            ++k;
+        }
+    }
+    if (rounds > 0) {
+        const unsigned gb = cc_blocks(C.graphs.size(), 1, (unsigned)p->sms * 2);
+        CC_KLAUNCH(ctx, CCK_BATCH_GIANT, kb_giant, gb, 1024, 0, st, K, 0x5eed1234u);
+        ++k;
+    }
+    CC_KLAUNCH(ctx, CCK_BATCH_LINK, kb_link, (unsigned)p->sms * 4, kB, 0, st, K);
+    CC_KLAUNCH(ctx, CCK_BATCH_HEAVY, kb_heavy, (unsigned)p->sms * 4, kB, 0, st, K);
+    CC_KLAUNCH(ctx, CCK_BATCH_FINAL, kb_final, tb, kB, 0, st, K);
+    k += 3;
+    if (kernels)
+        *kernels += k;
+    return CCGPU_OK;
+}
+
+/* The whole batch on `st`: per-graph outputs cleared, then every class on
+ * its own stream forked from st and joined back. */
+int enqueue_all(ccgpu_batch_plan *p, cudaStream_t st, int *kernels)
+{
+    const size_t gbytes = (size_t)(p->G ? p->G : 1) * sizeof(uint32_t);
+    CC_CUDA(cudaMemsetAsync(p->d_comps, 0, gbytes, st));
+    CC_CUDA(cudaMemsetAsync(p->d_tiles_done, 0, gbytes, st));
+    CC_CUDA(cudaMemsetAsync(p->d_done, 0, gbytes, st));
+    CC_CUDA(cudaEventRecord(p->fork, st));
+    for (int c = 0; c < CCGPU_BATCH_CLASSES; ++c) {
+        ClassPlan &C = p->cls[c];
+        if (C.graphs.empty())
+            continue;
+        CC_CUDA(cudaStreamWaitEvent(C.st, p->fork, 0));
+        CC_TRY(enqueue_class(p, c, C.st, kernels));
+        CC_CUDA(cudaEventRecord(C.ev, C.st));
+        CC_CUDA(cudaStreamWaitEvent(st, C.ev, 0));
+    }
+    return CCGPU_OK;
+}
+
+void drop_graph(ccgpu_batch_plan *p)
+{
+    if (p->exec)
+        cudaGraphExecDestroy(p->exec);
+    if (p->graph)
+        cudaGraphDestroy(p->graph);
+    p->exec = nullptr;
+    p->graph = nullptr;
+}
+
+int capture(ccgpu_batch_plan *p)
+{
+    drop_graph(p);
+    cudaStream_t cs = nullptr;
+    CC_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    int kernels = 0;
+    int rc = CCGPU_OK;
+    /* the launch profiler would record events into the graph: off while
+     * capturing */
+    struct cc_prof *saved = p->ctx->prof;
+    p->ctx->prof = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        rc = ccgpu_cuda_fail(e, "cudaStreamBeginCapture", __FILE__, __LINE__);
+    } else {
+        rc = enqueue_all(p, cs, &kernels);
+        cudaGraph_t g = nullptr;
+        e = cudaStreamEndCapture(cs, &g);
+        if (rc == CCGPU_OK && e != cudaSuccess)
+            rc = ccgpu_cuda_fail(e, "cudaStreamEndCapture", __FILE__, __LINE__);
+        if (rc == CCGPU_OK) {
+            e = cudaGraphInstantiate(&p->exec, g, 0);
+            if (e != cudaSuccess)
+                rc = ccgpu_cuda_fail(e, "cudaGraphInstantiate", __FILE__, __LINE__);
+            p->graph = g;
+        } else if (g) {
+            cudaGraphDestroy(g);
+        }
+    }
+    p->ctx->prof = saved;
+    cudaStreamDestroy(cs);
+    if (rc == CCGPU_OK)
+        p->kernels = kernels;
+    return rc;
+}
+
+int alloc_class_scratch(ccgpu_batch_plan *p, int c)
+{
+    ClassPlan &C = p->cls[c];
+    uint64_t cap = C.entries / (uint64_t)p->tune.heavy_degree + 1;
+    if (cap > C.vertices + 1)
+        cap = C.vertices + 1;
+    if (cap > 0xffffffffu)
+        cap = 0xffffffffu;
+    C.heavy_cap = (uint32_t)cap;
+    CC_CUDA(cudaMalloc((void **)&C.d_cnt, 256));
+    CC_CUDA(cudaMalloc((void **)&C.d_heavy, cap * sizeof(uint64_t)));
+    const size_t gb = (C.graphs.size() ? C.graphs.size() : 1) * sizeof(uint32_t);
+    CC_CUDA(cudaMalloc((void **)&C.d_graphs, gb));
+    if (!C.graphs.empty())
+        CC_CUDA(cudaMemcpy(C.d_graphs, C.graphs.data(), C.graphs.size() * 4,
+                           cudaMemcpyHostToDevice));
+    CC_CUDA(cudaStreamCreateWithFlags(&C.st, cudaStreamNonBlocking));
+    CC_CUDA(cudaEventCreateWithFlags(&C.ev, cudaEventDisableTiming));
+    return build_tiles(p, c);
+}
+
+int plan_setup(ccgpu_batch_plan *p, const ccgpu_batch *b)
+{
+    const uint32_t G = p->G;
+    p->vtx_off.assign(b->h_vtx_off, b->h_vtx_off + G + 1);
+    p->edge_off.assign(b->h_edge_off, b->h_edge_off + G + 1);
+    if (p->vtx_off[0] != 0 || p->edge_off[0] != 0)
+        return ccgpu_set_error(CCGPU_ERR_INVALID, "batch: offsets must start at 0");
+    for (uint32_t g = 0; g < G; ++g) {
+        if (p->vtx_off[g + 1] < p->vtx_off[g] || p->edge_off[g + 1] < p->edge_off[g])
+            return ccgpu_set_error(CCGPU_ERR_INVALID, "batch: offsets of graph %u decrease", g);
+        if (p->vtx_off[g + 1] - p->vtx_off[g] >= 0xffffffffull)
+            return ccgpu_set_error(CCGPU_ERR_LIMIT, "batch: graph %u has 2^32-1 or more vertices",
+                                   g);
+        const uint64_t n = p->vtx_off[g + 1] - p->vtx_off[g];
+        const uint64_t m = p->edge_off[g + 1] - p->edge_off[g];
+        ClassPlan &C = p->cls[class_of(p->tune, n, m)];
+        C.graphs.push_back(g);
+        C.vertices += n;
+        C.entries += m;
+    }
+    const size_t ob = (size_t)(G + 1) * sizeof(uint64_t);
+    CC_CUDA(cudaMalloc((void **)&p->d_vtx_off, ob));
+    CC_CUDA(cudaMalloc((void **)&p->d_edge_off, ob));
+    CC_CUDA(cudaMemcpy(p->d_vtx_off, p->vtx_off.data(), ob, cudaMemcpyHostToDevice));
+    CC_CUDA(cudaMemcpy(p->d_edge_off, p->edge_off.data(), ob, cudaMemcpyHostToDevice));
+    const size_t gb = (size_t)(G ? G : 1) * sizeof(uint32_t);
+    CC_CUDA(cudaMalloc((void **)&p->d_giants, gb));
+    CC_CUDA(cudaMalloc((void **)&p->d_comps, gb));
+    CC_CUDA(cudaMalloc((void **)&p->d_tiles_done, gb));
+    CC_CUDA(cudaMalloc((void **)&p->d_done, gb));
+    CC_CUDA(cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming));
+    for (int c = 0; c < CCGPU_BATCH_CLASSES; ++c) {
+        p->cls[c].o = p->tune.cls[c];
+        if (!p->cls[c].graphs.empty())
+            CC_TRY(alloc_class_scratch(p, c));
+    }
+    return CCGPU_OK;
+}
+
+/* Device time of `reps` solves of class c alone (after one warm-up). */
+int time_class(ccgpu_batch_plan *p, int c, cudaStream_t st, int reps, float *ms)
+{
+    cudaEvent_t a = nullptr, z = nullptr;
+    CC_CUDA(cudaEventCreate(&a));
+    CC_CUDA(cudaEventCreate(&z));
+    int rc = enqueue_class(p, c, st, nullptr);
+    if (rc == CCGPU_OK && cudaEventRecord(a, st) != cudaSuccess)
+        rc = ccgpu_set_error(CCGPU_ERR_CUDA, "batch autotune: event record failed");
+    for (int i = 0; rc == CCGPU_OK && i < reps; ++i)
+        rc = enqueue_class(p, c, st, nullptr);
+    if (rc == CCGPU_OK) {
+        cudaEventRecord(z, st);
+        cudaError_t e = cudaEventSynchronize(z);
+        if (e == cudaSuccess)
+            e = cudaEventElapsedTime(ms, a, z);
+        if (e != cudaSuccess)
+            rc = ccgpu_cuda_fail(e, "batch autotune timing", __FILE__, __LINE__);
+        *ms /= (float)reps;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(z);
+    return rc;
+}
+
+} // namespace
+
+/* ------------------------------------------------------------------ API */
+
+extern "C" void ccgpu_batch_tuning_default(ccgpu_batch_tuning *t)
+{
+    if (!t)
+        return;
+    memset(t, 0, sizeof(*t));
+    t->class_bounds[0] = 6.0f;
+    t->class_bounds[1] = 16.0f;
+    t->heavy_degree = 8192;
+    for (int c = 0; c < CCGPU_BATCH_CLASSES; ++c) {
+        t->cls[c].sample_rounds = 2;
+        t->cls[c].cadence = 1;
+        t->cls[c].tile = 4096;
+        t->cls[c].warp_degree = 32;
+    }
+}
+
+extern "C" int ccgpu_batch_plan_create(ccgpu_ctx *ctx, const ccgpu_batch *b,
+                                       const ccgpu_batch_tuning *tuning, ccgpu_batch_plan **out)
+{
+    if (!b || !out || !b->h_vtx_off || !b->h_edge_off)
+        return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_batch_plan_create: NULL argument");
+    *out = nullptr;
+    if (b->graphs == 0)
+        return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_batch_plan_create: empty batch");
+    if (!b->d_row_ptr || !b->d_labels || (b->h_edge_off[b->graphs] && !b->d_col))
+        return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_batch_plan_create: NULL device array");
+    CC_TRY(ccgpu_ctx_resolve(&ctx));
+    ccgpu_batch_tuning t;
+    if (tuning)
+        t = *tuning;
+    else
+        ccgpu_batch_tuning_default(&t);
+    if (t.heavy_degree < 32)
+        t.heavy_degree = 32;
+    for (int c = 0; c < CCGPU_BATCH_CLASSES; ++c)
+        CC_TRY(check_class_opts(t.cls[c]));
+    ccgpu_batch_plan *p = new ccgpu_batch_plan();
+    p->ctx = ctx;
+    p->G = b->graphs;
+    p->tune = t;
+    p->d_row_ptr = b->d_row_ptr;
+    p->d_col = b->d_col;
+    p->d_labels = b->d_labels;
+    p->sms = ctx->sm_count;
+    int rc = plan_setup(p, b);
+    if (rc != CCGPU_OK) {
+        ccgpu_batch_plan_destroy(p);
+        return rc;
+    }
+    *out = p;
+    return CCGPU_OK;
+}
+
+extern "C" int ccgpu_batch_plan_run(ccgpu_batch_plan *p, void *stream)
+{
+    if (!p)
+        return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_batch_plan_run: NULL plan");
+    return enqueue_all(p, (cudaStream_t)stream, nullptr);
+}
+
+extern "C" int ccgpu_batch_plan_launch(ccgpu_batch_plan *p, void *stream)
+{
+    if (!p)
+        return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_batch_plan_launch: NULL plan");
+    if (!p->exec)
+        CC_TRY(capture(p));
+    CC_CUDA(cudaGraphLaunch(p->exec, (cudaStream_t)stream));
+    return CCGPU_OK;
+}
+
+extern "C" int ccgpu_batch_plan_kernels(const ccgpu_batch_plan *p)
+{
+    return p ? p->kernels : 0;
+}
+
+extern "C" int ccgpu_batch_plan_tuning(const ccgpu_batch_plan *p, ccgpu_batch_tuning *out)
+{
+    if (!p || !out)
+        return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_batch_plan_tuning: NULL argument");
+    *out = p->tune;
+    return CCGPU_OK;
+}
+
+extern "C" int ccgpu_batch_plan_class_graphs(const ccgpu_batch_plan *p, uint32_t *counts)
+{
+    if (!p || !counts)
+        return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_batch_plan_class_graphs: NULL argument");
+    for (int c = 0; c < CCGPU_BATCH_CLASSES; ++c)
+        counts[c] = (uint32_t)p->cls[c].graphs.size();
+    return CCGPU_OK;
+}
+
+/* Coordinate descent per class over sampled neighbours, cadence, tile size
+ * and the warp-row threshold, each candidate timed on the class alone. */
+extern "C" int ccgpu_batch_plan_autotune(ccgpu_batch_plan *p, void *stream,
+                                         ccgpu_batch_tuning *chosen)
+{
+    if (!p)
+        return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_batch_plan_autotune: NULL plan");
+    cudaStream_t st = (cudaStream_t)stream;
+    struct cc_prof *saved = p->ctx->prof;
+    p->ctx->prof = nullptr;
+    int rc = CCGPU_OK;
+    for (int c = 0; c < CCGPU_BATCH_CLASSES && rc == CCGPU_OK; ++c) {
+        ClassPlan &C = p->cls[c];
+        if (C.graphs.empty())
+            continue;
+        ccgpu_batch_class_opts best = C.o;
+        float best_ms = 0.f;
+        rc = time_class(p, c, st, 3, &best_ms);
+        const int rounds[] = {0, 1, 2, 3};
+        const int tiles[] = {1024, 4096, 16384};
+        const int wdeg[] = {8, 16, 32, 64};
+        for (int axis = 0; axis < 4 && rc == CCGPU_OK; ++axis) {
+            const int *vals = axis == 0 ? rounds : axis == 2 ? tiles : axis == 3 ? wdeg : nullptr;
+            const int nv = axis == 0 ? 4 : axis == 1 ? 2 : axis == 2 ? 3 : 4;
+            for (int i = 0; i < nv && rc == CCGPU_OK; ++i) {
+                ccgpu_batch_class_opts cand = best;
+                if (axis == 0)
+                    cand.sample_rounds = vals[i];
+                else if (axis == 1)
+                    cand.cadence = i;
+                else if (axis == 2)
+                    cand.tile = vals[i];
+                else
+                    cand.warp_degree = vals[i];
+                if (!memcmp(&cand, &best, sizeof(cand)))
+                    continue;
+                C.o = cand;
+                rc = build_tiles(p, c);
+                float ms = 0.f;
+                if (rc == CCGPU_OK)
+                    rc = time_class(p, c, st, 3, &ms);
+                if (rc == CCGPU_OK && ms < best_ms) {
+                    best_ms = ms;
+                    best = cand;
+                }
+            }
+        }
+        C.o = best;
+        if (rc == CCGPU_OK)
+            rc = build_tiles(p, c);
+        p->tune.cls[c] = best;
+    }
+    p->ctx->prof = saved;
+    drop_graph(p);
+    if (rc == CCGPU_OK && chosen)
+        *chosen = p->tune;
+    return rc;
+}
+
+extern "C" int ccgpu_batch_plan_results(ccgpu_batch_plan *p, uint32_t *h_components,
+                                        uint32_t *h_done, void *stream)
+{
+    if (!p)
+        return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_batch_plan_results: NULL plan");
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t gb = (size_t)p->G * sizeof(uint32_t);
+    if (h_components)
+        CC_CUDA(cudaMemcpyAsync(h_components, p->d_comps, gb, cudaMemcpyDeviceToHost, st));
+    if (h_done)
+        CC_CUDA(cudaMemcpyAsync(h_done, p->d_done, gb, cudaMemcpyDeviceToHost, st));
+    CC_CUDA(cudaStreamSynchronize(st));
+    /* a graph without vertices has no tile: it is solved, with 0 components */
+    for (uint32_t g = 0; h_done && g < p->G; ++g)
+        if (p->vtx_off[g + 1] == p->vtx_off[g])
+            h_done[g] = 1;
+    return CCGPU_OK;
+}
+
+extern "C" void ccgpu_batch_plan_destroy(ccgpu_batch_plan *p)
+{
+    if (!p)
+        return;
+    drop_graph(p);
+    for (int c = 0; c < CCGPU_BATCH_CLASSES; ++c) {
+        ClassPlan &C = p->cls[c];
+        cudaFree(C.d_graphs);
+        cudaFree(C.d_tile_g);
+        cudaFree(C.d_tile_v0);
+        cudaFree(C.d_cnt);
+        cudaFree(C.d_heavy);
+        if (C.st)
+            cudaStreamDestroy(C.st);
+        if (C.ev)
+            cudaEventDestroy(C.ev);
+    }
+    if (p->fork)
+        cudaEventDestroy(p->fork);
+    cudaFree(p->d_vtx_off);
+    cudaFree(p->d_edge_off);
+    cudaFree(p->d_giants);
+    cudaFree(p->d_comps);
+    cudaFree(p->d_tiles_done);
+    cudaFree(p->d_done);
+    delete p;
+}
+
+extern "C" int ccgpu_batch_cc(ccgpu_ctx *ctx, const ccgpu_batch *b,
+                              const ccgpu_batch_tuning *tuning, uint32_t *h_components,
+                              void *stream)
+{
+    ccgpu_batch_plan *p = nullptr;
+    CC_TRY(ccgpu_batch_plan_create(ctx, b, tuning, &p));
+    int rc = ccgpu_batch_plan_run(p, stream);
+    if (rc == CCGPU_OK)
+        rc = ccgpu_batch_plan_results(p, h_components, nullptr, stream);
+    else
+        cudaStreamSynchronize((cudaStream_t)stream);
+    ccgpu_batch_plan_destroy(p);
+    return rc;
+}

@@ -84,6 +84,13 @@ enum {
     CCK_MISC,
     CCK_DIST_PAIRS_HEAVY,
     CCK_DIST_PAIRS_BITMAP,
+    CCK_BATCH_INIT,
+    CCK_BATCH_SAMPLE,
+    CCK_BATCH_COMPRESS,
+    CCK_BATCH_GIANT,
+    CCK_BATCH_LINK,
+    CCK_BATCH_HEAVY,
+    CCK_BATCH_FINAL,
     CCK_NUM
 };
 
@@ -315,6 +322,168 @@ __device__ __forceinline__ void cc_for_heavy_pieces(const uint32_t *list, uint32
             uint64_t jb = s_beg[lo] + (g - s_pre[lo]) * chunk;
             uint64_t je = jb + chunk < s_end[lo] ? jb + chunk : s_end[lo];
             fn(s_v[lo], jb, je);
+        }
+        __syncthreads();
+    }
+    (void)lane;
+}
+
+/* MurmurHash3 fmix32 finaliser (Appleby, public domain) as a sample mixer. */
+__device__ __forceinline__ uint32_t cc_mix32(uint32_t h)
+{
+    h ^= h >> 16;
+    h *= 0x85ebca6bu;
+    h ^= h >> 13;
+    h *= 0xc2b2ae35u;
+    h ^= h >> 16;
+    return h;
+}
+
+/* Most frequent value among the 1024 values of a 1024-thread block (one per
+ * thread, `val`); ties go to the smaller value, so the choice is
+ * deterministic.  Bitonic sort in shared memory, run lengths by binary
+ * search, then a max-reduction of (count, ~value).  Every thread must call
+ * it; all of them get the result. */
+__device__ __forceinline__ uint32_t cc_block_mode1024(uint32_t val, uint32_t *s,
+                                                      unsigned long long *s_best)
+{
+    const uint32_t i = threadIdx.x;
+    s[i] = val;
+    __syncthreads();
+    for (uint32_t k = 2; k <= 1024; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            uint32_t ij = i ^ j;
+            if (ij > i) {
+                uint32_t a = s[i], b = s[ij];
+                bool up = (i & k) == 0;
+                if ((a > b) == up) {
+                    s[i] = b;
+                    s[ij] = a;
+                }
+            }
+            __syncthreads();
+        }
+    }
+    uint32_t cnt = 0;
+    val = s[i];
+    if (i == 0 || s[i - 1] != val) {
+        uint32_t a = i, b = 1024;
+        while (a < b) {
+            uint32_t mid = (a + b) >> 1;
+            if (s[mid] <= val)
+                a = mid + 1;
+            else
+                b = mid;
+        }
+        cnt = a - i;
+    }
+    unsigned long long key = ((unsigned long long)cnt << 32) | (uint32_t)~val;
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
+        key = other > key ? other : key;
+    }
+    if ((i & 31) == 0)
+        s_best[i >> 5] = key;
+    __syncthreads();
+    key = s_best[i & 31];
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
+        key = other > key ? other : key;
+    }
+    __syncthreads();
+    return ~(uint32_t)key;
+}
+
+/* Warp-cooperative link of v with up to K entries per lane (all 32 lanes
+ * call it).  Hooking every entry's root under v's root one by one piles the
+ * CAS attempts of the whole row onto v's root (a herd: one wins per round,
+ * the rest retry).  Instead the warp first hooks v's tree under the
+ * smallest root among its entries; v's root is then no larger than any
+ * entry's root, so the remaining hooks go to each entry's own root. */
+template <int K>
+__device__ __forceinline__ void cc_warp_link_min_first(uint32_t *parent, uint32_t v,
+                                                       const uint32_t *u, const bool *ok,
+                                                       int lane)
+{
+    uint32_t r[K];
+    uint32_t mn = 0xffffffffu;
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+        r[i] = ok[i] ? cc_find(parent, u[i]) : 0xffffffffu;
+        mn = r[i] < mn ? r[i] : mn;
+    }
+    mn = __reduce_min_sync(0xffffffffu, mn);
+    if (mn == 0xffffffffu)
+        return;
+    if (lane == 0) {
+        uint32_t rv = cc_find(parent, v);
+        if (rv != mn)
+            cc_link_roots(parent, rv, mn);
+    }
+    __syncwarp();
+    uint32_t rv = cc_find(parent, v);
+#pragma unroll
+    for (int i = 0; i < K; ++i)
+        if (ok[i] && r[i] != rv)
+            cc_link_roots(parent, r[i], rv);
+}
+
+/* Generalisation of cc_for_heavy_pieces to rows whose bounds come from a
+ * functor: bounds(h, &beg, &end) gives the entry range of list item h,
+ * fn(h, jb, je) is called by all 32 lanes of a warp for each piece.  Piece g
+ * of a batch of 256 items goes to warp g mod (all warps).  Must be called
+ * by every thread of a 256-thread block. */
+template <typename Bounds, typename Fn>
+__device__ __forceinline__ void cc_for_pieces(uint32_t count, uint64_t chunk, Bounds bounds,
+                                              Fn fn)
+{
+    __shared__ uint64_t s_pre[257];
+    __shared__ uint64_t s_beg[256], s_end[256];
+    __shared__ uint64_t s_w[8];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t gwarp = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp;
+    const uint64_t nwarps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+    for (uint32_t b0 = 0; b0 < count; b0 += 256) {
+        const uint32_t h = b0 + threadIdx.x;
+        uint64_t pieces = 0;
+        if (h < count) {
+            uint64_t b = 0, e = 0;
+            bounds(h, b, e);
+            s_beg[threadIdx.x] = b;
+            s_end[threadIdx.x] = e;
+            pieces = (e - b + chunk - 1) / chunk;
+        }
+        uint64_t incl = pieces;
+        for (int o = 1; o < 32; o <<= 1) {
+            uint64_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o)
+                incl += y;
+        }
+        if (lane == 31)
+            s_w[warp] = incl;
+        __syncthreads();
+        uint64_t pre = 0, total = 0;
+        for (int w = 0; w < 8; ++w) {
+            pre += (w < warp) ? s_w[w] : 0ull;
+            total += s_w[w];
+        }
+        s_pre[threadIdx.x] = pre + incl - pieces;
+        if (threadIdx.x == 0)
+            s_pre[256] = total;
+        __syncthreads();
+        const int rows = count - b0 < 256u ? (int)(count - b0) : 256;
+        for (uint64_t g = gwarp; g < total; g += nwarps) {
+            int lo = 0, hi = rows;
+            while (hi - lo > 1) {
+                int mid = (lo + hi) >> 1;
+                if (s_pre[mid] <= g)
+                    lo = mid;
+                else
+                    hi = mid;
+            }
+            uint64_t jb = s_beg[lo] + (g - s_pre[lo]) * chunk;
+            uint64_t je = jb + chunk < s_end[lo] ? jb + chunk : s_end[lo];
+            fn(b0 + (uint32_t)lo, jb, je);
         }
         __syncthreads();
     }

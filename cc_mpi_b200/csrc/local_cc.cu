@@ -52,17 +52,6 @@ __device__ __forceinline__ Rows row_of(const uint64_t *__restrict__ row_ptr, uin
     return {b, e};
 }
 
-/* MurmurHash3 fmix32 finaliser (Appleby, public domain) as a sample mixer. */
-__device__ __forceinline__ uint32_t mix32(uint32_t h)
-{
-    h ^= h >> 16;
-    h *= 0x85ebca6bu;
-    h ^= h >> 13;
-    h *= 0xc2b2ae35u;
-    h ^= h >> 16;
-    return h;
-}
-
 /* Index s with seg[s] <= v < seg[s+1] (seg ascending, nseg >= 1). */
 __device__ __forceinline__ uint32_t seg_of(const uint64_t *__restrict__ seg, uint32_t nseg,
                                            uint64_t v)
@@ -223,53 +212,11 @@ __global__ void __launch_bounds__(kGiantSamples) k_giant(const uint32_t *parent,
         return;
     }
     uint64_t size = hi - lo;
-    uint32_t h = mix32(i * 0x9e3779b9u + seed + blockIdx.x);
+    uint32_t h = cc_mix32(i * 0x9e3779b9u + seed + blockIdx.x);
     uint32_t v = (uint32_t)(lo + (((uint64_t)h * size) >> 32));
-    s[i] = cc_find_ro(parent, v);
-    __syncthreads();
-    for (uint32_t k = 2; k <= kGiantSamples; k <<= 1) {
-        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-            uint32_t ij = i ^ j;
-            if (ij > i) {
-                uint32_t a = s[i], b = s[ij];
-                bool up = (i & k) == 0;
-                if ((a > b) == up) {
-                    s[i] = b;
-                    s[ij] = a;
-                }
-            }
-            __syncthreads();
-        }
-    }
-    uint32_t cnt = 0, val = s[i];
-    if (i == 0 || s[i - 1] != val) {
-        uint32_t a = i, b = kGiantSamples;
-        while (a < b) {
-            uint32_t mid = (a + b) >> 1;
-            if (s[mid] <= val)
-                a = mid + 1;
-            else
-                b = mid;
-        }
-        cnt = a - i;
-    }
-    unsigned long long key = ((unsigned long long)cnt << 32) | (uint32_t)~val;
-    for (int o = 16; o > 0; o >>= 1) {
-        unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
-        key = other > key ? other : key;
-    }
-    if ((i & 31) == 0)
-        s_best[i >> 5] = key;
-    __syncthreads();
-    if (i < 32) {
-        key = s_best[i];
-        for (int o = 16; o > 0; o >>= 1) {
-            unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
-            key = other > key ? other : key;
-        }
-        if (i == 0)
-            out[blockIdx.x] = ~(uint32_t)key;
-    }
+    uint32_t mode = cc_block_mode1024(cc_find_ro(parent, v), s, s_best);
+    if (i == 0)
+        out[blockIdx.x] = mode;
 }
 
 struct LinkParams {
@@ -290,39 +237,6 @@ struct LinkParams {
     int vec;                   /* col is 16-byte aligned                    */
     const uint64_t *fseg;      /* segment filter offsets, NULL = off        */
 };
-
-/* Warp-cooperative link of v with up to K entries per lane (all 32 lanes
- * call it).  Hooking every entry's root under v's root one by one piles the
- * CAS attempts of the whole row onto v's root (a herd: one wins per round,
- * the rest retry).  Instead the warp first hooks v's tree under the
- * smallest root among its entries; v's root is then no larger than any
- * entry's root, so the remaining hooks go to each entry's own root. */
-template <int K>
-__device__ __forceinline__ void warp_link_min_first(uint32_t *parent, uint32_t v, const uint32_t *u,
-                                                    const bool *ok, int lane)
-{
-    uint32_t r[K];
-    uint32_t mn = 0xffffffffu;
-#pragma unroll
-    for (int i = 0; i < K; ++i) {
-        r[i] = ok[i] ? cc_find(parent, u[i]) : 0xffffffffu;
-        mn = r[i] < mn ? r[i] : mn;
-    }
-    mn = __reduce_min_sync(0xffffffffu, mn);
-    if (mn == 0xffffffffu)
-        return;
-    if (lane == 0) {
-        uint32_t rv = cc_find(parent, v);
-        if (rv != mn)
-            cc_link_roots(parent, rv, mn);
-    }
-    __syncwarp();
-    uint32_t rv = cc_find(parent, v);
-#pragma unroll
-    for (int i = 0; i < K; ++i)
-        if (ok[i] && r[i] != rv)
-            cc_link_roots(parent, r[i], rv);
-}
 
 /* One warp links v with row entries [beg, end) that fall in sp: 16-byte
  * column loads for the aligned body, scalar loads for head and tail, every
@@ -350,7 +264,7 @@ __device__ __forceinline__ void warp_link_row(const LinkParams &P, uint32_t v, u
             u[0] = __ldg(P.col + (s < head ? beg + s : body_end + (s - head)));
             ok[0] = in_span(sp, u[0]);
         }
-        warp_link_min_first<1>(P.parent, v, u, ok, lane);
+        cc_warp_link_min_first<1>(P.parent, v, u, ok, lane);
     }
     const uint4 *c4 = reinterpret_cast<const uint4 *>(P.col);
     for (uint64_t q0 = a / 4; q0 < body_end / 4; q0 += 32) {
@@ -367,7 +281,7 @@ __device__ __forceinline__ void warp_link_row(const LinkParams &P, uint32_t v, u
             for (int i = 0; i < 4; ++i)
                 ok[i] = in_span(sp, u[i]);
         }
-        warp_link_min_first<4>(P.parent, v, u, ok, lane);
+        cc_warp_link_min_first<4>(P.parent, v, u, ok, lane);
     }
 }
 
@@ -528,7 +442,7 @@ __global__ void __launch_bounds__(kBlock) k_link_heavy(LinkParams P)
                                     u[0] = __ldg(P.col + j);
                                     ok[0] = in_span(sp, u[0]);
                                 }
-                                warp_link_min_first<1>(P.parent, v, u, ok, lane);
+                                cc_warp_link_min_first<1>(P.parent, v, u, ok, lane);
                             }
                         });
 }

@@ -189,7 +189,8 @@ static const char *const kKernelNames[CCK_NUM] = {
     "sort_hist", "sort_scan", "sort_scatter", "dist_dedup", "dist_ghosts", "dist_plan",
     "merge_init", "merge_hook", "merge_upd", "merge_exch_pack", "merge_exch_scatter",
     "dist_labels", "dist_bounds", "scan", "batch", "misc", "dist_pairs_heavy",
-    "dist_pairs_bitmap"};
+    "dist_pairs_bitmap", "batch_init", "batch_sample", "batch_compress", "batch_giant",
+    "batch_link", "batch_heavy", "batch_final"};
 
 struct cc_prof {
     std::vector<cudaEvent_t> pool;

@@ -283,6 +283,78 @@ int ccgpu_local_cc_noalloc(const uint64_t *d_row_ptr, const uint32_t *d_col_idx,
 size_t ccgpu_local_cc_noalloc_capacity(void);
 size_t ccgpu_local_cc_noalloc_required(uint32_t n, uint64_t m, const ccgpu_cc_opts *opts);
 
+/* ------------------------------------------------------------------------
+ * Batched CC: many independent graphs in one solve.  No counterpart in the
+ * reference, which solves one graph per call
+ * (compute_connected_components_pthreads, include/cc.h:27-28); every graph
+ * of a batch gets exactly that call's labels (minimum local vertex id of
+ * each component of its own graph).
+ *
+ * Packed CSR-of-CSRs, G graphs:
+ *   h_vtx_off[G+1], h_edge_off[G+1]  host prefix sums of n_g and m_g
+ *   d_row_ptr  graph g's n_g + 1 local row pointers (0 .. m_g) at
+ *              d_row_ptr[vtx_off[g] + g]
+ *   d_col      graph g's local neighbour ids at d_col[edge_off[g]]
+ *   d_labels   out: graph g's labels at d_labels[vtx_off[g]]
+ * Graphs are grouped into CCGPU_BATCH_CLASSES degree classes by mean row
+ * length (m_g / n_g against class_bounds); each class has its own schedule
+ * (sampled neighbours, shortcut cadence, tile size, warp-row threshold),
+ * tile list and stream, so classes run concurrently.  A plan's launch
+ * replays the whole batch as one CUDA graph (captured on the first launch).
+ * ---------------------------------------------------------------------- */
+#define CCGPU_BATCH_CLASSES 3
+
+typedef struct {
+    uint32_t graphs;
+    const uint64_t *h_vtx_off;
+    const uint64_t *h_edge_off;
+    const uint64_t *d_row_ptr;
+    const uint32_t *d_col;
+    uint32_t *d_labels;
+} ccgpu_batch;
+
+typedef struct {
+    int sample_rounds; /* neighbours linked per vertex before the giant skip (0..4) */
+    int cadence;       /* 1: shortcut pass after every sampled neighbour            */
+    int tile;          /* vertices per tile, power of two in 256..2^20              */
+    int warp_degree;   /* rows with at least this many entries get a whole warp     */
+} ccgpu_batch_class_opts;
+
+typedef struct {
+    float class_bounds[CCGPU_BATCH_CLASSES - 1]; /* mean-row-length cut points (6, 16) */
+    int heavy_degree;                            /* rows above it are queued (8192)    */
+    ccgpu_batch_class_opts cls[CCGPU_BATCH_CLASSES];
+} ccgpu_batch_tuning;
+
+void ccgpu_batch_tuning_default(ccgpu_batch_tuning *t);
+
+typedef struct ccgpu_batch_plan ccgpu_batch_plan;
+/* Validates the offsets, builds the classes' tile lists and scratch (owned
+ * by the plan).  tuning NULL = defaults. */
+int ccgpu_batch_plan_create(ccgpu_ctx *ctx, const ccgpu_batch *b, const ccgpu_batch_tuning *tuning,
+                            ccgpu_batch_plan **out);
+/* Enqueues the solve kernel by kernel on `stream` (asynchronous). */
+int ccgpu_batch_plan_run(ccgpu_batch_plan *p, void *stream);
+/* Enqueues the solve as one CUDA graph launch on `stream` (asynchronous). */
+int ccgpu_batch_plan_launch(ccgpu_batch_plan *p, void *stream);
+/* Kernels one graph launch runs (0 before the first launch). */
+int ccgpu_batch_plan_kernels(const ccgpu_batch_plan *p);
+/* Times candidate schedules per class on the device (coordinate descent over
+ * sample_rounds, cadence, tile, warp_degree) and keeps the fastest; the
+ * chosen tuning is written to *chosen (may be NULL).  Synchronous. */
+int ccgpu_batch_plan_autotune(ccgpu_batch_plan *p, void *stream, ccgpu_batch_tuning *chosen);
+int ccgpu_batch_plan_tuning(const ccgpu_batch_plan *p, ccgpu_batch_tuning *out);
+/* Graphs per class (array of CCGPU_BATCH_CLASSES). */
+int ccgpu_batch_plan_class_graphs(const ccgpu_batch_plan *p, uint32_t *counts);
+/* Per-graph component counts and done flags of the last solve (host arrays
+ * of G entries, either may be NULL).  Synchronous on `stream`. */
+int ccgpu_batch_plan_results(ccgpu_batch_plan *p, uint32_t *h_components, uint32_t *h_done,
+                             void *stream);
+void ccgpu_batch_plan_destroy(ccgpu_batch_plan *p);
+/* One-shot: plan, solve, per-graph component counts (may be NULL), destroy. */
+int ccgpu_batch_cc(ccgpu_ctx *ctx, const ccgpu_batch *b, const ccgpu_batch_tuning *tuning,
+                   uint32_t *h_components, void *stream);
+
 /* Number of v with d_labels[v] == v (one root per component when the labels
  * are min-id labels).  Synchronous; result in *count. */
 int ccgpu_count_roots(ccgpu_ctx *ctx, const uint32_t *d_labels, uint32_t n,
