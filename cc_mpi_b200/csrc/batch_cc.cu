@@ -37,13 +37,11 @@
  *   kb_final     labels[v] = root(v); per-graph root count, and the graph's
  *                done flag set by its last tile
  */
-#include <algorithm>
-#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <vector>
 
-#include "ccgpu_internal.h"
+#include "batch_core.h"
 
 namespace {
 
@@ -53,8 +51,7 @@ constexpr uint64_t kPiece = 512;
 constexpr uint32_t kNone = 0xffffffffu;
 
 struct BatchK {
-    const uint64_t *vtx_off;  /* [G+1] */
-    const uint64_t *edge_off; /* [G+1] */
+    const BGraph *gr;         /* [G] graph descriptors           */
     const uint64_t *row_ptr;
     const uint32_t *col;
     uint32_t *labels;
@@ -79,7 +76,7 @@ struct BatchK {
 
 struct Tile {
     uint32_t g, v0, v1, n;
-    uint64_t ebase, m;
+    uint64_t m;
     const uint64_t *rp;
     uint32_t *parent;
     const uint32_t *col;
@@ -90,14 +87,13 @@ __device__ __forceinline__ Tile tile_of(const BatchK &K, uint32_t t)
     Tile T;
     T.g = __ldg(K.tile_g + t);
     T.v0 = __ldg(K.tile_v0 + t);
-    const uint64_t vb = __ldg(K.vtx_off + T.g);
-    T.n = (uint32_t)(__ldg(K.vtx_off + T.g + 1) - vb);
+    const BGraph *d = K.gr + T.g;
+    T.n = __ldg(&d->n);
     T.v1 = T.v0 + K.tile < T.n ? T.v0 + K.tile : T.n;
-    T.ebase = __ldg(K.edge_off + T.g);
-    T.m = __ldg(K.edge_off + T.g + 1) - T.ebase;
-    T.rp = K.row_ptr + vb + T.g;
-    T.parent = K.labels + vb;
-    T.col = K.col + T.ebase;
+    T.m = __ldg(&d->m);
+    T.rp = K.row_ptr + __ldg(&d->rp);
+    T.parent = K.labels + __ldg(&d->lab);
+    T.col = K.col + __ldg(&d->col);
     return T;
 }
 
@@ -159,8 +155,7 @@ __global__ void __launch_bounds__(1024) kb_giant(BatchK K, uint32_t seed)
     __shared__ unsigned long long s_best[32];
     for (uint32_t i = blockIdx.x; i < K.ngraphs; i += gridDim.x) {
         const uint32_t g = __ldg(K.graphs + i);
-        const uint64_t vb = __ldg(K.vtx_off + g);
-        const uint32_t n = (uint32_t)(__ldg(K.vtx_off + g + 1) - vb);
+        const uint32_t n = __ldg(&K.gr[g].n);
         if (n == 0) {
             if (threadIdx.x == 0)
                 K.giants[g] = kNone;
@@ -168,7 +163,7 @@ __global__ void __launch_bounds__(1024) kb_giant(BatchK K, uint32_t seed)
         }
         const uint32_t h = cc_mix32(threadIdx.x * 0x9e3779b9u + seed + g);
         const uint32_t v = (uint32_t)(((uint64_t)h * n) >> 32);
-        const uint32_t mode = cc_block_mode1024(cc_find_ro(K.labels + vb, v), s, s_best);
+        const uint32_t mode = cc_block_mode1024(cc_find_ro(K.labels + __ldg(&K.gr[g].lab), v), s, s_best);
         if (threadIdx.x == 0)
             K.giants[g] = mode;
     }
@@ -311,9 +306,8 @@ __global__ void __launch_bounds__(kB) kb_heavy(BatchK K)
         [&](uint32_t h, uint64_t &b, uint64_t &e) {
             const uint64_t gv = K.heavy_list[h];
             const uint32_t g = (uint32_t)(gv >> 32), v = (uint32_t)gv;
-            const uint64_t vb = __ldg(K.vtx_off + g);
-            const uint64_t m = __ldg(K.edge_off + g + 1) - __ldg(K.edge_off + g);
-            const uint64_t *rp = K.row_ptr + vb + g;
+            const uint64_t m = __ldg(&K.gr[g].m);
+            const uint64_t *rp = K.row_ptr + __ldg(&K.gr[g].rp);
             b = __ldg(rp + v);
             e = __ldg(rp + v + 1);
             if (e > m)
@@ -324,10 +318,9 @@ __global__ void __launch_bounds__(kB) kb_heavy(BatchK K)
         [&](uint32_t h, uint64_t jb, uint64_t je) {
             const uint64_t gv = K.heavy_list[h];
             const uint32_t g = (uint32_t)(gv >> 32), v = (uint32_t)gv;
-            const uint64_t vb = __ldg(K.vtx_off + g);
-            const uint32_t n = (uint32_t)(__ldg(K.vtx_off + g + 1) - vb);
-            const uint32_t *col = K.col + __ldg(K.edge_off + g);
-            uint32_t *parent = K.labels + vb;
+            const uint32_t n = __ldg(&K.gr[g].n);
+            const uint32_t *col = K.col + __ldg(&K.gr[g].col);
+            uint32_t *parent = K.labels + __ldg(&K.gr[g].lab);
             for (uint64_t j0 = jb; j0 < je; j0 += 32) {
                 const uint64_t j = j0 + lane;
                 uint32_t u[1] = {0};
@@ -372,46 +365,97 @@ __global__ void __launch_bounds__(kB) kb_final(BatchK K)
     }
 }
 
-/* ------------------------------------------------------------------ host */
+/* ------------------------------------------------------------- the core */
 
-struct ClassPlan {
-    ccgpu_batch_class_opts o;
-    std::vector<uint32_t> graphs;  /* host copy of the class's graph list */
-    uint64_t vertices = 0, entries = 0;
-    uint32_t *d_graphs = nullptr;
-    uint32_t *d_tile_g = nullptr, *d_tile_v0 = nullptr;
-    uint32_t tiles = 0;
-    uint32_t tiles_for = 0;        /* tile size the tile list was built for */
-    unsigned long long *d_cnt = nullptr; /* [0] grab, [1] heavy count */
-    uint64_t *d_heavy = nullptr;
-    uint32_t heavy_cap = 0;
-    cudaStream_t st = nullptr;
-    cudaEvent_t ev = nullptr;
-};
+/* Grows the pair of tile arrays of a class together (one capacity). */
+int grow_tiles(BatchClass &C, size_t need)
+{
+    if (need <= C.tile_cap && C.d_tile_g)
+        return CCGPU_OK;
+    cudaFree(C.d_tile_g);
+    cudaFree(C.d_tile_v0);
+    C.d_tile_g = C.d_tile_v0 = nullptr;
+    C.tile_cap = 0;
+    const size_t want = need + need / 2 + 64;
+    CC_CUDA(cudaMalloc((void **)&C.d_tile_g, want * sizeof(uint32_t)));
+    CC_CUDA(cudaMalloc((void **)&C.d_tile_v0, want * sizeof(uint32_t)));
+    C.tile_cap = want;
+    return CCGPU_OK;
+}
+
+template <typename T>
+int grow(T **p, size_t *cap, size_t need)
+{
+    if (need <= *cap && *p)
+        return CCGPU_OK;
+    size_t want = need + need / 2 + 64;
+    cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    CC_CUDA(cudaMalloc((void **)p, want * sizeof(T)));
+    *cap = want;
+    return CCGPU_OK;
+}
+
+BatchK kargs(BatchCore *c, int k)
+{
+    BatchClass &C = c->cls[k];
+    BatchK K;
+    K.gr = c->d_gr;
+    K.row_ptr = c->row_ptr;
+    K.col = c->col;
+    K.labels = c->labels;
+    K.tile_g = C.d_tile_g;
+    K.tile_v0 = C.d_tile_v0;
+    K.tiles = C.tiles;
+    K.tile = (uint32_t)C.o.tile;
+    K.graphs = C.d_graphs;
+    K.ngraphs = (uint32_t)C.graphs.size();
+    K.giants = c->d_giants;
+    K.comps = c->d_comps;
+    K.tiles_done = c->d_tiles_done;
+    K.done = c->d_done;
+    K.grab = C.d_cnt;
+    K.heavy_count = (uint32_t *)(C.d_cnt + 1);
+    K.heavy_list = C.d_heavy;
+    K.heavy_cap = C.heavy_used;
+    K.heavy_deg = (uint32_t)c->tune.heavy_degree;
+    K.warp_deg = (uint32_t)C.o.warp_degree;
+    K.skip = C.o.sample_rounds > 0;
+    return K;
+}
+
+/* Tile list of class k into `tg`/`tv` (host). */
+void tiles_of(const BatchCore *c, int k, std::vector<uint32_t> &tg, std::vector<uint32_t> &tv)
+{
+    const BatchClass &C = c->cls[k];
+    const uint32_t T = (uint32_t)C.o.tile;
+    tg.clear();
+    tv.clear();
+    for (uint32_t g : C.graphs)
+        for (uint64_t v0 = 0; v0 < c->gr[g].n; v0 += T) {
+            tg.push_back(g);
+            tv.push_back((uint32_t)v0);
+        }
+}
+
+int stage(BatchCore *c, size_t bytes)
+{
+    if (bytes <= c->stage_cap && c->h_stage)
+        return CCGPU_OK;
+    if (c->h_stage)
+        CC_CUDA(cudaFreeHost(c->h_stage));
+    c->h_stage = nullptr;
+    c->stage_cap = 0;
+    const size_t want = bytes + bytes / 2 + 4096;
+    CC_CUDA(cudaMallocHost(&c->h_stage, want));
+    c->stage_cap = want;
+    return CCGPU_OK;
+}
 
 } // namespace
 
-struct ccgpu_batch_plan {
-    ccgpu_ctx *ctx;
-    uint32_t G;
-    std::vector<uint64_t> vtx_off, edge_off;
-    ccgpu_batch_tuning tune;
-    uint64_t *d_vtx_off = nullptr, *d_edge_off = nullptr;
-    const uint64_t *d_row_ptr;
-    const uint32_t *d_col;
-    uint32_t *d_labels;
-    uint32_t *d_giants = nullptr, *d_comps = nullptr, *d_tiles_done = nullptr, *d_done = nullptr;
-    ClassPlan cls[CCGPU_BATCH_CLASSES];
-    cudaEvent_t fork = nullptr;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    int kernels = 0;
-    int sms = 148;
-};
-
-namespace {
-
-int class_of(const ccgpu_batch_tuning &t, uint64_t n, uint64_t m)
+int batch_class_of(const ccgpu_batch_tuning &t, uint64_t n, uint64_t m)
 {
     const double avg = n ? (double)m / (double)n : 0.0;
     int c = 0;
@@ -420,137 +464,265 @@ int class_of(const ccgpu_batch_tuning &t, uint64_t n, uint64_t m)
     return c;
 }
 
-int check_class_opts(const ccgpu_batch_class_opts &o)
+int batch_check_tuning(ccgpu_batch_tuning *t)
 {
-    if (o.sample_rounds < 0 || o.sample_rounds > 4)
-        return ccgpu_set_error(CCGPU_ERR_INVALID, "batch: sample_rounds %d not in 0..4",
-                               o.sample_rounds);
-    if (o.tile < 256 || o.tile > (1 << 20) || (o.tile & (o.tile - 1)))
-        return ccgpu_set_error(CCGPU_ERR_INVALID,
-                               "batch: tile %d is not a power of two in 256..2^20", o.tile);
-    if (o.warp_degree < 2 || o.warp_degree > 1024)
-        return ccgpu_set_error(CCGPU_ERR_INVALID, "batch: warp_degree %d not in 2..1024",
-                               o.warp_degree);
+    if (t->heavy_degree < 32)
+        t->heavy_degree = 32;
+    for (int c = 0; c < CCGPU_BATCH_CLASSES; ++c) {
+        const ccgpu_batch_class_opts &o = t->cls[c];
+        if (o.sample_rounds < 0 || o.sample_rounds > 4)
+            return ccgpu_set_error(CCGPU_ERR_INVALID, "batch: sample_rounds %d not in 0..4",
+                                   o.sample_rounds);
+        if (o.tile < 256 || o.tile > (1 << 20) || (o.tile & (o.tile - 1)))
+            return ccgpu_set_error(CCGPU_ERR_INVALID,
+                                   "batch: tile %d is not a power of two in 256..2^20", o.tile);
+        if (o.warp_degree < 2 || o.warp_degree > 1024)
+            return ccgpu_set_error(CCGPU_ERR_INVALID, "batch: warp_degree %d not in 2..1024",
+                                   o.warp_degree);
+    }
     return CCGPU_OK;
 }
 
-/* (Re)builds the tile list of class c for its current tile size. */
-int build_tiles(ccgpu_batch_plan *p, int c)
+int batch_core_init(BatchCore *c, ccgpu_ctx *ctx, const ccgpu_batch_tuning *tuning)
 {
-    ClassPlan &C = p->cls[c];
-    const uint32_t T = (uint32_t)C.o.tile;
-    if (T == 0)
-        return ccgpu_set_error(CCGPU_ERR_INVALID, "batch: tile size 0");
-    if (C.d_tile_g && C.tiles_for == T)
-        return CCGPU_OK;
-    std::vector<uint32_t> tg, tv;
-    for (uint32_t g : C.graphs) {
-        const uint64_t n = p->vtx_off[g + 1] - p->vtx_off[g];
-        for (uint64_t v0 = 0; v0 < n; v0 += T) {
-            tg.push_back(g);
-            tv.push_back((uint32_t)v0);
+    c->ctx = ctx;
+    c->sms = ctx->sm_count;
+    if (tuning)
+        c->tune = *tuning;
+    else
+        ccgpu_batch_tuning_default(&c->tune);
+    CC_TRY(batch_check_tuning(&c->tune));
+    CC_CUDA(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming));
+    for (int k = 0; k < CCGPU_BATCH_CLASSES; ++k) {
+        c->cls[k].o = c->tune.cls[k];
+        CC_CUDA(cudaStreamCreateWithFlags(&c->cls[k].st, cudaStreamNonBlocking));
+        CC_CUDA(cudaEventCreateWithFlags(&c->cls[k].ev, cudaEventDisableTiming));
+        CC_CUDA(cudaMalloc((void **)&c->cls[k].d_cnt, 256));
+    }
+    return CCGPU_OK;
+}
+
+void batch_core_free(BatchCore *c)
+{
+    for (int k = 0; k < CCGPU_BATCH_CLASSES; ++k) {
+        BatchClass &C = c->cls[k];
+        cudaFree(C.d_graphs);
+        cudaFree(C.d_tile_g);
+        cudaFree(C.d_tile_v0);
+        cudaFree(C.d_cnt);
+        cudaFree(C.d_heavy);
+        if (C.st)
+            cudaStreamDestroy(C.st);
+        if (C.ev)
+            cudaEventDestroy(C.ev);
+        C = BatchClass();
+    }
+    if (c->fork)
+        cudaEventDestroy(c->fork);
+    cudaFree(c->d_gr);
+    cudaFree(c->d_giants);
+    cudaFree(c->d_comps);
+    cudaFree(c->d_tiles_done);
+    cudaFree(c->d_done);
+    if (c->h_stage)
+        cudaFreeHost(c->h_stage);
+    *c = BatchCore();
+}
+
+int batch_core_reserve(BatchCore *c, size_t graphs, size_t tiles, size_t heavy)
+{
+    if (graphs > c->g_cap || !c->d_gr) {
+        cudaFree(c->d_gr);
+        cudaFree(c->d_giants);
+        cudaFree(c->d_comps);
+        cudaFree(c->d_tiles_done);
+        cudaFree(c->d_done);
+        c->d_gr = nullptr;
+        c->d_giants = c->d_comps = c->d_tiles_done = c->d_done = nullptr;
+        c->g_cap = 0;
+        CC_CUDA(cudaMalloc((void **)&c->d_gr, graphs * sizeof(BGraph)));
+        CC_CUDA(cudaMalloc((void **)&c->d_giants, graphs * sizeof(uint32_t)));
+        CC_CUDA(cudaMalloc((void **)&c->d_comps, graphs * sizeof(uint32_t)));
+        CC_CUDA(cudaMalloc((void **)&c->d_tiles_done, graphs * sizeof(uint32_t)));
+        CC_CUDA(cudaMalloc((void **)&c->d_done, graphs * sizeof(uint32_t)));
+        c->g_cap = graphs;
+    }
+    for (int k = 0; k < CCGPU_BATCH_CLASSES; ++k) {
+        BatchClass &C = c->cls[k];
+        CC_TRY(grow(&C.d_graphs, &C.graphs_cap, graphs));
+        CC_TRY(grow_tiles(C, tiles));
+        CC_TRY(grow(&C.d_heavy, &C.heavy_cap, heavy));
+    }
+    return stage(c, graphs * sizeof(BGraph) +
+                        CCGPU_BATCH_CLASSES * ((graphs + 2 * tiles) * sizeof(uint32_t) + 64));
+}
+
+int batch_core_set(BatchCore *c, const uint64_t *row_ptr, const uint32_t *col, uint32_t *labels,
+                   const BGraph *gr, uint32_t G, cudaStream_t st, int sync)
+{
+    c->row_ptr = row_ptr;
+    c->col = col;
+    c->labels = labels;
+    c->gr.assign(gr, gr + G);
+    for (int k = 0; k < CCGPU_BATCH_CLASSES; ++k) {
+        BatchClass &C = c->cls[k];
+        C.graphs.clear();
+        C.vertices = C.entries = 0;
+    }
+    for (uint32_t g = 0; g < G; ++g) {
+        BatchClass &C = c->cls[batch_class_of(c->tune, gr[g].n, gr[g].m)];
+        C.graphs.push_back(g);
+        C.vertices += gr[g].n;
+        C.entries += gr[g].m;
+    }
+    if (G > c->g_cap || !c->d_gr) { /* per-graph arrays grow together */
+        cudaFree(c->d_gr);
+        cudaFree(c->d_giants);
+        cudaFree(c->d_comps);
+        cudaFree(c->d_tiles_done);
+        cudaFree(c->d_done);
+        c->d_gr = nullptr;
+        c->d_giants = c->d_comps = c->d_tiles_done = c->d_done = nullptr;
+        c->g_cap = 0;
+        const size_t want = (size_t)G + G / 2 + 64;
+        CC_CUDA(cudaMalloc((void **)&c->d_gr, want * sizeof(BGraph)));
+        CC_CUDA(cudaMalloc((void **)&c->d_giants, want * sizeof(uint32_t)));
+        CC_CUDA(cudaMalloc((void **)&c->d_comps, want * sizeof(uint32_t)));
+        CC_CUDA(cudaMalloc((void **)&c->d_tiles_done, want * sizeof(uint32_t)));
+        CC_CUDA(cudaMalloc((void **)&c->d_done, want * sizeof(uint32_t)));
+        c->g_cap = want;
+    }
+    /* staging: descriptors, then per class graph list and tile list */
+    std::vector<uint32_t> tg[CCGPU_BATCH_CLASSES], tv[CCGPU_BATCH_CLASSES];
+    size_t bytes = (size_t)G * sizeof(BGraph);
+    for (int k = 0; k < CCGPU_BATCH_CLASSES; ++k) {
+        tiles_of(c, k, tg[k], tv[k]);
+        bytes += (c->cls[k].graphs.size() + 2 * tg[k].size()) * sizeof(uint32_t) + 64;
+    }
+    CC_TRY(stage(c, bytes));
+    char *h = (char *)c->h_stage;
+    size_t off = 0;
+    auto put = [&](const void *src, size_t n) -> char * {
+        char *dst = h + off;
+        if (n)
+            memcpy(dst, src, n);
+        off = (off + n + 15) & ~(size_t)15;
+        return dst;
+    };
+    char *hg = put(gr, (size_t)G * sizeof(BGraph));
+    if (G)
+        CC_CUDA(cudaMemcpyAsync(c->d_gr, hg, (size_t)G * sizeof(BGraph), cudaMemcpyHostToDevice,
+                                st));
+    for (int k = 0; k < CCGPU_BATCH_CLASSES; ++k) {
+        BatchClass &C = c->cls[k];
+        const size_t ng = C.graphs.size(), nt = tg[k].size();
+        CC_TRY(grow(&C.d_graphs, &C.graphs_cap, ng ? ng : 1));
+        CC_TRY(grow_tiles(C, nt ? nt : 1));
+        uint64_t hc = C.entries / (uint64_t)c->tune.heavy_degree + 1;
+        if (hc > C.vertices + 1)
+            hc = C.vertices + 1;
+        if (hc > 0xffffffffull)
+            hc = 0xffffffffull;
+        CC_TRY(grow(&C.d_heavy, &C.heavy_cap, (size_t)hc));
+        C.heavy_used = (uint32_t)hc;
+        C.tiles = (uint32_t)nt;
+        if (ng) {
+            char *p = put(C.graphs.data(), ng * 4);
+            CC_CUDA(cudaMemcpyAsync(C.d_graphs, p, ng * 4, cudaMemcpyHostToDevice, st));
+        }
+        if (nt) {
+            char *p = put(tg[k].data(), nt * 4);
+            CC_CUDA(cudaMemcpyAsync(C.d_tile_g, p, nt * 4, cudaMemcpyHostToDevice, st));
+            p = put(tv[k].data(), nt * 4);
+            CC_CUDA(cudaMemcpyAsync(C.d_tile_v0, p, nt * 4, cudaMemcpyHostToDevice, st));
         }
     }
-    cudaFree(C.d_tile_g);
-    cudaFree(C.d_tile_v0);
-    C.d_tile_g = C.d_tile_v0 = nullptr;
-    C.tiles = (uint32_t)tg.size();
-    C.tiles_for = T;
-    const size_t bytes = (tg.size() ? tg.size() : 1) * sizeof(uint32_t);
-    CC_CUDA(cudaMalloc((void **)&C.d_tile_g, bytes));
-    CC_CUDA(cudaMalloc((void **)&C.d_tile_v0, bytes));
-    if (!tg.empty()) {
-        CC_CUDA(cudaMemcpy(C.d_tile_g, tg.data(), tg.size() * 4, cudaMemcpyHostToDevice));
-        CC_CUDA(cudaMemcpy(C.d_tile_v0, tv.data(), tv.size() * 4, cudaMemcpyHostToDevice));
-    }
+    if (sync)
+        CC_CUDA(cudaStreamSynchronize(st));
     return CCGPU_OK;
 }
 
-BatchK kargs(ccgpu_batch_plan *p, int c)
+int batch_core_retile(BatchCore *c, int k)
 {
-    ClassPlan &C = p->cls[c];
-    BatchK K;
-    K.vtx_off = p->d_vtx_off;
-    K.edge_off = p->d_edge_off;
-    K.row_ptr = p->d_row_ptr;
-    K.col = p->d_col;
-    K.labels = p->d_labels;
-    K.tile_g = C.d_tile_g;
-    K.tile_v0 = C.d_tile_v0;
-    K.tiles = C.tiles;
-    K.tile = (uint32_t)C.o.tile;
-    K.graphs = C.d_graphs;
-    K.ngraphs = (uint32_t)C.graphs.size();
-    K.giants = p->d_giants;
-    K.comps = p->d_comps;
-    K.tiles_done = p->d_tiles_done;
-    K.done = p->d_done;
-    K.grab = C.d_cnt;
-    K.heavy_count = (uint32_t *)(C.d_cnt + 1);
-    K.heavy_list = C.d_heavy;
-    K.heavy_cap = C.heavy_cap;
-    K.heavy_deg = (uint32_t)p->tune.heavy_degree;
-    K.warp_deg = (uint32_t)C.o.warp_degree;
-    K.skip = C.o.sample_rounds > 0;
-    return K;
+    BatchClass &C = c->cls[k];
+    std::vector<uint32_t> tg, tv;
+    tiles_of(c, k, tg, tv);
+    const size_t nt = tg.size();
+    CC_TRY(grow_tiles(C, nt ? nt : 1));
+    if (nt) {
+        CC_CUDA(cudaMemcpy(C.d_tile_g, tg.data(), nt * 4, cudaMemcpyHostToDevice));
+        CC_CUDA(cudaMemcpy(C.d_tile_v0, tv.data(), nt * 4, cudaMemcpyHostToDevice));
+    }
+    C.tiles = (uint32_t)nt;
+    return CCGPU_OK;
 }
 
-/* Enqueues class c's whole solve on stream st. */
-int enqueue_class(ccgpu_batch_plan *p, int c, cudaStream_t st, int *kernels)
+int batch_core_enqueue_class(BatchCore *c, int k, cudaStream_t st, int *kernels)
 {
-    ClassPlan &C = p->cls[c];
+    BatchClass &C = c->cls[k];
     if (C.graphs.empty() || C.tiles == 0)
         return CCGPU_OK;
-    ccgpu_ctx *ctx = p->ctx;
-    const BatchK K = kargs(p, c);
-    const unsigned tb = cc_blocks(C.tiles, 1, (unsigned)p->sms * 8);
-    int k = 0;
+    ccgpu_ctx *ctx = c->ctx;
+    const BatchK K = kargs(c, k);
+    const unsigned tb = cc_blocks(C.tiles, 1, (unsigned)c->sms * 8);
+    int n = 0;
     CC_CUDA(cudaMemsetAsync(C.d_cnt, 0, 2 * sizeof(unsigned long long), st));
     CC_KLAUNCH(ctx, CCK_BATCH_INIT, kb_init, tb, kB, 0, st, K);
-    ++k;
+    ++n;
     const int rounds = C.o.sample_rounds;
     for (int r = 0; r < rounds; ++r) {
         CC_KLAUNCH(ctx, CCK_BATCH_SAMPLE, kb_sample, tb, kB, 0, st, K, r);
-        ++k;
+        ++n;
         if (C.o.cadence || r + 1 == rounds) {
             CC_KLAUNCH(ctx, CCK_BATCH_COMPRESS, kb_compress, tb, kB, 0, st, K);
-            ++k;
+            ++n;
         }
     }
     if (rounds > 0) {
-        const unsigned gb = cc_blocks(C.graphs.size(), 1, (unsigned)p->sms * 2);
+        const unsigned gb = cc_blocks(C.graphs.size(), 1, (unsigned)c->sms * 2);
         CC_KLAUNCH(ctx, CCK_BATCH_GIANT, kb_giant, gb, 1024, 0, st, K, 0x5eed1234u);
-        ++k;
+        ++n;
     }
-    CC_KLAUNCH(ctx, CCK_BATCH_LINK, kb_link, (unsigned)p->sms * 4, kB, 0, st, K);
-    CC_KLAUNCH(ctx, CCK_BATCH_HEAVY, kb_heavy, (unsigned)p->sms * 4, kB, 0, st, K);
+    CC_KLAUNCH(ctx, CCK_BATCH_LINK, kb_link, (unsigned)c->sms * 4, kB, 0, st, K);
+    CC_KLAUNCH(ctx, CCK_BATCH_HEAVY, kb_heavy, (unsigned)c->sms * 4, kB, 0, st, K);
     CC_KLAUNCH(ctx, CCK_BATCH_FINAL, kb_final, tb, kB, 0, st, K);
-    k += 3;
+    n += 3;
     if (kernels)
-        *kernels += k;
+        *kernels += n;
     return CCGPU_OK;
 }
 
-/* The whole batch on `st`: per-graph outputs cleared, then every class on
- * its own stream forked from st and joined back. */
-int enqueue_all(ccgpu_batch_plan *p, cudaStream_t st, int *kernels)
+int batch_core_enqueue(BatchCore *c, cudaStream_t st, int *kernels)
 {
-    const size_t gbytes = (size_t)(p->G ? p->G : 1) * sizeof(uint32_t);
-    CC_CUDA(cudaMemsetAsync(p->d_comps, 0, gbytes, st));
-    CC_CUDA(cudaMemsetAsync(p->d_tiles_done, 0, gbytes, st));
-    CC_CUDA(cudaMemsetAsync(p->d_done, 0, gbytes, st));
-    CC_CUDA(cudaEventRecord(p->fork, st));
-    for (int c = 0; c < CCGPU_BATCH_CLASSES; ++c) {
-        ClassPlan &C = p->cls[c];
+    const size_t gbytes = (c->gr.empty() ? 1 : c->gr.size()) * sizeof(uint32_t);
+    CC_CUDA(cudaMemsetAsync(c->d_comps, 0, gbytes, st));
+    CC_CUDA(cudaMemsetAsync(c->d_tiles_done, 0, gbytes, st));
+    CC_CUDA(cudaMemsetAsync(c->d_done, 0, gbytes, st));
+    CC_CUDA(cudaEventRecord(c->fork, st));
+    for (int k = 0; k < CCGPU_BATCH_CLASSES; ++k) {
+        BatchClass &C = c->cls[k];
         if (C.graphs.empty())
             continue;
-        CC_CUDA(cudaStreamWaitEvent(C.st, p->fork, 0));
-        CC_TRY(enqueue_class(p, c, C.st, kernels));
+        CC_CUDA(cudaStreamWaitEvent(C.st, c->fork, 0));
+        CC_TRY(batch_core_enqueue_class(c, k, C.st, kernels));
         CC_CUDA(cudaEventRecord(C.ev, C.st));
         CC_CUDA(cudaStreamWaitEvent(st, C.ev, 0));
     }
     return CCGPU_OK;
 }
+
+/* -------------------------------------------------- packed-batch plans */
+
+struct ccgpu_batch_plan {
+    BatchCore core;
+    uint32_t G = 0;
+    std::vector<uint64_t> vtx_off;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int kernels = 0;
+};
+
+namespace {
 
 void drop_graph(ccgpu_batch_plan *p)
 {
@@ -571,13 +743,14 @@ int capture(ccgpu_batch_plan *p)
     int rc = CCGPU_OK;
     /* the launch profiler would record events into the graph: off while
      * capturing */
-    struct cc_prof *saved = p->ctx->prof;
-    p->ctx->prof = nullptr;
+    ccgpu_ctx *ctx = p->core.ctx;
+    struct cc_prof *saved = ctx->prof;
+    ctx->prof = nullptr;
     cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) {
         rc = ccgpu_cuda_fail(e, "cudaStreamBeginCapture", __FILE__, __LINE__);
     } else {
-        rc = enqueue_all(p, cs, &kernels);
+        rc = batch_core_enqueue(&p->core, cs, &kernels);
         cudaGraph_t g = nullptr;
         e = cudaStreamEndCapture(cs, &g);
         if (rc == CCGPU_OK && e != cudaSuccess)
@@ -591,84 +764,24 @@ int capture(ccgpu_batch_plan *p)
             cudaGraphDestroy(g);
         }
     }
-    p->ctx->prof = saved;
+    ctx->prof = saved;
     cudaStreamDestroy(cs);
     if (rc == CCGPU_OK)
         p->kernels = kernels;
     return rc;
 }
 
-int alloc_class_scratch(ccgpu_batch_plan *p, int c)
-{
-    ClassPlan &C = p->cls[c];
-    uint64_t cap = C.entries / (uint64_t)p->tune.heavy_degree + 1;
-    if (cap > C.vertices + 1)
-        cap = C.vertices + 1;
-    if (cap > 0xffffffffu)
-        cap = 0xffffffffu;
-    C.heavy_cap = (uint32_t)cap;
-    CC_CUDA(cudaMalloc((void **)&C.d_cnt, 256));
-    CC_CUDA(cudaMalloc((void **)&C.d_heavy, cap * sizeof(uint64_t)));
-    const size_t gb = (C.graphs.size() ? C.graphs.size() : 1) * sizeof(uint32_t);
-    CC_CUDA(cudaMalloc((void **)&C.d_graphs, gb));
-    if (!C.graphs.empty())
-        CC_CUDA(cudaMemcpy(C.d_graphs, C.graphs.data(), C.graphs.size() * 4,
-                           cudaMemcpyHostToDevice));
-    CC_CUDA(cudaStreamCreateWithFlags(&C.st, cudaStreamNonBlocking));
-    CC_CUDA(cudaEventCreateWithFlags(&C.ev, cudaEventDisableTiming));
-    return build_tiles(p, c);
-}
-
-int plan_setup(ccgpu_batch_plan *p, const ccgpu_batch *b)
-{
-    const uint32_t G = p->G;
-    p->vtx_off.assign(b->h_vtx_off, b->h_vtx_off + G + 1);
-    p->edge_off.assign(b->h_edge_off, b->h_edge_off + G + 1);
-    if (p->vtx_off[0] != 0 || p->edge_off[0] != 0)
-        return ccgpu_set_error(CCGPU_ERR_INVALID, "batch: offsets must start at 0");
-    for (uint32_t g = 0; g < G; ++g) {
-        if (p->vtx_off[g + 1] < p->vtx_off[g] || p->edge_off[g + 1] < p->edge_off[g])
-            return ccgpu_set_error(CCGPU_ERR_INVALID, "batch: offsets of graph %u decrease", g);
-        if (p->vtx_off[g + 1] - p->vtx_off[g] >= 0xffffffffull)
-            return ccgpu_set_error(CCGPU_ERR_LIMIT, "batch: graph %u has 2^32-1 or more vertices",
-                                   g);
-        const uint64_t n = p->vtx_off[g + 1] - p->vtx_off[g];
-        const uint64_t m = p->edge_off[g + 1] - p->edge_off[g];
-        ClassPlan &C = p->cls[class_of(p->tune, n, m)];
-        C.graphs.push_back(g);
-        C.vertices += n;
-        C.entries += m;
-    }
-    const size_t ob = (size_t)(G + 1) * sizeof(uint64_t);
-    CC_CUDA(cudaMalloc((void **)&p->d_vtx_off, ob));
-    CC_CUDA(cudaMalloc((void **)&p->d_edge_off, ob));
-    CC_CUDA(cudaMemcpy(p->d_vtx_off, p->vtx_off.data(), ob, cudaMemcpyHostToDevice));
-    CC_CUDA(cudaMemcpy(p->d_edge_off, p->edge_off.data(), ob, cudaMemcpyHostToDevice));
-    const size_t gb = (size_t)(G ? G : 1) * sizeof(uint32_t);
-    CC_CUDA(cudaMalloc((void **)&p->d_giants, gb));
-    CC_CUDA(cudaMalloc((void **)&p->d_comps, gb));
-    CC_CUDA(cudaMalloc((void **)&p->d_tiles_done, gb));
-    CC_CUDA(cudaMalloc((void **)&p->d_done, gb));
-    CC_CUDA(cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming));
-    for (int c = 0; c < CCGPU_BATCH_CLASSES; ++c) {
-        p->cls[c].o = p->tune.cls[c];
-        if (!p->cls[c].graphs.empty())
-            CC_TRY(alloc_class_scratch(p, c));
-    }
-    return CCGPU_OK;
-}
-
-/* Device time of `reps` solves of class c alone (after one warm-up). */
-int time_class(ccgpu_batch_plan *p, int c, cudaStream_t st, int reps, float *ms)
+/* Device time of `reps` solves of class k alone (after one warm-up). */
+int time_class(BatchCore *c, int k, cudaStream_t st, int reps, float *ms)
 {
     cudaEvent_t a = nullptr, z = nullptr;
     CC_CUDA(cudaEventCreate(&a));
     CC_CUDA(cudaEventCreate(&z));
-    int rc = enqueue_class(p, c, st, nullptr);
+    int rc = batch_core_enqueue_class(c, k, st, nullptr);
     if (rc == CCGPU_OK && cudaEventRecord(a, st) != cudaSuccess)
         rc = ccgpu_set_error(CCGPU_ERR_CUDA, "batch autotune: event record failed");
     for (int i = 0; rc == CCGPU_OK && i < reps; ++i)
-        rc = enqueue_class(p, c, st, nullptr);
+        rc = batch_core_enqueue_class(c, k, st, nullptr);
     if (rc == CCGPU_OK) {
         cudaEventRecord(z, st);
         cudaError_t e = cudaEventSynchronize(z);
@@ -713,25 +826,38 @@ extern "C" int ccgpu_batch_plan_create(ccgpu_ctx *ctx, const ccgpu_batch *b,
         return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_batch_plan_create: empty batch");
     if (!b->d_row_ptr || !b->d_labels || (b->h_edge_off[b->graphs] && !b->d_col))
         return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_batch_plan_create: NULL device array");
-    CC_TRY(ccgpu_ctx_resolve(&ctx));
+    const uint32_t G = b->graphs;
+    const uint64_t *vo = b->h_vtx_off, *eo = b->h_edge_off;
+    if (vo[0] != 0 || eo[0] != 0)
+        return ccgpu_set_error(CCGPU_ERR_INVALID, "batch: offsets must start at 0");
+    std::vector<BGraph> gr(G);
+    for (uint32_t g = 0; g < G; ++g) {
+        if (vo[g + 1] < vo[g] || eo[g + 1] < eo[g])
+            return ccgpu_set_error(CCGPU_ERR_INVALID, "batch: offsets of graph %u decrease", g);
+        if (vo[g + 1] - vo[g] >= 0xffffffffull)
+            return ccgpu_set_error(CCGPU_ERR_LIMIT, "batch: graph %u has 2^32-1 or more vertices",
+                                   g);
+        gr[g].rp = vo[g] + g;
+        gr[g].col = eo[g];
+        gr[g].lab = vo[g];
+        gr[g].n = (uint32_t)(vo[g + 1] - vo[g]);
+        gr[g].m = eo[g + 1] - eo[g];
+        gr[g].pad = 0;
+    }
     ccgpu_batch_tuning t;
     if (tuning)
         t = *tuning;
     else
         ccgpu_batch_tuning_default(&t);
-    if (t.heavy_degree < 32)
-        t.heavy_degree = 32;
-    for (int c = 0; c < CCGPU_BATCH_CLASSES; ++c)
-        CC_TRY(check_class_opts(t.cls[c]));
+    CC_TRY(batch_check_tuning(&t));
+    CC_TRY(ccgpu_ctx_resolve(&ctx));
     ccgpu_batch_plan *p = new ccgpu_batch_plan();
-    p->ctx = ctx;
-    p->G = b->graphs;
-    p->tune = t;
-    p->d_row_ptr = b->d_row_ptr;
-    p->d_col = b->d_col;
-    p->d_labels = b->d_labels;
-    p->sms = ctx->sm_count;
-    int rc = plan_setup(p, b);
+    p->G = G;
+    p->vtx_off.assign(vo, vo + G + 1);
+    int rc = batch_core_init(&p->core, ctx, &t);
+    if (rc == CCGPU_OK)
+        rc = batch_core_set(&p->core, b->d_row_ptr, b->d_col, b->d_labels, gr.data(), G,
+                            nullptr, 1);
     if (rc != CCGPU_OK) {
         ccgpu_batch_plan_destroy(p);
         return rc;
@@ -744,7 +870,7 @@ extern "C" int ccgpu_batch_plan_run(ccgpu_batch_plan *p, void *stream)
 {
     if (!p)
         return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_batch_plan_run: NULL plan");
-    return enqueue_all(p, (cudaStream_t)stream, nullptr);
+    return batch_core_enqueue(&p->core, (cudaStream_t)stream, nullptr);
 }
 
 extern "C" int ccgpu_batch_plan_launch(ccgpu_batch_plan *p, void *stream)
@@ -766,7 +892,7 @@ extern "C" int ccgpu_batch_plan_tuning(const ccgpu_batch_plan *p, ccgpu_batch_tu
 {
     if (!p || !out)
         return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_batch_plan_tuning: NULL argument");
-    *out = p->tune;
+    *out = p->core.tune;
     return CCGPU_OK;
 }
 
@@ -775,7 +901,7 @@ extern "C" int ccgpu_batch_plan_class_graphs(const ccgpu_batch_plan *p, uint32_t
     if (!p || !counts)
         return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_batch_plan_class_graphs: NULL argument");
     for (int c = 0; c < CCGPU_BATCH_CLASSES; ++c)
-        counts[c] = (uint32_t)p->cls[c].graphs.size();
+        counts[c] = (uint32_t)p->core.cls[c].graphs.size();
     return CCGPU_OK;
 }
 
@@ -787,54 +913,57 @@ extern "C" int ccgpu_batch_plan_autotune(ccgpu_batch_plan *p, void *stream,
     if (!p)
         return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_batch_plan_autotune: NULL plan");
     cudaStream_t st = (cudaStream_t)stream;
-    struct cc_prof *saved = p->ctx->prof;
-    p->ctx->prof = nullptr;
+    BatchCore *c = &p->core;
+    struct cc_prof *saved = c->ctx->prof;
+    c->ctx->prof = nullptr;
     int rc = CCGPU_OK;
-    for (int c = 0; c < CCGPU_BATCH_CLASSES && rc == CCGPU_OK; ++c) {
-        ClassPlan &C = p->cls[c];
+    for (int k = 0; k < CCGPU_BATCH_CLASSES && rc == CCGPU_OK; ++k) {
+        BatchClass &C = c->cls[k];
         if (C.graphs.empty())
             continue;
         ccgpu_batch_class_opts best = C.o;
         float best_ms = 0.f;
-        rc = time_class(p, c, st, 3, &best_ms);
+        rc = time_class(c, k, st, 3, &best_ms);
         const int rounds[] = {0, 1, 2, 3};
         const int tiles[] = {1024, 4096, 16384};
         const int wdeg[] = {8, 16, 32, 64};
         for (int axis = 0; axis < 4 && rc == CCGPU_OK; ++axis) {
-            const int *vals = axis == 0 ? rounds : axis == 2 ? tiles : axis == 3 ? wdeg : nullptr;
             const int nv = axis == 0 ? 4 : axis == 1 ? 2 : axis == 2 ? 3 : 4;
             for (int i = 0; i < nv && rc == CCGPU_OK; ++i) {
                 ccgpu_batch_class_opts cand = best;
                 if (axis == 0)
-                    cand.sample_rounds = vals[i];
+                    cand.sample_rounds = rounds[i];
                 else if (axis == 1)
                     cand.cadence = i;
                 else if (axis == 2)
-                    cand.tile = vals[i];
+                    cand.tile = tiles[i];
                 else
-                    cand.warp_degree = vals[i];
+                    cand.warp_degree = wdeg[i];
                 if (!memcmp(&cand, &best, sizeof(cand)))
                     continue;
+                const bool retile = cand.tile != C.o.tile;
                 C.o = cand;
-                rc = build_tiles(p, c);
+                if (retile)
+                    rc = batch_core_retile(c, k);
                 float ms = 0.f;
                 if (rc == CCGPU_OK)
-                    rc = time_class(p, c, st, 3, &ms);
+                    rc = time_class(c, k, st, 3, &ms);
                 if (rc == CCGPU_OK && ms < best_ms) {
                     best_ms = ms;
                     best = cand;
                 }
             }
         }
+        const bool retile = best.tile != C.o.tile;
         C.o = best;
-        if (rc == CCGPU_OK)
-            rc = build_tiles(p, c);
-        p->tune.cls[c] = best;
+        if (rc == CCGPU_OK && retile)
+            rc = batch_core_retile(c, k);
+        c->tune.cls[k] = best;
     }
-    p->ctx->prof = saved;
+    c->ctx->prof = saved;
     drop_graph(p);
     if (rc == CCGPU_OK && chosen)
-        *chosen = p->tune;
+        *chosen = c->tune;
     return rc;
 }
 
@@ -846,9 +975,9 @@ extern "C" int ccgpu_batch_plan_results(ccgpu_batch_plan *p, uint32_t *h_compone
     cudaStream_t st = (cudaStream_t)stream;
     const size_t gb = (size_t)p->G * sizeof(uint32_t);
     if (h_components)
-        CC_CUDA(cudaMemcpyAsync(h_components, p->d_comps, gb, cudaMemcpyDeviceToHost, st));
+        CC_CUDA(cudaMemcpyAsync(h_components, p->core.d_comps, gb, cudaMemcpyDeviceToHost, st));
     if (h_done)
-        CC_CUDA(cudaMemcpyAsync(h_done, p->d_done, gb, cudaMemcpyDeviceToHost, st));
+        CC_CUDA(cudaMemcpyAsync(h_done, p->core.d_done, gb, cudaMemcpyDeviceToHost, st));
     CC_CUDA(cudaStreamSynchronize(st));
     /* a graph without vertices has no tile: it is solved, with 0 components */
     for (uint32_t g = 0; h_done && g < p->G; ++g)
@@ -862,26 +991,7 @@ extern "C" void ccgpu_batch_plan_destroy(ccgpu_batch_plan *p)
     if (!p)
         return;
     drop_graph(p);
-    for (int c = 0; c < CCGPU_BATCH_CLASSES; ++c) {
-        ClassPlan &C = p->cls[c];
-        cudaFree(C.d_graphs);
-        cudaFree(C.d_tile_g);
-        cudaFree(C.d_tile_v0);
-        cudaFree(C.d_cnt);
-        cudaFree(C.d_heavy);
-        if (C.st)
-            cudaStreamDestroy(C.st);
-        if (C.ev)
-            cudaEventDestroy(C.ev);
-    }
-    if (p->fork)
-        cudaEventDestroy(p->fork);
-    cudaFree(p->d_vtx_off);
-    cudaFree(p->d_edge_off);
-    cudaFree(p->d_giants);
-    cudaFree(p->d_comps);
-    cudaFree(p->d_tiles_done);
-    cudaFree(p->d_done);
+    batch_core_free(&p->core);
     delete p;
 }
 

@@ -355,6 +355,64 @@ void ccgpu_batch_plan_destroy(ccgpu_batch_plan *p);
 int ccgpu_batch_cc(ccgpu_ctx *ctx, const ccgpu_batch *b, const ccgpu_batch_tuning *tuning,
                    uint32_t *h_components, void *stream);
 
+/* ------------------------------------------------------------------------
+ * Served CC: a request server with continuous batching.  No counterpart in
+ * the reference; each request's labels are those of
+ * compute_connected_components_pthreads on its graph alone.
+ *
+ * A worker thread admits submitted requests, oldest first, while a slot
+ * (max_graphs) is free and the request's CSR and labels fit in the server's
+ * HBM pool (hbm_bytes; 0 = half of the free device memory at creation).
+ * Whenever one of `streams` batch slots is idle, up to max_batch admitted
+ * requests become one batched solve on that slot's stream, so batches that
+ * form while others run overlap them on the device.  CSRs and labels stay in
+ * HBM from admission to completion.  Host buffers passed to submit must
+ * stay valid until its wait returns; pinned buffers let the copies run
+ * asynchronously.  Times are seconds on the server's clock.
+ * ---------------------------------------------------------------------- */
+typedef struct {
+    size_t hbm_bytes;    /* pool for request data; 0 = half the free HBM  */
+    uint32_t max_graphs; /* requests resident in HBM at once (8192)       */
+    uint32_t max_batch;  /* requests per batched solve (4096)             */
+    int streams;         /* batches in flight at once, 1..8 (2)           */
+} ccgpu_server_opts;
+
+typedef struct {
+    double t_submit, t_admit, t_start, t_done;
+    uint32_t components;   /* components of the request's graph          */
+    uint32_t batch_graphs; /* requests in the batch it was solved in     */
+    int status;
+} ccgpu_request_info;
+
+typedef struct {
+    uint64_t submitted, completed, batches;
+    uint32_t in_flight, max_in_flight, max_batch_seen, pending, resident;
+    size_t pool_bytes, pool_used, pool_peak;
+} ccgpu_server_stats;
+
+typedef struct ccgpu_server ccgpu_server;
+void ccgpu_server_opts_default(ccgpu_server_opts *o);
+/* Creates the pool, the batch slots and the worker thread on the current
+ * device.  tuning NULL = the batched solver's defaults. */
+int ccgpu_server_create(const ccgpu_server_opts *opts, const ccgpu_batch_tuning *tuning,
+                        ccgpu_server **out);
+/* Queues one symmetric CSR (host arrays); h_labels (n entries) receives the
+ * labels.  CCGPU_ERR_LIMIT if the graph can never fit in the pool. */
+int ccgpu_server_submit(ccgpu_server *s, const uint64_t *h_row_ptr, const uint32_t *h_col_idx,
+                        uint32_t n, uint64_t m, uint32_t *h_labels, uint64_t *ticket);
+/* Waits for a request (timeout_s < 0: no limit), copies its labels from
+ * HBM into the buffer given at submission, returns its blocks to the pool
+ * and releases the ticket (t_done = labels in that buffer).  One wait per
+ * ticket at a time; CCGPU_ERR_TIMEOUT leaves the ticket valid.  A solved
+ * request keeps its pool blocks until it is waited for. */
+int ccgpu_server_wait(ccgpu_server *s, uint64_t ticket, double timeout_s,
+                      ccgpu_request_info *info);
+int ccgpu_server_stats_get(ccgpu_server *s, ccgpu_server_stats *out);
+double ccgpu_server_now(ccgpu_server *s);
+/* Lets the batches in flight finish, drops requests not yet in a batch,
+ * stops the worker and frees the pool (labels not yet waited for are lost). */
+void ccgpu_server_destroy(ccgpu_server *s);
+
 /* Number of v with d_labels[v] == v (one root per component when the labels
  * are min-id labels).  Synchronous; result in *count. */
 int ccgpu_count_roots(ccgpu_ctx *ctx, const uint32_t *d_labels, uint32_t n,
