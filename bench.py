@@ -240,12 +240,16 @@ def dist_bytes(n, m, st):
     """Algorithmic bytes per launch of the partitioned path's kernels (the
     local-CC kernels are counted as in algorithmic_bytes, without the
     sampled-entry term)."""
-    R, U, G, reps = int(st.boundary_raw), int(st.pair_count), int(st.ghost_count), \
+    R, U, G, reps = int(st.sorted_keys), int(st.pair_count), int(st.ghost_count), \
         int(st.rep_count)
+    lm = int(st.local_entries)
     return {
         "init": 4 * n, "sample": 8 * (n + 1) + 8 * n, "compress": 8 * n,
         "final_compress": 8 * n, "link_rows": 4 * n + 8 * n, "giant": 4096,
-        "dist_reps": 4 * n + 12 * reps, "dist_pairs": 8 * (n + 1) + 4 * m + 4 * n + 8 * R,
+        "dist_local_count": 4 * m, "dist_tiles": 8 * (n + 1),
+        "dist_local_fill": 4 * m + 4 * lm + 16 * (n + 1),
+        "dist_gflag": 4 * n + n // 8, "dist_pairs_bitmap": 4 * n + 8 * G,
+        "dist_reps": 4 * n + 12 * reps, "dist_pairs": 8 * (n + 1) + 4 * m + n // 8 + 8 * R,
         "sort_hist": 8 * R, "sort_scatter": 16 * R, "dist_dedup": 8 * R,
         "dist_ghosts": 8 * R + 8 * U + 24 * G, "merge_hook": 12 * U,
         "merge_upd": 12 * reps, "merge_exch_pack": 16 * G, "merge_exch_scatter": 16 * G,
@@ -387,7 +391,8 @@ def run_dist(args, torch, dist_mod, rank, world, dev):
         cfg.update(partitions=parts, chunk_size=args.chunk, exchange_interval=args.exchange,
                    bounds=[int(x) for x in bounds], components=int(st.roots),
                    rounds=int(st.rounds), exchanges=int(st.exchanges),
-                   boundary_raw=int(st.boundary_raw), boundary_dedup=int(st.pair_count),
+                   boundary_raw=int(st.boundary_raw), sorted_keys=int(st.sorted_keys),
+                   boundary_dedup=int(st.pair_count),
                    ghosts=int(st.ghost_count), reps=int(st.rep_count),
                    sent_pairs=int(st.sent_pairs), sort_passes=int(st.sort_passes),
                    phases_ms={"bounds": st.ms_bounds, "local": st.ms_local,
@@ -658,41 +663,38 @@ def run_batch(args, torch, dist_mod, rank, world, dev):
 
 
 def serve_run(server, pool, order, rate, seconds, want_comps, want_labels, check_every,
-              closed=False):
+              closed=False, waiters=4):
     """Feeds requests `order` (pool indices) to `server`: Poisson arrivals at
-    `rate` per second for `seconds`, or all at once when `closed`.  A waiter
-    thread collects results in submission order and checks them (component
-    count always, full labels every `check_every`-th request).  Returns
-    latencies (s), achieved throughput, batch sizes and the check result."""
+    `rate` per second for `seconds`, or all at once when `closed`.  Waiter
+    threads collect results (the wait copies labels out of HBM) and check
+    them: component count always, full labels every `check_every`-th
+    request.  Returns latencies (s), achieved throughput, batch sizes and the
+    number of mismatches."""
+    import queue
     import numpy as np
     rng = np.random.default_rng(12345)
-    tickets = []
-    lock = threading.Condition()
-    done_flag = [False]
-    lat, sizes, bad = [], [], [0]
-    finished = [0]
+    q = queue.Queue()
+    lat, sizes, bad, last = [], [], [0], [0.0]
+    mu = threading.Lock()
 
     def waiter():
-        i = 0
         while True:
-            with lock:
-                while i >= len(tickets) and not done_flag[0]:
-                    lock.wait(0.01)
-                if i >= len(tickets):
-                    return
-                t, g, lab = tickets[i]
-                tickets[i] = None
+            item = q.get()
+            if item is None:
+                return
+            i, t, g, lab = item
             _, info = server.wait(t, timeout=600)
-            lat.append(info.t_done - info.t_submit)
-            sizes.append(info.batch_graphs)
-            if info.components != want_comps[g] or \
-                    (i % check_every == 0 and not (lab == want_labels[g]).all()):
-                bad[0] += 1
-            finished[0] = server.now()
-            i += 1
+            ok = info.components == want_comps[g] and \
+                (i % check_every != 0 or bool((lab == want_labels[g]).all()))
+            with mu:
+                lat.append(info.t_done - info.t_submit)
+                sizes.append(info.batch_graphs)
+                bad[0] += not ok
+                last[0] = max(last[0], info.t_done)
 
-    th = threading.Thread(target=waiter, daemon=True)
-    th.start()
+    th = [threading.Thread(target=waiter, daemon=True) for _ in range(waiters)]
+    for t in th:
+        t.start()
     t_start = server.now()
     next_t = t_start
     n_sub = 0
@@ -706,16 +708,13 @@ def serve_run(server, pool, order, rate, seconds, want_comps, want_labels, check
                 time.sleep(d)
         rp, col = pool[g]
         lab = np.empty(len(rp) - 1, dtype=np.uint32)
-        t = server.submit(rp, col, lab)
-        with lock:
-            tickets.append((t, g, lab))
-            lock.notify()
+        q.put((n_sub, server.submit(rp, col, lab), g, lab))
         n_sub += 1
-    with lock:
-        done_flag[0] = True
-        lock.notify()
-    th.join()
-    span = finished[0] - t_start
+    for _ in th:
+        q.put(None)
+    for t in th:
+        t.join()
+    span = last[0] - t_start
     return {"submitted": n_sub, "graphs_per_s": n_sub / span if span > 0 else None,
             "span_s": span, "latency": lat, "batch_sizes": sizes, "bad": bad[0]}
 

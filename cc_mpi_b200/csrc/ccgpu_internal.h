@@ -91,6 +91,10 @@ enum {
     CCK_BATCH_LINK,
     CCK_BATCH_HEAVY,
     CCK_BATCH_FINAL,
+    CCK_DIST_LOCAL_COUNT,
+    CCK_DIST_LOCAL_FILL,
+    CCK_DIST_TILES,
+    CCK_DIST_GFLAG,
     CCK_NUM
 };
 

@@ -42,8 +42,9 @@ namespace {
 
 constexpr int kB = 256;
 constexpr int kW = kB / 32;
-constexpr int kEmitBuf = 512;           /* keys per warp buffer           */
-constexpr uint64_t kHeavyChunk = 1024;  /* entries per warp in heavy rows */
+constexpr int kEmitBuf = 256;           /* keys per warp buffer           */
+constexpr int kTileE = 16;              /* column entries per thread in a tile */
+constexpr int kTile = kB * kTileE;      /* column entries per tile             */
 constexpr int kDedupItems = 16;
 constexpr uint64_t kDedupTile = kB * kDedupItems;
 
@@ -129,14 +130,12 @@ struct EmitParams {
     int rb, gb;              /* key bit widths of rep and remote          */
     uint64_t *out;           /* keys, capacity m                          */
     unsigned long long *count;
-    uint32_t *heavy_list;
-    uint32_t *heavy_count;
-    uint32_t heavy_cap;
-    uint32_t heavy_deg;
     unsigned long long *raw; /* cut edges seen (the reference's raw count) */
-    uint32_t *bitmap;        /* [parts][bm_words] (p, remote) bits, giant rep */
-    uint64_t bm_words;
-    const uint32_t *giants;  /* [parts] giant root of each partition, NULL = no bitmap */
+    uint32_t *gflag;         /* [n/32] bit v: v's label is its partition's giant label */
+    uint32_t *pmask;         /* [n] bit p: the vertex has a neighbour in p's giant tree */
+    const uint32_t *giants;  /* [parts] giant root of each partition, NULL = no masks */
+    uint64_t tiles;          /* column tiles of kTile entries     */
+    const uint32_t *tile_first; /* [tiles+1] first row starting after each tile's first entry */
 };
 
 struct WarpBuf {
@@ -144,7 +143,7 @@ struct WarpBuf {
     uint32_t cnt;
 };
 
-__device__ __forceinline__ void wb_flush(WarpBuf &w, const EmitParams &E, int lane)
+__device__ __noinline__ void wb_flush(WarpBuf &w, const EmitParams &E, int lane)
 {
     __syncwarp();
     unsigned long long base = 0;
@@ -177,23 +176,17 @@ __device__ __forceinline__ uint64_t make_key(const EmitParams &E, int p, uint32_
 
 /* Cut edges into the giant local component of a partition all carry that
  * partition's giant rep, so most raw pairs repeat the same (p, remote, giant)
- * key.  Those edges set bit (p, remote) of a bitmap instead of emitting a
- * key (read-before-set keeps repeated hits off the atomic unit; a stale read
- * only costs one redundant atomicOr); k_bitmap_keys turns the bitmap into
- * one key per set bit.  Every other cut edge emits its key as before, so the
- * sorted, deduplicated pair list is the same set. */
-__device__ __forceinline__ void bitmap_set(const EmitParams &E, int p, uint32_t u)
-{
-    uint32_t *w = E.bitmap + (uint64_t)p * E.bm_words + (u >> 5);
-    const uint32_t bit = 1u << (u & 31);
-    uint32_t cur;
-    asm volatile("ld.global.ca.u32 %0, [%1];" : "=r"(cur) : "l"(w));
-    if (!(cur & bit))
-        atomicOr(w, bit);
-}
+ * key.  The pairs are emitted from the remote end: the graph is symmetric,
+ * so the boundary pair (p, u, rep(v)) of a cut edge v-u with v in p is seen
+ * as entry v of row u.  When v lies in p's giant tree (one bit per vertex,
+ * gflag, small enough to stay in L2) the row only records partition p in a
+ * mask it owns (pmask[u], one atomicOr per row segment of a thread);
+ * k_mask_keys then writes one (p, u, giant rep) key per mask bit.  Every
+ * other cut edge emits its key, so the sorted, deduplicated pair list is
+ * the reference's. */
 
 /* Giant label (global min id) of every partition, ~0 when it has none or the
- * bitmap path is off. */
+ * mask path is off. */
 __device__ __forceinline__ void load_giant_labels(const EmitParams &E, uint32_t *s_gl)
 {
     for (int i = threadIdx.x; i < E.parts; i += blockDim.x) {
@@ -212,118 +205,181 @@ __device__ __forceinline__ void add_raw(const EmitParams &E, unsigned long long 
         atomicAdd(E.raw, raw);
 }
 
-__global__ void __launch_bounds__(kB) k_emit(EmitParams E)
+/* Giant flags: bit v of gflag is set when label[v] is the giant label of
+ * v's partition. */
+__global__ void __launch_bounds__(kB) k_giant_flags(EmitParams E)
 {
-    __shared__ uint64_t s_buf[kW][kEmitBuf];
     __shared__ uint32_t s_b[CCGPU_MAX_PARTS + 1];
     __shared__ uint32_t s_gl[CCGPU_MAX_PARTS];
     for (int i = threadIdx.x; i <= E.parts; i += kB)
         s_b[i] = E.bounds[i];
     load_giant_labels(E, s_gl);
+    __syncthreads();
+    const uint64_t stride = (uint64_t)gridDim.x * kB;
+    for (uint64_t b0 = (uint64_t)blockIdx.x * kB; b0 < E.n; b0 += stride) {
+        const uint64_t v = b0 + threadIdx.x;
+        bool g = false;
+        if (v < E.n) {
+            const int p = part_of(s_b, E.parts, (uint32_t)v);
+            g = __ldg(E.label + v) == s_gl[p];
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, g);
+        if ((threadIdx.x & 31) == 0 && b0 + threadIdx.x < E.n)
+            E.gflag[(b0 + threadIdx.x) >> 5] = bal;
+    }
+}
+
+/* Boundary pairs (src/cc_mpi.c:364-394) from the remote end, streamed over
+ * the column array in tiles of kTile entries (16 per thread, 16-byte
+ * loads).  The row of each entry comes from a max-scan of the rows' start
+ * marks over the tile (rows are laid out in vertex order, so the last row
+ * start at or before a position is its row).  Long rows need no special
+ * path. */
+/* Partition of v: compares against bounds held in registers when there
+ * are at most 8 partitions, else a binary search in shared memory. */
+template <int PMAX>
+__device__ __forceinline__ int part_fast(const uint32_t *s_b, const uint32_t *rb, int parts,
+                                         uint32_t v)
+{
+    if (PMAX <= 8) {
+        int p = 0;
+#pragma unroll
+        for (int i = 1; i < PMAX; ++i)
+            p += (i < parts) & (v >= rb[i]);
+        return p;
+    }
+    return part_of(s_b, parts, v);
+}
+
+/* ORs bits into a partition mask unless a (possibly stale) cached read
+ * already shows them: bits are only ever added, so a stale value that has
+ * them means the current one has them too. */
+__device__ __forceinline__ void mask_or(uint32_t *w, uint32_t bits)
+{
+    uint32_t cur;
+    asm("ld.global.ca.u32 %0, [%1];" : "=r"(cur) : "l"(w));
+    if ((cur & bits) != bits)
+        atomicOr(w, bits);
+}
+
+/* Position i of a tile's row-start array, padded by one word per 32 so
+ * that thread t reading its 16 consecutive positions (t * 16 + k) hits 32
+ * distinct banks across a warp. */
+#define HP(i) ((i) + ((i) >> 5))
+
+template <int PMAX>
+__global__ void __launch_bounds__(kB, 4) k_emit(EmitParams E)
+{
+    __shared__ uint64_t s_buf[kW][kEmitBuf];
+    __shared__ uint32_t s_b[CCGPU_MAX_PARTS + 1];
+    __shared__ uint32_t s_head[kTile + kTile / 32]; /* padded: see HP() */
+    __shared__ uint32_t s_w[kW];
+    for (int i = threadIdx.x; i <= E.parts; i += kB)
+        s_b[i] = E.bounds[i];
     unsigned long long raw = 0;
     __syncthreads();
+    uint32_t sb[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+        sb[i] = i <= E.parts ? s_b[i] : 0xffffffffu;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     WarpBuf w = {s_buf[warp], 0};
-    const uint64_t wstride = (uint64_t)gridDim.x * kW * 32;
-    for (uint64_t w0 = ((uint64_t)blockIdx.x * kW + warp) * 32; w0 < E.n; w0 += wstride) {
-        const uint64_t v64 = w0 + lane;
-        const bool valid = v64 < E.n;
-        const uint32_t v = valid ? (uint32_t)v64 : 0u;
-        int p = part_of(s_b, E.parts, v);
-        uint32_t lo = s_b[p], hi = s_b[p + 1];
-        uint32_t rep = valid ? __ldg(E.label + v) - lo : 0u;
-        uint64_t beg = 0, end = 0;
-        if (valid) {
-            beg = __ldg(E.row_ptr + v);
-            end = __ldg(E.row_ptr + v + 1);
-            if (end > E.m)
-                end = E.m;
-            if (beg > end)
-                beg = end;
+    for (uint64_t t = blockIdx.x; t < E.tiles; t += gridDim.x) {
+        const uint64_t lo = t * kTile;
+        const uint32_t v0 = E.tile_first[t], v1 = E.tile_first[t + 1];
+        for (int i = threadIdx.x; i < kTile + kTile / 32; i += kB)
+            s_head[i] = 0;
+        __syncthreads();
+        if (threadIdx.x == 0)
+            s_head[0] = v0 > 0 ? v0 - 1 : 0; /* the row holding the tile's first entry */
+        __syncthreads();
+        for (uint64_t v = (uint64_t)v0 + threadIdx.x; v < v1 && v < E.n; v += kB) {
+            const uint64_t rp = __ldg(E.row_ptr + v);
+            if (rp < lo + kTile)
+                atomicMax(s_head + HP(rp - lo), (uint32_t)v);
         }
-        uint64_t deg = end - beg;
-        if (deg > E.heavy_deg) {
-            uint32_t slot = atomicAdd(E.heavy_count, 1u);
-            if (slot < E.heavy_cap) {
-                E.heavy_list[slot] = v;
-                deg = 0;
+        __syncthreads();
+        /* inclusive max-scan of s_head: 16 positions per thread */
+        uint32_t run = 0;
+#pragma unroll
+        for (int k = 0; k < kTileE; ++k) {
+            const uint32_t h = s_head[HP(threadIdx.x * kTileE + k)];
+            run = h > run ? h : run;
+        }
+        uint32_t incl = run;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o)
+                incl = y > incl ? y : incl;
+        }
+        if (lane == 31)
+            s_w[warp] = incl;
+        __syncthreads();
+        uint32_t pre = 0;
+        for (int k = 0; k < warp; ++k)
+            pre = s_w[k] > pre ? s_w[k] : pre;
+        uint32_t before = __shfl_up_sync(0xffffffffu, incl, 1);
+        if (lane == 0)
+            before = 0;
+        before = before > pre ? before : pre; /* max over earlier threads */
+        /* this thread's 16 entries */
+        const uint64_t j0 = lo + (uint64_t)threadIdx.x * kTileE;
+        uint32_t c[kTileE];
+        if (j0 + kTileE <= E.m) {
+            const uint4 *c4 = reinterpret_cast<const uint4 *>(E.col + j0);
+#pragma unroll
+            for (int q = 0; q < kTileE / 4; ++q) {
+                const uint4 x = __ldg(c4 + q);
+                c[4 * q] = x.x;
+                c[4 * q + 1] = x.y;
+                c[4 * q + 2] = x.z;
+                c[4 * q + 3] = x.w;
             }
+        } else {
+#pragma unroll
+            for (int k = 0; k < kTileE; ++k)
+                c[k] = j0 + k < E.m ? __ldg(E.col + j0 + k) : 0u;
         }
-        unsigned big = __ballot_sync(0xffffffffu, deg >= 32);
-        while (big) {
-            int src = __ffs(big) - 1;
-            big &= big - 1;
-            uint64_t bb = __shfl_sync(0xffffffffu, beg, src);
-            uint64_t ee = __shfl_sync(0xffffffffu, end, src);
-            int pp = __shfl_sync(0xffffffffu, p, src);
-            uint32_t ll = __shfl_sync(0xffffffffu, lo, src);
-            uint32_t hh = __shfl_sync(0xffffffffu, hi, src);
-            uint32_t rr = __shfl_sync(0xffffffffu, rep, src);
-            for (uint64_t j0 = bb; j0 < ee; j0 += 32) {
-                uint64_t j = j0 + lane;
-                uint32_t u = j < ee ? __ldg(E.col + j) : E.n;
-                bool bnd = u < E.n && (u < ll || u >= hh);
-                bool gnt = bnd && rr + ll == s_gl[pp];
-                if (gnt)
-                    bitmap_set(E, pp, u);
-                raw += bnd;
-                wb_append(w, E, lane, bnd && !gnt, make_key(E, pp, u, rr));
+        uint32_t row = 0xffffffffu, bits = 0;
+        int pu = 0;
+        uint32_t cur = before;
+#pragma unroll
+        for (int k = 0; k < kTileE; ++k) {
+            const uint32_t h = s_head[HP(threadIdx.x * kTileE + k)];
+            cur = h > cur ? h : cur;
+            const uint32_t v = c[k];
+            const bool ok = j0 + k < E.m && cur < E.n && v < E.n;
+            if (ok && cur != row) {
+                if (bits)
+                    mask_or(E.pmask + row, bits);
+                bits = 0;
+                row = cur;
+                pu = part_fast<PMAX>(s_b, sb, E.parts, row);
             }
-        }
-        uint32_t sdeg = deg < 32 ? (uint32_t)deg : 0u;
-        uint32_t maxd = __reduce_max_sync(0xffffffffu, sdeg);
-        for (uint32_t it = 0; it < maxd; ++it) {
-            uint32_t u = it < sdeg ? __ldg(E.col + beg + it) : E.n;
-            bool bnd = u < E.n && (u < lo || u >= hi);
-            bool gnt = bnd && rep + lo == s_gl[p];
+            const int pv = ok ? part_fast<PMAX>(s_b, sb, E.parts, v) : 0;
+            const bool bnd = ok && pv != pu;
+            bool gnt = false;
+            if (bnd && E.gflag)
+                gnt = (__ldg(E.gflag + (v >> 5)) >> (v & 31)) & 1u;
             if (gnt)
-                bitmap_set(E, p, u);
+                bits |= 1u << pv;
             raw += bnd;
-            wb_append(w, E, lane, bnd && !gnt, make_key(E, p, u, rep));
+            uint64_t key = 0;
+            if (bnd && !gnt)
+                key = make_key(E, pv, row, __ldg(E.label + v) - s_b[pv]);
+            wb_append(w, E, lane, bnd && !gnt, key);
         }
+        if (bits)
+            mask_or(E.pmask + row, bits);
+        __syncthreads();
     }
     wb_flush(w, E, lane);
     add_raw(E, raw, lane);
 }
 
-__global__ void __launch_bounds__(kB) k_emit_heavy(EmitParams E)
-{
-    __shared__ uint64_t s_buf[kW][kEmitBuf];
-    __shared__ uint32_t s_b[CCGPU_MAX_PARTS + 1];
-    __shared__ uint32_t s_gl[CCGPU_MAX_PARTS];
-    for (int i = threadIdx.x; i <= E.parts; i += kB)
-        s_b[i] = E.bounds[i];
-    load_giant_labels(E, s_gl);
-    unsigned long long raw = 0;
-    __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    WarpBuf w = {s_buf[warp], 0};
-    uint32_t cnt = *E.heavy_count;
-    if (cnt > E.heavy_cap)
-        cnt = E.heavy_cap;
-    cc_for_heavy_pieces(E.heavy_list, cnt, E.row_ptr, E.m, 0, kHeavyChunk,
-                        [&](uint32_t v, uint64_t jb, uint64_t je) {
-                            const int p = part_of(s_b, E.parts, v);
-                            const uint32_t lo = s_b[p], hi = s_b[p + 1];
-                            const uint32_t rep = __ldg(E.label + v) - lo;
-                            for (uint64_t j0 = jb; j0 < je; j0 += 32) {
-                                uint64_t j = j0 + lane;
-                                uint32_t u = j < je ? __ldg(E.col + j) : E.n;
-                                bool bnd = u < E.n && (u < lo || u >= hi);
-                                bool gnt = bnd && rep + lo == s_gl[p];
-                                if (gnt)
-                                    bitmap_set(E, p, u);
-                                raw += bnd;
-                                wb_append(w, E, lane, bnd && !gnt, make_key(E, p, u, rep));
-                            }
-                        });
-    wb_flush(w, E, lane);
-    add_raw(E, raw, lane);
-}
-
-/* One key (p, remote, giant rep of p) per set bit of the giant bitmap,
- * appended after the keys k_emit wrote (the sort orders them). */
-__global__ void __launch_bounds__(kB) k_bitmap_keys(EmitParams E)
+/* One key (p, u, giant rep of p) per bit p of pmask[u], appended after the
+ * keys k_emit wrote (the sort orders them). */
+__global__ void __launch_bounds__(kB) k_mask_keys(EmitParams E)
 {
     __shared__ uint32_t s_b[CCGPU_MAX_PARTS + 1];
     __shared__ uint32_t s_gl[CCGPU_MAX_PARTS];
@@ -332,15 +388,14 @@ __global__ void __launch_bounds__(kB) k_bitmap_keys(EmitParams E)
     load_giant_labels(E, s_gl);
     __syncthreads();
     const int lane = threadIdx.x & 31;
-    const uint64_t total = (uint64_t)E.parts * E.bm_words;
     const uint64_t stride = (uint64_t)gridDim.x * kB;
-    for (uint64_t base = (uint64_t)blockIdx.x * kB; base < total; base += stride) {
-        const uint64_t i = base + threadIdx.x;
-        uint32_t word = i < total ? E.bitmap[i] : 0u;
-        uint32_t c = __popc(word);
+    for (uint64_t b0 = (uint64_t)blockIdx.x * kB; b0 < E.n; b0 += stride) {
+        const uint64_t u = b0 + threadIdx.x;
+        uint32_t bits = u < E.n ? E.pmask[u] : 0u;
+        const uint32_t c = __popc(bits);
         uint32_t incl = c;
         for (int o = 1; o < 32; o <<= 1) {
-            uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
             if (lane >= o)
                 incl += y;
         }
@@ -349,16 +404,233 @@ __global__ void __launch_bounds__(kB) k_bitmap_keys(EmitParams E)
         if (lane == 31 && wtot)
             at = atomicAdd(E.count, (unsigned long long)wtot);
         at = __shfl_sync(0xffffffffu, at, 31) + (incl - c);
-        if (word) {
-            const int p = (int)(i / E.bm_words);
-            const uint32_t u0 = (uint32_t)((i - (uint64_t)p * E.bm_words) << 5);
-            const uint32_t rep = s_gl[p] - s_b[p];
-            while (word) {
-                const int b = __ffs(word) - 1;
-                word &= word - 1;
-                E.out[at++] = make_key(E, p, u0 + (uint32_t)b, rep);
-            }
+        while (bits) {
+            const int p = __ffs(bits) - 1;
+            bits &= bits - 1;
+            E.out[at++] = make_key(E, p, (uint32_t)u, s_gl[p] - s_b[p]);
         }
+    }
+}
+
+/* ------------------------------------------------------ local subgraph */
+
+/* The local CSR of every partition (src/cc_mpi.c:252-297: the entries of a
+ * vertex whose other end lies in the same partition), built by streaming
+ * the column array in tiles of kTile entries.  Partitions are contiguous
+ * vertex ranges, so partition p's rows fill the contiguous column range
+ * [pcol[p], pcol[p+1]) with pcol[p] = row_ptr[bounds[p]]: whether an entry
+ * is kept depends only on its position, and the stream needs no row
+ * lookup.  Pass 1 counts kept entries per tile; after a scan of the tile
+ * counts, pass 2 compacts each tile in order and gives every row whose start
+ * falls in the tile its local row pointer.  Ids stay global; one CSR over
+ * all n vertices holds every partition's subgraph.  Both passes read the
+ * columns with 16-byte loads, fully coalesced. */
+
+struct LocalParams {
+    const uint64_t *row_ptr;
+    const uint32_t *col;
+    uint32_t n;
+    uint64_t m;
+    const uint32_t *bounds;     /* [parts+1] vertex bounds            */
+    const uint64_t *pcol;       /* [parts+1] column bounds            */
+    int parts;
+    uint64_t tiles;
+    uint32_t *tile_cnt;         /* [tiles] kept entries per tile      */
+    const uint64_t *tile_off;   /* [tiles+1] scanned                  */
+    uint32_t *tile_first;       /* [tiles+1] first row starting after the tile's first entry */
+    uint64_t *lrp;              /* [n+1] local row pointers           */
+    uint32_t *lcol;             /* [tile_off[tiles]] kept entries     */
+};
+
+/* tile_first[t] = smallest v with row_ptr[v] > t * kTile (v in [0, n]),
+ * tile_first[tiles] = n + 1. */
+__global__ void __launch_bounds__(kB) k_tile_first(LocalParams L)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * kB;
+    for (uint64_t v = (uint64_t)blockIdx.x * kB + threadIdx.x; v <= L.n; v += stride) {
+        if (v == 0) {
+            /* tiles before the first row or after the last one hold no row
+             * start (only for a row_ptr that does not span [0, m]) */
+            L.tile_first[L.tiles] = L.n + 1;
+            uint64_t r0 = __ldg(L.row_ptr), rn = __ldg(L.row_ptr + L.n);
+            r0 = r0 > L.m ? L.m : r0;
+            rn = rn > L.m ? L.m : rn;
+            for (uint64_t t = 0; t * kTile < r0; ++t)
+                L.tile_first[t] = 0;
+            for (uint64_t t = (rn + kTile - 1) / kTile; t < L.tiles; ++t)
+                L.tile_first[t] = L.n + 1;
+            continue;
+        }
+        uint64_t a = __ldg(L.row_ptr + v - 1), b = __ldg(L.row_ptr + v);
+        if (b > L.m)
+            b = L.m;
+        if (a > b)
+            a = b;
+        /* tiles whose first entry t*kTile lies in [a, b) */
+        for (uint64_t t = (a + kTile - 1) / kTile; t * kTile < b; ++t)
+            L.tile_first[t] = (uint32_t)v;
+    }
+}
+
+/* Partition whose column range holds position j (pcol ascending). */
+__device__ __forceinline__ int part_at(const uint64_t *s_pcol, int parts, uint64_t j)
+{
+    int lo = 0, hi = parts;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (s_pcol[mid] <= j)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+/* The kTileE entries of thread t of tile `tile`: kept mask (bit k = entry k)
+ * and values. */
+__device__ __forceinline__ uint32_t tile_keep(const LocalParams &L, const uint32_t *s_b,
+                                              const uint64_t *s_pcol, uint64_t tile,
+                                              uint32_t *u)
+{
+    const uint64_t j0 = tile * kTile + (uint64_t)threadIdx.x * kTileE;
+    if (j0 + kTileE <= L.m) {
+        const uint4 *c4 = reinterpret_cast<const uint4 *>(L.col + j0);
+#pragma unroll
+        for (int q = 0; q < kTileE / 4; ++q) {
+            const uint4 x = __ldg(c4 + q);
+            u[4 * q] = x.x;
+            u[4 * q + 1] = x.y;
+            u[4 * q + 2] = x.z;
+            u[4 * q + 3] = x.w;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < kTileE; ++k)
+            u[k] = j0 + k < L.m ? __ldg(L.col + j0 + k) : 0u;
+    }
+    int p = j0 < L.m ? part_at(s_pcol, L.parts, j0) : 0;
+    uint64_t pend = s_pcol[p + 1];
+    uint32_t mask = 0;
+#pragma unroll
+    for (int k = 0; k < kTileE; ++k) {
+        const uint64_t j = j0 + k;
+        if (j >= L.m)
+            break;
+        while (j >= pend && p < L.parts - 1) { /* crossed into the next partition */
+            ++p;
+            pend = s_pcol[p + 1];
+        }
+        if (u[k] >= s_b[p] && u[k] < s_b[p + 1])
+            mask |= 1u << k;
+    }
+    return mask;
+}
+
+__global__ void __launch_bounds__(kB) k_local_count(LocalParams L)
+{
+    __shared__ uint32_t s_b[CCGPU_MAX_PARTS + 1];
+    __shared__ uint64_t s_pcol[CCGPU_MAX_PARTS + 1];
+    __shared__ uint32_t s_w[kW];
+    for (int i = threadIdx.x; i <= L.parts; i += kB) {
+        s_b[i] = L.bounds[i];
+        s_pcol[i] = L.pcol[i];
+    }
+    __syncthreads();
+    for (uint64_t t = blockIdx.x; t < L.tiles; t += gridDim.x) {
+        uint32_t u[kTileE];
+        uint32_t c = __popc(tile_keep(L, s_b, s_pcol, t, u));
+        c = __reduce_add_sync(0xffffffffu, c);
+        if ((threadIdx.x & 31) == 0)
+            s_w[threadIdx.x >> 5] = c;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t sum = 0;
+            for (int k = 0; k < kW; ++k)
+                sum += s_w[k];
+            L.tile_cnt[t] = sum;
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kB) k_local_fill(LocalParams L)
+{
+    __shared__ uint32_t s_b[CCGPU_MAX_PARTS + 1];
+    __shared__ uint64_t s_pcol[CCGPU_MAX_PARTS + 1];
+    __shared__ uint32_t s_excl[kB + 1];
+    __shared__ uint32_t s_mask[kB];
+    __shared__ uint32_t s_w[kW];
+    for (int i = threadIdx.x; i <= L.parts; i += kB) {
+        s_b[i] = L.bounds[i];
+        s_pcol[i] = L.pcol[i];
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint64_t t = blockIdx.x; t < L.tiles; t += gridDim.x) {
+        uint32_t u[kTileE];
+        const uint32_t mask = tile_keep(L, s_b, s_pcol, t, u);
+        const uint32_t c = __popc(mask);
+        uint32_t incl = c;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o)
+                incl += y;
+        }
+        if (lane == 31)
+            s_w[warp] = incl;
+        __syncthreads();
+        uint32_t pre = 0, total = 0;
+#pragma unroll
+        for (int k = 0; k < kW; ++k) {
+            const uint32_t y = s_w[k];
+            pre += k < warp ? y : 0u;
+            total += y;
+        }
+        const uint32_t excl = pre + incl - c;
+        s_excl[threadIdx.x] = excl;
+        s_mask[threadIdx.x] = mask;
+        if (threadIdx.x == 0)
+            s_excl[kB] = total;
+        const uint64_t base = L.tile_off[t];
+        uint32_t k = excl;
+#pragma unroll
+        for (int q = 0; q < kTileE; ++q)
+            if (mask & (1u << q))
+                L.lcol[base + k++] = u[q];
+        __syncthreads();
+        /* local row pointers of the rows starting in (tile start, tile end] */
+        const uint64_t lo = t * kTile;
+        const uint32_t v0 = L.tile_first[t], v1 = L.tile_first[t + 1];
+        for (uint64_t v = (uint64_t)v0 + threadIdx.x; v < v1; v += kB) {
+            uint64_t rp = __ldg(L.row_ptr + v);
+            if (rp > L.m)
+                rp = L.m;
+            const uint32_t pos = (uint32_t)(rp - lo); /* in (0, kTile] */
+            uint32_t kb;
+            if (pos >= kTile) {
+                kb = total;
+            } else {
+                const uint32_t q = pos / kTileE, bit = pos % kTileE;
+                kb = s_excl[q] + __popc(s_mask[q] & ((1u << bit) - 1u));
+            }
+            L.lrp[v] = base + kb;
+        }
+        /* rows that start at position 0 (no entries before them) */
+        if (t == 0)
+            for (uint32_t v = threadIdx.x; v < v0; v += kB)
+                L.lrp[v] = 0;
+        __syncthreads();
+    }
+}
+
+/* pcol[p] = row_ptr[bounds[p]] (clamped to m): the column range of each
+ * partition's rows. */
+__global__ void k_part_cols(const uint64_t *row_ptr, uint64_t m, const uint32_t *bounds,
+                            int parts, uint64_t *pcol)
+{
+    for (int p = threadIdx.x; p <= parts; p += blockDim.x) {
+        uint64_t x = row_ptr[bounds[p]];
+        pcol[p] = x > m ? m : x;
     }
 }
 
@@ -654,8 +926,11 @@ __global__ void __launch_bounds__(kB) k_upd(MergeParams M)
 __global__ void __launch_bounds__(kB) k_pack(MergeParams M)
 {
     __shared__ uint32_t s_b[CCGPU_MAX_PARTS + 1];
-    for (int i = threadIdx.x; i <= M.parts; i += kB)
+    __shared__ uint64_t s_gh[CCGPU_MAX_PARTS + 1];
+    for (int i = threadIdx.x; i <= M.parts; i += kB) {
         s_b[i] = M.bounds[i];
+        s_gh[i] = M.gh_off[i];
+    }
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const uint64_t stride = (uint64_t)gridDim.x * kB;
@@ -670,7 +945,7 @@ __global__ void __launch_bounds__(kB) k_pack(MergeParams M)
             int lo = 0, hi = M.parts; /* partition p whose ghost range holds g */
             while (hi - lo > 1) {
                 int mid = (lo + hi) >> 1;
-                if (M.gh_off[mid] <= g)
+                if (s_gh[mid] <= g)
                     lo = mid;
                 else
                     hi = mid;
@@ -741,6 +1016,79 @@ __global__ void __launch_bounds__(kB) k_scatter(MergeParams M)
             if (lbl < M.hook[r])
                 atomicMin(M.hook + r, lbl);
         }
+    }
+}
+
+/* Receiver side over the sent messages only, for up to 16 partitions: the
+ * (q -> p) region holds msg_count[q*P+p] messages from its start, so a
+ * block scans the P*P counts in shared memory and walks the flattened
+ * message index; ghost_labels and the hook minima are updated as in
+ * k_scatter. */
+constexpr int kSmallParts = 16;
+
+__global__ void __launch_bounds__(kB) k_scatter_sent(MergeParams M)
+{
+    __shared__ uint64_t s_seg[kSmallParts * kSmallParts];   /* region start, p-major */
+    __shared__ uint32_t s_pre[kSmallParts * kSmallParts + 1]; /* messages before region */
+    const int P = M.parts, R = P * P;
+    if (threadIdx.x == 0) {
+        uint32_t acc = 0;
+        for (int r = 0; r < R; ++r) {
+            const int p = r / P, q = r % P;
+            s_seg[r] = M.seg[(uint64_t)p * (P + 1) + q];
+            s_pre[r] = acc;
+            acc += M.msg_count[q * P + p];
+        }
+        s_pre[R] = acc;
+    }
+    __syncthreads();
+    const uint32_t total = s_pre[R];
+    const int lane = threadIdx.x & 31;
+    const uint64_t stride = (uint64_t)gridDim.x * kB;
+    for (uint64_t base = (uint64_t)blockIdx.x * kB; base < total; base += stride) {
+        const uint64_t i = base + threadIdx.x;
+        const bool has = i < total;
+        uint64_t k0 = 0, k1 = 0;
+        uint32_t lbl = 0;
+        if (has) {
+            int lo = 0, hi = R; /* last region with s_pre <= i */
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (s_pre[mid] <= i)
+                    lo = mid;
+                else
+                    hi = mid;
+            }
+            const uint64_t rstart = s_seg[lo];
+            const uint64_t pr = M.msg[rstart + (i - s_pre[lo])];
+            const uint64_t g = rstart + (pr >> 32);
+            lbl = (uint32_t)pr;
+            M.ghost_labels[g] = lbl;
+            k0 = M.ghost_pairs[g];
+            k1 = M.ghost_pairs[g + 1];
+        }
+        /* hook minima, one pair per lane per step: lanes whose pairs share a
+         * rep (most cut pairs of a partition carry its giant rep) combine
+         * their labels first and one of them issues the atomicMin.  Hook
+         * values only decrease, so a plain read that is already <= the
+         * minimum means the atomic would change nothing. */
+        uint64_t nk = k1 - k0;
+        uint64_t steps = nk;
+        for (int o = 16; o > 0; o >>= 1) {
+            const uint64_t y = __shfl_xor_sync(0xffffffffu, steps, o);
+            steps = y > steps ? y : steps;
+        }
+        for (uint64_t t = 0; t < steps; ++t) {
+            const bool act = t < nk;
+            const uint32_t r = act ? M.pair_rep[k0 + t] : 0xffffffffu;
+            const unsigned peers = __match_any_sync(0xffffffffu, r);
+            const uint32_t mn = __reduce_min_sync(peers, act ? lbl : 0xffffffffu);
+            if (act && (__ffs(peers) - 1) == lane && mn < M.hook[r])
+                atomicMin(M.hook + r, mn);
+        }
+        const unsigned got = __popc(__ballot_sync(0xffffffffu, has));
+        if (lane == 0 && got)
+            atomicAdd(M.sent, (unsigned long long)got);
     }
 }
 
@@ -870,10 +1218,49 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
             max_local = hb[p + 1] - hb[p];
     CC_TRY(clock_mark(clk, st)); /* 1 */
 
-    /* 2. local CC of every partition's local subgraph */
+    /* 2. local CSR of every partition, then local CC on it */
     uint32_t *label = nullptr;
     CC_TRY(cc_bufs_get(&B, (void **)&label, (size_t)n * sizeof(uint32_t)));
-    LocalCCArgs a = {d_row_ptr, d_col, n, m, label, seg64, (uint32_t)P, {}, 1};
+    const uint64_t *l_rp = d_row_ptr;
+    const uint32_t *l_col = d_col;
+    uint64_t l_m = m;
+    uint32_t *tile_first = nullptr;
+    uint64_t col_tiles = 0;
+    if (P > 1 && m > 0) {
+        LocalParams Lp;
+        Lp.row_ptr = d_row_ptr;
+        Lp.col = d_col;
+        Lp.n = n;
+        Lp.m = m;
+        Lp.bounds = bounds;
+        Lp.parts = P;
+        Lp.tiles = (m + kTile - 1) / kTile;
+        uint64_t *pcol = nullptr, *tile_off = nullptr;
+        CC_TRY(cc_bufs_get(&B, (void **)&pcol, (P + 1) * sizeof(uint64_t)));
+        CC_TRY(cc_bufs_get(&B, (void **)&Lp.tile_cnt, Lp.tiles * sizeof(uint32_t)));
+        CC_TRY(cc_bufs_get(&B, (void **)&tile_off, (Lp.tiles + 1) * sizeof(uint64_t)));
+        CC_TRY(cc_bufs_get(&B, (void **)&Lp.tile_first, (Lp.tiles + 1) * sizeof(uint32_t)));
+        CC_TRY(cc_bufs_get(&B, (void **)&Lp.lrp, ((size_t)n + 1) * sizeof(uint64_t)));
+        CC_KLAUNCH(ctx, CCK_DIST_TILES, k_part_cols, 1, 32, 0, st, d_row_ptr, m, bounds, P, pcol);
+        Lp.pcol = pcol;
+        Lp.tile_off = tile_off;
+        Lp.lcol = nullptr;
+        const unsigned tb = cc_blocks(Lp.tiles, 1, (unsigned)ctx->sm_count * 8);
+        CC_KLAUNCH(ctx, CCK_DIST_LOCAL_COUNT, k_local_count, tb, kB, 0, st, Lp);
+        CC_KLAUNCH(ctx, CCK_DIST_TILES, k_tile_first,
+                   cc_blocks((uint64_t)n + 1, kB, (unsigned)ctx->sm_count * 8), kB, 0, st, Lp);
+        CC_TRY(cc_scan_u32(ctx, Lp.tile_cnt, tile_off, Lp.tiles, &B, st));
+        CC_CUDA(cudaMemcpyAsync(&l_m, tile_off + Lp.tiles, sizeof(uint64_t),
+                                cudaMemcpyDeviceToHost, st));
+        CC_CUDA(cudaStreamSynchronize(st));
+        CC_TRY(cc_bufs_get(&B, (void **)&Lp.lcol, (size_t)(l_m ? l_m : 1) * sizeof(uint32_t)));
+        CC_KLAUNCH(ctx, CCK_DIST_LOCAL_FILL, k_local_fill, tb, kB, 0, st, Lp);
+        l_rp = Lp.lrp;
+        l_col = Lp.lcol;
+        tile_first = Lp.tile_first;
+        col_tiles = Lp.tiles;
+    }
+    LocalCCArgs a = {l_rp, l_col, n, l_m, label, seg64, (uint32_t)P, {}, 0};
     ccgpu_cc_opts lo;
     ccgpu_cc_opts_default(&lo);
     lo.chunk_size = o.chunk_size;
@@ -921,31 +1308,33 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
     E.gb = gb;
     E.out = keys;
     E.count = counters;
-    E.heavy_deg = 16384;
-    E.heavy_cap = (uint32_t)(m / E.heavy_deg + 1);
-    CC_TRY(cc_bufs_get(&B, (void **)&E.heavy_list, (size_t)E.heavy_cap * sizeof(uint32_t)));
-    CC_TRY(cc_bufs_get(&B, (void **)&E.heavy_count, 256));
-    CC_CUDA(cudaMemsetAsync(E.heavy_count, 0, sizeof(uint32_t), st));
+    E.tiles = col_tiles;
+    E.tile_first = tile_first;
     E.raw = counters + 4;
-    /* giant bitmap: P bits per vertex, used while it stays small */
-    E.bm_words = ((uint64_t)n + 31) / 32;
+    /* giant flags and per-vertex partition masks (P <= 32) */
+    E.gflag = nullptr;
+    E.pmask = nullptr;
     E.giants = nullptr;
-    E.bitmap = nullptr;
-    const bool use_bitmap = P > 1 && a.o.sample_rounds > 0 && a.o.skip_giant &&
-                            (uint64_t)P * E.bm_words * 4 <= (1ull << 31);
-    if (use_bitmap) {
-        CC_TRY(cc_bufs_get(&B, (void **)&E.bitmap, (size_t)P * E.bm_words * 4));
-        CC_CUDA(cudaMemsetAsync(E.bitmap, 0, (size_t)P * E.bm_words * 4, st));
+    const bool use_mask = P > 1 && P <= 32 && a.o.sample_rounds > 0 && a.o.skip_giant;
+    if (use_mask) {
+        CC_TRY(cc_bufs_get(&B, (void **)&E.gflag, (((size_t)n + 31) / 32) * 4));
+        CC_TRY(cc_bufs_get(&B, (void **)&E.pmask, (size_t)n * 4));
+        CC_CUDA(cudaMemsetAsync(E.pmask, 0, (size_t)n * 4, st));
         E.giants = ls.giants;
+        CC_KLAUNCH(ctx, CCK_DIST_GFLAG, k_giant_flags,
+                   cc_blocks(n, kB, (unsigned)ctx->sm_count * 8), kB, 0, st, E);
     }
-    if (P > 1) {
-        const unsigned eb = (unsigned)ctx->sm_count * 4;
-        CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit, eb, kB, 0, st, E);
-        CC_KLAUNCH(ctx, CCK_DIST_PAIRS_HEAVY, k_emit_heavy, eb, kB, 0, st, E);
-        if (use_bitmap)
-            CC_KLAUNCH(ctx, CCK_DIST_PAIRS_BITMAP, k_bitmap_keys,
-                       cc_blocks((uint64_t)P * E.bm_words, kB, (unsigned)ctx->sm_count * 8), kB,
-                       0, st, E);
+    if (P > 1 && col_tiles) {
+        const unsigned eb = cc_blocks(col_tiles, 1, (unsigned)ctx->sm_count * 4);
+        if (P <= 4)
+            CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit<4>, eb, kB, 0, st, E);
+        else if (P <= 8)
+            CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit<8>, eb, kB, 0, st, E);
+        else
+            CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit<CCGPU_MAX_PARTS>, eb, kB, 0, st, E);
+        if (use_mask)
+            CC_KLAUNCH(ctx, CCK_DIST_PAIRS_BITMAP, k_mask_keys,
+                       cc_blocks(n, kB, (unsigned)ctx->sm_count * 8), kB, 0, st, E);
     }
     unsigned long long hc[5];
     CC_CUDA(cudaMemcpyAsync(hc, counters, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
@@ -953,6 +1342,8 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
     CC_CUDA(cudaStreamSynchronize(st));
     const uint64_t R = hc[0];
     S.boundary_raw = hc[4];
+    S.sorted_keys = R;
+    S.local_entries = l_m;
     S.rep_count = hc[1];
     CC_TRY(clock_mark(clk, st)); /* 3 */
 
@@ -1104,8 +1495,12 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
         if (steps >= interval || !any_changed) {
             M.cur = pc;
             CC_KLAUNCH(ctx, CCK_MERGE_EXCH_PACK, k_pack, cc_blocks(G, kB, gbk), kB, 0, st, M);
-            CC_KLAUNCH(ctx, CCK_MERGE_EXCH_SCATTER, k_scatter, cc_blocks(G, kB, gbk), kB, 0, st,
-                       M);
+            if (P <= kSmallParts)
+                CC_KLAUNCH(ctx, CCK_MERGE_EXCH_SCATTER, k_scatter_sent, cc_blocks(G, kB, gbk), kB,
+                           0, st, M);
+            else
+                CC_KLAUNCH(ctx, CCK_MERGE_EXCH_SCATTER, k_scatter, cc_blocks(G, kB, gbk), kB, 0,
+                           st, M);
             CC_CUDA(cudaMemsetAsync(M.msg_count, 0, (size_t)P * P * sizeof(uint32_t), st));
             S.exchanges++;
             for (int p = 0; p < P; ++p)

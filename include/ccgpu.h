@@ -213,6 +213,8 @@ typedef struct {
     uint64_t roots;         /* components of the whole graph                */
     uint64_t sent_pairs;    /* (position, label) pairs moved in exchanges   */
     double ms_bounds, ms_local, ms_pairs, ms_sort, ms_ghosts, ms_merge, ms_total;
+    uint64_t sorted_keys;   /* boundary keys the radix sort ordered         */
+    uint64_t local_entries; /* entries of the partitions' local subgraphs   */
 } ccgpu_dist_stats;
 
 void ccgpu_dist_opts_default(ccgpu_dist_opts *opts);
