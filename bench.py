@@ -52,6 +52,10 @@ WORKLOADS = {
     # plus 5% R-MAT scale-22 requests
     "served": dict(kind="served", pool=512, n_min=1_000, n_max=2_000_000, big_scale=22,
                    big_frac=0.05, seconds=6.0, served=True),
+    # the same server on small requests (1k-50k vertices, no large ones),
+    # where per-request launch and copy overheads dominate
+    "served_small": dict(kind="served", pool=1024, n_min=1_000, n_max=50_000, big_scale=22,
+                         big_frac=0.0, seconds=6.0, served=True),
 }
 L2_BYTES = 126 * 1024 * 1024
 FALLBACK_HBM_GBS = 6650.0
@@ -730,7 +734,8 @@ def run_served(args, torch, dist_mod, rank, world, dev):
     t0 = time.perf_counter()
     spec = batch.mix_spec(spec_w["pool"], spec_w["n_min"], spec_w["n_max"],
                           seed=args.seed + rank)
-    spec += [("rmat", 1 << spec_w["big_scale"], args.seed + 1000 + i) for i in range(4)]
+    nbig = 4 if spec_w["big_frac"] > 0 else 0
+    spec += [("rmat", 1 << spec_w["big_scale"], args.seed + 1000 + i) for i in range(nbig)]
     pool, want_comps, want_labels = [], [], []
     for kind, n, seed in spec:
         rp_d, col_d = batch.build_one_torch(torch, kind, n, seed)
@@ -747,12 +752,12 @@ def run_served(args, torch, dist_mod, rank, world, dev):
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
     gen_s = time.perf_counter() - t0
-    P = len(spec) - 4
+    P = len(spec) - nbig
     rng = np.random.default_rng(args.seed)
     # request order: a mix graph, or with probability big_frac a scale-22 R-MAT
-    nreq = 200000
+    nreq = 400000
     big = rng.random(nreq) < spec_w["big_frac"]
-    order = np.where(big, P + rng.integers(0, 4, nreq), rng.integers(0, P, nreq))
+    order = np.where(big, P + rng.integers(0, max(nbig, 1), nreq), rng.integers(0, P, nreq))
     seconds = spec_w["seconds"]
     entries = np.array([len(c) for _, c in pool])
     log(f"served: pool of {len(pool)} graphs built in {gen_s:.1f} s")
@@ -764,7 +769,8 @@ def run_served(args, torch, dist_mod, rank, world, dev):
         srv = serve.Server(**srv_kw)
         # warm-up and capacity: a closed loop of requests submitted at once
         serve_run(srv, pool, order[:64], 0, 0, want_comps, want_labels, 16, closed=True)
-        cap_n = 1500 if srv_kw.get("max_batch", 4096) > 1 else 300
+        cap_n = (1500 if srv_kw.get("max_batch", 4096) > 1 else 300) * \
+            (8 if spec_w["n_max"] <= 100_000 else 1)
         cap = serve_run(srv, pool, order[64:64 + cap_n], 0, 0, want_comps, want_labels, 16,
                         closed=True)
         out = {"capacity_graphs_per_s": cap["graphs_per_s"], "capacity_bad": cap["bad"]}
@@ -792,8 +798,8 @@ def run_served(args, torch, dist_mod, rank, world, dev):
     runs, runs1 = [], []
     for i, frac in enumerate((0.70, 0.95)):
         rate = frac * capacity
-        runs.append(dict(load=frac, **poisson(kw, rate, 2000 + i * 60000)))
-        runs1.append(dict(load=frac, **poisson(kw1, rate, 2000 + i * 60000)))
+        runs.append(dict(load=frac, **poisson(kw, rate, 20000 + i * 180000)))
+        runs1.append(dict(load=frac, **poisson(kw1, rate, 20000 + i * 180000)))
     ok = all(r["mismatches"] == 0 for r in runs + runs1) and cap_b["capacity_bad"] == 0 and \
         cap_1["capacity_bad"] == 0
     if rank == 0:
@@ -804,8 +810,10 @@ def run_served(args, torch, dist_mod, rank, world, dev):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic",
             "config": {"workload": args.workload, "pool_graphs": len(pool),
-                       "request_mix": "batched mix (log-uniform 1k-2M vertices, ER/R-MAT/grid "
-                                      "thirds) + 5% R-MAT scale-22",
+                       "request_mix": f"log-uniform {spec_w['n_min']}-{spec_w['n_max']} "
+                                      "vertices, ER/R-MAT/grid thirds" +
+                                      (f" + {int(spec_w['big_frac'] * 100)}% R-MAT scale "
+                                       f"{spec_w['big_scale']}" if nbig else ""),
                        "arrivals": "Poisson at 0.70 and 0.95 x measured capacity",
                        "seconds_per_run": seconds, "server": kw, "build_s": gen_s,
                        "verified": ok},
