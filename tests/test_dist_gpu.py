@@ -90,6 +90,17 @@ def test_many_partitions_and_er(torch):
         check_against_oracle(torch, rp, col, parts, 0, 3)
 
 
+@pytest.mark.parametrize("parts", [5, 9, 17, 33])
+def test_rmat_partition_widths(torch, parts):
+    """Every code path by partition count: the partition lookup specialised
+    for <= 4 / <= 8 / more partitions, the message scatter over sent
+    messages (<= 16) or over all ghosts, and the giant masks (<= 32) or
+    plain keys; R-MAT hubs put long rows across column tiles."""
+    rp, col = graphs.rmat_csr(13, 16, seed=40 + parts)
+    for interval in (1, 3):
+        check_against_oracle(torch, rp, col, parts, 1, interval)
+
+
 def test_bounds_match_reference_restatement(torch):
     rp, col = graphs.rmat_csr(12, 8, seed=6)
     d_rp, _ = dev(torch, rp, col)
