@@ -638,7 +638,7 @@ __global__ void k_part_cols(const uint64_t *row_ptr, uint64_t m, const uint32_t 
 
 __global__ void __launch_bounds__(kB) k_reps(const uint32_t *__restrict__ label, uint32_t n,
                                              uint32_t *rep_list, unsigned long long *rep_count,
-                                             uint32_t *cur, uint32_t *hook)
+                                             uint32_t *cur, uint32_t *nxt, uint32_t *hook)
 {
     const int lane = threadIdx.x & 31;
     const uint64_t stride = (uint64_t)gridDim.x * kB;
@@ -653,8 +653,40 @@ __global__ void __launch_bounds__(kB) k_reps(const uint32_t *__restrict__ label,
         if (is_rep) {
             rep_list[slot + __popc(mask & ((1u << lane) - 1u))] = (uint32_t)v;
             cur[v] = (uint32_t)v; /* comp_label[i] = v_start + i, src/cc_mpi.c:361-362 */
+            nxt[v] = (uint32_t)v; /* reps no round updates keep it in both buffers */
             hook[v] = 0xffffffffu;
         }
+    }
+}
+
+/* Reps that own at least one boundary pair.  A rep without one has no hook
+ * and its own label as its only jump target, so a merge round never
+ * changes it (src/cc_mpi.c:575-622): the rounds walk only the others. */
+__global__ void __launch_bounds__(kB) k_mark_pair_reps(const uint32_t *__restrict__ pair_rep,
+                                                       uint64_t pairs, uint8_t *flag)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * kB;
+    for (uint64_t k = (uint64_t)blockIdx.x * kB + threadIdx.x; k < pairs; k += stride)
+        flag[__ldg(pair_rep + k)] = 1;
+}
+
+__global__ void __launch_bounds__(kB) k_active_reps(const uint32_t *__restrict__ rep_list,
+                                                    uint64_t reps, const uint8_t *flag,
+                                                    uint32_t *act, unsigned long long *act_count)
+{
+    const int lane = threadIdx.x & 31;
+    const uint64_t stride = (uint64_t)gridDim.x * kB;
+    for (uint64_t base = (uint64_t)blockIdx.x * kB; base < reps; base += stride) {
+        const uint64_t i = base + threadIdx.x;
+        const uint32_t r = i < reps ? __ldg(rep_list + i) : 0u;
+        const bool a = i < reps && flag[r];
+        const unsigned mask = __ballot_sync(0xffffffffu, a);
+        unsigned long long slot = 0;
+        if (lane == 0 && mask)
+            slot = atomicAdd(act_count, (unsigned long long)__popc(mask));
+        slot = __shfl_sync(0xffffffffu, slot, 0);
+        if (a)
+            act[slot + __popc(mask & ((1u << lane) - 1u))] = r;
     }
 }
 
@@ -1284,7 +1316,7 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
     if (rb + gb + pb > 64)
         return ccgpu_set_error(CCGPU_ERR_LIMIT, "boundary key needs %d bits", rb + gb + pb);
     uint32_t *rep_list = nullptr, *cur = nullptr, *nxt = nullptr, *hook = nullptr;
-    unsigned long long *counters = nullptr; /* [0] keys [1] reps [2] roots [3] sent [4] raw */
+    unsigned long long *counters = nullptr; /* [0] keys [1] reps [2] roots [3] sent [4] raw [5] active reps */
     CC_TRY(cc_bufs_get(&B, (void **)&rep_list, (size_t)n * sizeof(uint32_t)));
     CC_TRY(cc_bufs_get(&B, (void **)&cur, (size_t)n * sizeof(uint32_t)));
     CC_TRY(cc_bufs_get(&B, (void **)&nxt, (size_t)n * sizeof(uint32_t)));
@@ -1293,7 +1325,7 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
     CC_CUDA(cudaMemsetAsync(counters, 0, 8 * sizeof(unsigned long long), st));
     const unsigned sb = cc_blocks(n, kB, (unsigned)ctx->sm_count * 8);
     CC_KLAUNCH(ctx, CCK_DIST_REPS, k_reps, sb, kB, 0, st, label, n, rep_list, counters + 1, cur,
-               hook);
+               nxt, hook);
     uint64_t *keys = nullptr, *alt = nullptr;
     CC_TRY(cc_bufs_get(&B, (void **)&keys, (size_t)(m ? m : 1) * sizeof(uint64_t)));
     EmitParams E;
@@ -1428,13 +1460,31 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
                S.sort_passes);
     }
 
-    /* 6. merge rounds */
+    /* 6. merge rounds, over the reps that own boundary pairs */
+    uint32_t *act = nullptr;
+    uint64_t act_count = 0;
+    if (U > 0) {
+        uint8_t *flag = nullptr;
+        CC_TRY(cc_bufs_get(&B, (void **)&flag, (size_t)n));
+        CC_TRY(cc_bufs_get(&B, (void **)&act, (size_t)S.rep_count * sizeof(uint32_t) + 4));
+        CC_CUDA(cudaMemsetAsync(flag, 0, (size_t)n, st));
+        CC_CUDA(cudaMemsetAsync(counters + 5, 0, sizeof(unsigned long long), st));
+        const unsigned gb2 = (unsigned)ctx->sm_count * 8;
+        CC_KLAUNCH(ctx, CCK_MERGE_INIT, k_mark_pair_reps, cc_blocks(U, kB, gb2), kB, 0, st,
+                   D.pair_rep, U, flag);
+        CC_KLAUNCH(ctx, CCK_MERGE_INIT, k_active_reps, cc_blocks(S.rep_count, kB, gb2), kB, 0,
+                   st, rep_list, S.rep_count, flag, act, counters + 5);
+        unsigned long long ac = 0;
+        CC_CUDA(cudaMemcpyAsync(&ac, counters + 5, sizeof(ac), cudaMemcpyDeviceToHost, st));
+        CC_CUDA(cudaStreamSynchronize(st));
+        act_count = ac;
+    }
     MergeParams M;
     M.label = label;
     M.bounds = bounds;
     M.parts = P;
-    M.rep_list = rep_list;
-    M.rep_count = S.rep_count;
+    M.rep_list = act;
+    M.rep_count = act_count;
     M.hook = hook;
     M.pair_rep = D.pair_rep;
     M.pair_g = D.pair_g;
@@ -1461,7 +1511,7 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
      * and reps; a partition with none joins the rounds and exchanges
      * without effect (the reference would stall there). */
     std::vector<int> pending(P, 0), changed(P, 0);
-    int global_pending = (G > 0 && U > 0 && S.rep_count > 0) ? 1 : 0;
+    int global_pending = (G > 0 && U > 0 && act_count > 0) ? 1 : 0;
     for (int p = 0; p < P; ++p)
         pending[p] = global_pending;
     int steps = 0;
@@ -1470,7 +1520,7 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
         M.cur = pc;
         M.next = pn;
         CC_CUDA(cudaMemsetAsync(M.changed, 0, P * sizeof(int), st));
-        CC_KLAUNCH(ctx, CCK_MERGE_UPD, k_upd, cc_blocks(S.rep_count, kB, gbk), kB, 0, st, M);
+        CC_KLAUNCH(ctx, CCK_MERGE_UPD, k_upd, cc_blocks(act_count, kB, gbk), kB, 0, st, M);
         CC_CUDA(cudaMemcpyAsync(changed.data(), M.changed, P * sizeof(int),
                                 cudaMemcpyDeviceToHost, st));
         CC_CUDA(cudaStreamSynchronize(st));
