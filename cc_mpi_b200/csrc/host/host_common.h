@@ -17,4 +17,17 @@ int ccb200_set_error(int status, const char *fmt, ...);
 void **cc_group_slots(cc_group *view);
 void cc_group_store_stats(cc_group *g, const ccgpu_dist_stats *s);
 
+/* Pairwise mailboxes of the neighbourhood exchanges.  post: this rank
+ * offers buf, with element offset off[q] and count cnt[q] for each reader
+ * rank q, to `readers` readers (waits first until its previous post has
+ * been read by all of its readers).  take: waits for src's next post and
+ * calls copy(arg, buf, off[me], cnt[me]).  drain: waits until this rank's
+ * post has been read by all of its readers.  Waits are bounded
+ * (CCB200_GROUP_TIMEOUT_S, default 600 s); a timeout returns
+ * CCGPU_ERR_TIMEOUT. */
+int cc_group_post(cc_group *view, const void *buf, const int *off, const int *cnt, int readers);
+int cc_group_take(cc_group *view, int src,
+                  void (*copy)(void *arg, const void *buf, int off, int cnt), void *arg);
+int cc_group_drain(cc_group *view);
+
 #endif
