@@ -285,13 +285,19 @@ __device__ __forceinline__ void warp_link_row(const LinkParams &P, uint32_t v, u
     }
 }
 
+/* Vertices a thread takes per step of the finish pass: consecutive, so a
+ * step covers kBlock * kVPT vertices and its barriers are paid once per
+ * kVPT vertices per thread. */
+constexpr int kVPT = 4;
+constexpr int kStep = kBlock * kVPT;
+
 template <bool LAZY>
 __global__ void __launch_bounds__(kBlock, 4) k_link_rows(LinkParams P)
 {
-    __shared__ uint32_t s_off[kBlock + 1];
-    __shared__ uint64_t s_beg[kBlock];
+    __shared__ uint32_t s_off[kStep + 1];
+    __shared__ uint64_t s_beg[kStep];
     __shared__ uint32_t s_wsum[kWarps];
-    __shared__ Span s_span[kBlock];
+    __shared__ Span s_span[kStep];
     __shared__ unsigned long long s_base;
 
     const uint32_t giant0 = (P.giants && P.nseg == 1) ? P.giants[0] : kNoGiant;
@@ -302,7 +308,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_link_rows(LinkParams P)
     uint64_t st_lo = 0, st_hi = 0;
     if (P.chunk == 0) {
         uint64_t per = ((uint64_t)P.n + gridDim.x - 1) / gridDim.x;
-        per = (per + kBlock - 1) / kBlock * kBlock;
+        per = (per + kStep - 1) / kStep * kStep;
         st_lo = per * blockIdx.x;
         st_hi = st_lo + per;
         if (st_lo > P.n)
@@ -330,48 +336,60 @@ __global__ void __launch_bounds__(kBlock, 4) k_link_rows(LinkParams P)
             base = st_lo;
             cend = st_hi;
         }
-        for (uint64_t t0 = base; t0 < cend; t0 += kBlock) {
-            const uint64_t v64 = t0 + threadIdx.x;
-            const uint32_t v = (uint32_t)v64;
-            uint64_t beg = 0, end = 0;
-            const Span sp = span_of(P.fseg, P.nseg, P.n, v64 < cend ? v64 : t0);
-            if (v64 < cend) {
-                uint32_t giant = giant0;
-                if (P.giants && P.nseg > 1)
-                    giant = P.giants[seg_of(P.seg, P.nseg, v64)];
-                if (giant == kNoGiant || cc_ldp(P.parent, v) != giant) {
-                    Rows r = row_of(P.row_ptr, v, P.m);
-                    beg = r.beg + P.skip_from;
-                    end = r.end;
-                    if (beg > end)
-                        beg = end;
-                    my_rows++;
-                    my_edges += end - beg;
+        for (uint64_t t0 = base; t0 < cend; t0 += kStep) {
+            /* this thread's kVPT consecutive vertices: slots kVPT*t + k */
+            uint64_t beg[kVPT], end[kVPT];
+            uint32_t small[kVPT];
+            uint32_t mine = 0;
+#pragma unroll
+            for (int k = 0; k < kVPT; ++k) {
+                const uint64_t v64 = t0 + (uint64_t)threadIdx.x * kVPT + k;
+                const uint32_t v = (uint32_t)v64;
+                beg[k] = end[k] = 0;
+                const Span sp = span_of(P.fseg, P.nseg, P.n, v64 < cend ? v64 : t0);
+                if (v64 < cend) {
+                    uint32_t giant = giant0;
+                    if (P.giants && P.nseg > 1)
+                        giant = P.giants[seg_of(P.seg, P.nseg, v64)];
+                    if (giant == kNoGiant || cc_ldp(P.parent, v) != giant) {
+                        Rows r = row_of(P.row_ptr, v, P.m);
+                        beg[k] = r.beg + P.skip_from;
+                        end[k] = r.end;
+                        if (beg[k] > end[k])
+                            beg[k] = end[k];
+                        my_rows++;
+                        my_edges += end[k] - beg[k];
+                    }
                 }
-            }
-            uint64_t deg = end - beg;
-            if (deg > P.heavy_deg) {
-                uint32_t slot = atomicAdd(&P.cnt->heavy_count, 1u);
-                if (slot < P.heavy_cap) {
-                    P.heavy_list[slot] = v;
-                    deg = 0;
+                uint64_t deg = end[k] - beg[k];
+                if (deg > P.heavy_deg) {
+                    uint32_t slot = atomicAdd(&P.cnt->heavy_count, 1u);
+                    if (slot < P.heavy_cap) {
+                        P.heavy_list[slot] = v;
+                        deg = 0;
+                        end[k] = beg[k];
+                    }
                 }
+                /* warp-cooperative rows */
+                unsigned big = __ballot_sync(0xffffffffu, deg >= 32);
+                while (big) {
+                    int src = __ffs(big) - 1;
+                    big &= big - 1;
+                    uint32_t vv = __shfl_sync(0xffffffffu, v, src);
+                    uint64_t bb = __shfl_sync(0xffffffffu, beg[k], src);
+                    uint64_t ee = __shfl_sync(0xffffffffu, end[k], src);
+                    Span ss = {__shfl_sync(0xffffffffu, sp.lo, src),
+                               __shfl_sync(0xffffffffu, sp.hi, src)};
+                    warp_link_row<LAZY>(P, vv, bb, ee, lane, ss);
+                }
+                small[k] = deg < 32 ? (uint32_t)deg : 0u;
+                mine += small[k];
+                s_beg[threadIdx.x * kVPT + k] = beg[k];
+                s_span[threadIdx.x * kVPT + k] = sp;
             }
-            /* warp-cooperative rows */
-            unsigned big = __ballot_sync(0xffffffffu, deg >= 32);
-            while (big) {
-                int src = __ffs(big) - 1;
-                big &= big - 1;
-                uint32_t vv = __shfl_sync(0xffffffffu, v, src);
-                uint64_t bb = __shfl_sync(0xffffffffu, beg, src);
-                uint64_t ee = __shfl_sync(0xffffffffu, end, src);
-                Span ss = {__shfl_sync(0xffffffffu, sp.lo, src),
-                           __shfl_sync(0xffffffffu, sp.hi, src)};
-                warp_link_row<LAZY>(P, vv, bb, ee, lane, ss);
-            }
-            /* short rows: CTA-wide gather, walked edge-parallel */
-            uint32_t small = deg < 32 ? (uint32_t)deg : 0u;
-            uint32_t incl = small;
+            /* short rows: CTA-wide gather over the step's slots, walked
+             * edge-parallel */
+            uint32_t incl = mine;
             for (int o = 1; o < 32; o <<= 1) {
                 uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
                 if (lane >= o)
@@ -379,8 +397,6 @@ __global__ void __launch_bounds__(kBlock, 4) k_link_rows(LinkParams P)
             }
             if (lane == 31)
                 s_wsum[warp] = incl;
-            s_beg[threadIdx.x] = beg;
-            s_span[threadIdx.x] = sp;
             __syncthreads();
             uint32_t wpre = 0, total = 0;
 #pragma unroll
@@ -389,12 +405,17 @@ __global__ void __launch_bounds__(kBlock, 4) k_link_rows(LinkParams P)
                 wpre += (w < warp) ? x : 0u;
                 total += x;
             }
-            s_off[threadIdx.x] = wpre + incl - small;
+            uint32_t run = wpre + incl - mine;
+#pragma unroll
+            for (int k = 0; k < kVPT; ++k) {
+                s_off[threadIdx.x * kVPT + k] = run;
+                run += small[k];
+            }
             if (threadIdx.x == 0)
-                s_off[kBlock] = total;
+                s_off[kStep] = total;
             __syncthreads();
             for (uint32_t e = threadIdx.x; e < total; e += kBlock) {
-                int lo = 0, hi = kBlock;
+                int lo = 0, hi = kStep;
                 while (hi - lo > 1) {
                     int mid = (lo + hi) >> 1;
                     if (s_off[mid] <= e)
