@@ -216,10 +216,15 @@ __device__ __forceinline__ void warp_row(const Tile &T, uint32_t v, uint64_t b, 
 /* Finish pass: tiles grabbed with an atomic counter; rows of vertices in
  * the graph's giant tree are skipped (valid for symmetric graphs: every
  * edge leaving the tree is seen from its other end). */
+/* Vertices a thread takes per step of the finish pass (consecutive), so
+ * the step's barriers are paid once per kVPT vertices per thread. */
+constexpr int kVPT = 4;
+constexpr int kStep = kB * kVPT;
+
 __global__ void __launch_bounds__(kB, 4) kb_link(BatchK K)
 {
-    __shared__ uint32_t s_off[kB + 1];
-    __shared__ uint64_t s_beg[kB];
+    __shared__ uint32_t s_off[kStep + 1];
+    __shared__ uint64_t s_beg[kStep];
     __shared__ uint32_t s_wsum[kWarpsB];
     __shared__ unsigned long long s_t;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -233,30 +238,38 @@ __global__ void __launch_bounds__(kB, 4) kb_link(BatchK K)
             break;
         const Tile T = tile_of(K, (uint32_t)t);
         const uint32_t giant = K.skip ? __ldg(K.giants + T.g) : kNone;
-        for (uint32_t t0 = T.v0; t0 < T.v1; t0 += kB) {
-            const uint32_t v = t0 + threadIdx.x;
-            uint64_t beg = 0, end = 0;
-            if (v < T.v1 && (giant == kNone || cc_ldp(T.parent, v) != giant))
-                row_bounds(T, v, beg, end);
-            uint64_t deg = end - beg;
-            if (deg > K.heavy_deg) {
-                const uint32_t slot = atomicAdd(K.heavy_count, 1u);
-                if (slot < K.heavy_cap) {
-                    K.heavy_list[slot] = ((uint64_t)T.g << 32) | v;
-                    deg = 0;
+        for (uint32_t t0 = T.v0; t0 < T.v1; t0 += kStep) {
+            uint64_t beg[kVPT], end[kVPT];
+            uint32_t small[kVPT], mine = 0;
+#pragma unroll
+            for (int k = 0; k < kVPT; ++k) {
+                const uint32_t v = t0 + threadIdx.x * kVPT + k;
+                beg[k] = end[k] = 0;
+                if (v < T.v1 && (giant == kNone || cc_ldp(T.parent, v) != giant))
+                    row_bounds(T, v, beg[k], end[k]);
+                uint64_t deg = end[k] - beg[k];
+                if (deg > K.heavy_deg) {
+                    const uint32_t slot = atomicAdd(K.heavy_count, 1u);
+                    if (slot < K.heavy_cap) {
+                        K.heavy_list[slot] = ((uint64_t)T.g << 32) | v;
+                        deg = 0;
+                        end[k] = beg[k];
+                    }
                 }
+                unsigned big = __ballot_sync(0xffffffffu, deg >= K.warp_deg);
+                while (big) {
+                    const int src = __ffs(big) - 1;
+                    big &= big - 1;
+                    const uint32_t vv = __shfl_sync(0xffffffffu, v, src);
+                    const uint64_t bb = __shfl_sync(0xffffffffu, beg[k], src);
+                    const uint64_t ee = __shfl_sync(0xffffffffu, end[k], src);
+                    warp_row(T, vv, bb, ee, lane);
+                }
+                small[k] = deg < K.warp_deg ? (uint32_t)deg : 0u;
+                mine += small[k];
+                s_beg[threadIdx.x * kVPT + k] = beg[k];
             }
-            unsigned big = __ballot_sync(0xffffffffu, deg >= K.warp_deg);
-            while (big) {
-                const int src = __ffs(big) - 1;
-                big &= big - 1;
-                const uint32_t vv = __shfl_sync(0xffffffffu, v, src);
-                const uint64_t bb = __shfl_sync(0xffffffffu, beg, src);
-                const uint64_t ee = __shfl_sync(0xffffffffu, end, src);
-                warp_row(T, vv, bb, ee, lane);
-            }
-            const uint32_t small = deg < K.warp_deg ? (uint32_t)deg : 0u;
-            uint32_t incl = small;
+            uint32_t incl = mine;
             for (int o = 1; o < 32; o <<= 1) {
                 const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
                 if (lane >= o)
@@ -264,7 +277,6 @@ __global__ void __launch_bounds__(kB, 4) kb_link(BatchK K)
             }
             if (lane == 31)
                 s_wsum[warp] = incl;
-            s_beg[threadIdx.x] = beg;
             __syncthreads();
             uint32_t wpre = 0, total = 0;
 #pragma unroll
@@ -273,12 +285,17 @@ __global__ void __launch_bounds__(kB, 4) kb_link(BatchK K)
                 wpre += (w < warp) ? x : 0u;
                 total += x;
             }
-            s_off[threadIdx.x] = wpre + incl - small;
+            uint32_t run = wpre + incl - mine;
+#pragma unroll
+            for (int k = 0; k < kVPT; ++k) {
+                s_off[threadIdx.x * kVPT + k] = run;
+                run += small[k];
+            }
             if (threadIdx.x == 0)
-                s_off[kB] = total;
+                s_off[kStep] = total;
             __syncthreads();
             for (uint32_t e = threadIdx.x; e < total; e += kB) {
-                int lo = 0, hi = kB;
+                int lo = 0, hi = kStep;
                 while (hi - lo > 1) {
                     const int mid = (lo + hi) >> 1;
                     if (s_off[mid] <= e)
