@@ -177,10 +177,62 @@ def algorithmic_bytes(torch, rp_d, n, m, k, st):
     }
 
 
+def run_reference_graphs(args, world, spec_w):
+    """--impl reference on the batched and served workloads: the reference
+    solves one graph per call, so it is timed on the workload's graphs one
+    by one (a bounded, seeded sample), reported in graphs per second."""
+    import numpy as np
+    import torch
+    import oracle
+    from cc_mpi_b200 import batch
+    torch.cuda.set_device(0)
+    n_graphs = spec_w.get("graphs", spec_w.get("pool", 512))
+    spec = batch.mix_spec(n_graphs, spec_w["n_min"], spec_w["n_max"], seed=args.seed)
+    order = np.random.default_rng(args.seed).permutation(len(spec))
+    threads = os.cpu_count() or 1
+    graphs_h = []
+    for g in order[:64]:
+        kind, n, seed = spec[g]
+        rp_d, col_d = batch.build_one_torch(torch, kind, n, seed)
+        graphs_h.append((rp_d.cpu().numpy().view(np.uint64), col_d.cpu().numpy().view(np.uint32)))
+    for rp, col in graphs_h[:args.warmup]:
+        oracle.ref_pthreads_labels(rp, col, threads, 8192)
+    t_all, done, edges = 0.0, 0, 0
+    for _ in range(args.steps):
+        for rp, col in graphs_h:
+            t0 = time.perf_counter()
+            oracle.ref_pthreads_labels(rp, col, threads, 8192)
+            t_all += time.perf_counter() - t0
+            done += 1
+            edges += len(col) // 2
+        if t_all > 60.0:
+            break
+    gps = done / t_all
+    line = {
+        "impl": "reference", "metric": "batched CC graphs/s" if spec_w.get("batch")
+        else "served CC graphs/s", "value": gps, "unit": "graphs/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_all / max(done, 1) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic",
+        "config": {"workload": args.workload, "graphs_timed": done, "gteps": edges / t_all / 1e9},
+        "cpu_baseline": {"value": gps, "unit": "graphs/s", "cores": threads,
+                         "kind": "reference" if oracle.have_ref() else "port",
+                         "sample": f"{len(graphs_h)} graphs of the workload's mix in seeded "
+                                   f"random order, solved one by one, {args.steps} rounds"},
+        "e2e": {"value": gps, "unit": "graphs/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_reference(args, rank, world):
     """--impl reference: the reference's own CPU code on this host."""
     if rank != 0:
         return 0
+    spec_w = WORKLOADS[args.workload]
+    if spec_w.get("batch") or spec_w.get("served"):
+        return run_reference_graphs(args, world, spec_w)
     import numpy as np
     import torch
     import oracle
@@ -252,7 +304,8 @@ def dist_bytes(n, m, st):
         "final_compress": 8 * n, "link_rows": 4 * n + 8 * n, "giant": 4096,
         "dist_local_count": 4 * m, "dist_tiles": 8 * (n + 1),
         "dist_local_fill": 4 * m + 4 * lm + 16 * (n + 1),
-        "dist_gflag": 4 * n + n // 8, "dist_pairs_bitmap": 4 * n + 8 * G,
+        "dist_gflag": 4 * n + n // 8, "dist_pairs_bitmap": 4 * n + 4 * G,
+        "dist_merge_keys": 16 * (R + G),
         "dist_reps": 4 * n + 12 * reps, "dist_pairs": 8 * (n + 1) + 4 * m + n // 8 + 8 * R,
         "sort_hist": 8 * R, "sort_scatter": 16 * R, "dist_dedup": 8 * R,
         "dist_ghosts": 8 * R + 8 * U + 24 * G, "merge_hook": 12 * U,

@@ -95,6 +95,7 @@ enum {
     CCK_DIST_LOCAL_FILL,
     CCK_DIST_TILES,
     CCK_DIST_GFLAG,
+    CCK_DIST_MERGE_KEYS,
     CCK_NUM
 };
 

@@ -377,38 +377,143 @@ __global__ void __launch_bounds__(kB, 4) k_emit(EmitParams E)
     add_raw(E, raw, lane);
 }
 
-/* One key (p, u, giant rep of p) per bit p of pmask[u], appended after the
- * keys k_emit wrote (the sort orders them). */
-__global__ void __launch_bounds__(kB) k_mask_keys(EmitParams E)
+/* The mask keys in sorted order: key (p, u, giant rep of p) for every bit
+ * p of pmask[u], partition-major and ascending in u - already the sort
+ * order, so they skip the radix sort and are merged with the sorted plain
+ * keys.  Pass 1 counts the bits of each partition per block of kMaskBlock
+ * vertices (counts stored partition-major); after a scan, pass 2 writes
+ * each block's keys at its offsets in vertex order. */
+constexpr int kMaskBlock = kB * 8;
+
+__global__ void __launch_bounds__(kB) k_mask_count(EmitParams E, uint32_t nblk, uint32_t *cnt)
+{
+    __shared__ uint32_t s_c[32];
+    for (uint32_t blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
+        if (threadIdx.x < 32)
+            s_c[threadIdx.x] = 0;
+        __syncthreads();
+        const uint64_t v0 = (uint64_t)blk * kMaskBlock;
+        uint32_t mine[32];
+#pragma unroll
+        for (int p = 0; p < 32; ++p)
+            mine[p] = 0;
+        for (int k = 0; k < 8; ++k) {
+            const uint64_t u = v0 + (uint64_t)k * kB + threadIdx.x;
+            const uint32_t bits = u < E.n ? E.pmask[u] : 0u;
+#pragma unroll
+            for (int p = 0; p < 32; ++p)
+                mine[p] += (bits >> p) & 1u;
+        }
+        for (int p = 0; p < E.parts; ++p) {
+            const uint32_t c = __reduce_add_sync(0xffffffffu, mine[p]);
+            if ((threadIdx.x & 31) == 0 && c)
+                atomicAdd(&s_c[p], c);
+        }
+        __syncthreads();
+        if (threadIdx.x < (unsigned)E.parts)
+            cnt[(uint64_t)threadIdx.x * nblk + blk] = s_c[threadIdx.x];
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(kB) k_mask_write(EmitParams E, uint32_t nblk,
+                                                   const uint64_t *off, uint64_t *out)
 {
     __shared__ uint32_t s_b[CCGPU_MAX_PARTS + 1];
     __shared__ uint32_t s_gl[CCGPU_MAX_PARTS];
+    __shared__ uint32_t s_w[kW];
     for (int i = threadIdx.x; i <= E.parts; i += kB)
         s_b[i] = E.bounds[i];
     load_giant_labels(E, s_gl);
     __syncthreads();
-    const int lane = threadIdx.x & 31;
-    const uint64_t stride = (uint64_t)gridDim.x * kB;
-    for (uint64_t b0 = (uint64_t)blockIdx.x * kB; b0 < E.n; b0 += stride) {
-        const uint64_t u = b0 + threadIdx.x;
-        uint32_t bits = u < E.n ? E.pmask[u] : 0u;
-        const uint32_t c = __popc(bits);
-        uint32_t incl = c;
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o)
-                incl += y;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint32_t blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
+        const uint64_t v0 = (uint64_t)blk * kMaskBlock;
+        for (int p = 0; p < E.parts; ++p) {
+            uint64_t at = off[(uint64_t)p * nblk + blk];
+            const uint64_t rep = s_gl[p] - s_b[p];
+            for (int k = 0; k < 8; ++k) {
+                const uint64_t u = v0 + (uint64_t)k * kB + threadIdx.x;
+                const bool has = u < E.n && ((E.pmask[u] >> p) & 1u);
+                const unsigned bal = __ballot_sync(0xffffffffu, has);
+                if (lane == 0)
+                    s_w[warp] = __popc(bal);
+                __syncthreads();
+                uint32_t pre = 0, tot = 0;
+#pragma unroll
+                for (int w = 0; w < kW; ++w) {
+                    pre += w < warp ? s_w[w] : 0u;
+                    tot += s_w[w];
+                }
+                if (has)
+                    out[at + pre + __popc(bal & ((1u << lane) - 1u))] =
+                        make_key(E, p, (uint32_t)u, (uint32_t)rep);
+                at += tot;
+                __syncthreads();
+            }
         }
-        const uint32_t wtot = __shfl_sync(0xffffffffu, incl, 31);
-        unsigned long long at = 0;
-        if (lane == 31 && wtot)
-            at = atomicAdd(E.count, (unsigned long long)wtot);
-        at = __shfl_sync(0xffffffffu, at, 31) + (incl - c);
-        while (bits) {
-            const int p = __ffs(bits) - 1;
-            bits &= bits - 1;
-            E.out[at++] = make_key(E, p, (uint32_t)u, s_gl[p] - s_b[p]);
+    }
+}
+
+/* Stable merge of two ascending key arrays (ties take a first): each block
+ * finds where its kMergeTile outputs start on the merge path by binary
+ * search, stages those inputs in shared memory, and each thread merges
+ * kMergeItems outputs from its own split point. */
+constexpr int kMergeItems = 8;
+constexpr int kMergeTile = kB * kMergeItems;
+
+__device__ __forceinline__ uint64_t merge_split(const uint64_t *a, uint64_t na, const uint64_t *b,
+                                                uint64_t nb, uint64_t d)
+{
+    uint64_t lo = d > nb ? d - nb : 0, hi = d < na ? d : na;
+    while (lo < hi) {
+        const uint64_t mid = (lo + hi) >> 1;
+        if (a[mid] <= b[d - mid - 1])
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(kB) k_merge(const uint64_t *__restrict__ a, uint64_t na,
+                                              const uint64_t *__restrict__ b, uint64_t nb,
+                                              uint64_t *__restrict__ out)
+{
+    __shared__ uint64_t s_k[kMergeTile];
+    __shared__ uint64_t s_ia[2];
+    const uint64_t total = na + nb;
+    for (uint64_t d0 = (uint64_t)blockIdx.x * kMergeTile; d0 < total;
+         d0 += (uint64_t)gridDim.x * kMergeTile) {
+        const uint64_t d1 = d0 + kMergeTile < total ? d0 + kMergeTile : total;
+        if (threadIdx.x < 2)
+            s_ia[threadIdx.x] = merge_split(a, na, b, nb, threadIdx.x ? d1 : d0);
+        __syncthreads();
+        const uint64_t ia0 = s_ia[0], ia1 = s_ia[1];
+        const uint64_t ib0 = d0 - ia0, ib1 = d1 - ia1;
+        const uint32_t la = (uint32_t)(ia1 - ia0), lb = (uint32_t)(ib1 - ib0);
+        for (uint32_t i = threadIdx.x; i < la + lb; i += kB)
+            s_k[i] = i < la ? a[ia0 + i] : b[ib0 + (i - la)];
+        __syncthreads();
+        const uint32_t dt = threadIdx.x * kMergeItems;
+        if (dt < la + lb) {
+            /* split of this thread's diagonal inside the tile */
+            uint32_t lo = dt > lb ? dt - lb : 0, hi = dt < la ? dt : la;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (s_k[mid] <= s_k[la + (dt - mid - 1)])
+                    lo = mid + 1;
+                else
+                    hi = mid;
+            }
+            uint32_t ia = lo, ib = dt - lo;
+            const uint32_t end = dt + kMergeItems < la + lb ? dt + kMergeItems : la + lb;
+            for (uint32_t o = dt; o < end; ++o) {
+                const bool take_a = ib >= lb || (ia < la && s_k[ia] <= s_k[la + ib]);
+                out[d0 + o] = take_a ? s_k[ia++] : s_k[la + ib++];
+            }
         }
+        __syncthreads();
     }
 }
 
@@ -1364,9 +1469,6 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
             CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit<8>, eb, kB, 0, st, E);
         else
             CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit<CCGPU_MAX_PARTS>, eb, kB, 0, st, E);
-        if (use_mask)
-            CC_KLAUNCH(ctx, CCK_DIST_PAIRS_BITMAP, k_mask_keys,
-                       cc_blocks(n, kB, (unsigned)ctx->sm_count * 8), kB, 0, st, E);
     }
     unsigned long long hc[5];
     CC_CUDA(cudaMemcpyAsync(hc, counters, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
@@ -1379,12 +1481,44 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
     S.rep_count = hc[1];
     CC_TRY(clock_mark(clk, st)); /* 3 */
 
-    /* 4. sort */
+    /* 4. sort the plain keys; the mask keys come out sorted and are merged
+     * in */
     uint64_t *sorted = keys;
     if (R > 1) {
         CC_TRY(cc_bufs_get(&B, (void **)&alt, (size_t)R * sizeof(uint64_t)));
         CC_TRY(cc_radix_sort_u64(ctx, keys, alt, R, rb + gb + pb, &sorted, &S.sort_passes, &B,
                                  st));
+    }
+    uint64_t R_all = R;
+    if (use_mask) {
+        const uint32_t nblk = (uint32_t)(((uint64_t)n + kMaskBlock - 1) / kMaskBlock);
+        uint32_t *mcnt = nullptr;
+        uint64_t *moff = nullptr, *mkeys = nullptr, *merged = nullptr;
+        CC_TRY(cc_bufs_get(&B, (void **)&mcnt, (size_t)P * nblk * sizeof(uint32_t)));
+        CC_TRY(cc_bufs_get(&B, (void **)&moff, ((size_t)P * nblk + 1) * sizeof(uint64_t)));
+        const unsigned mb = cc_blocks(nblk, 1, (unsigned)ctx->sm_count * 8);
+        CC_KLAUNCH(ctx, CCK_DIST_PAIRS_BITMAP, k_mask_count, mb, kB, 0, st, E, nblk, mcnt);
+        CC_TRY(cc_scan_u32(ctx, mcnt, moff, (uint64_t)P * nblk, &B, st));
+        uint64_t M_keys = 0;
+        CC_CUDA(cudaMemcpyAsync(&M_keys, moff + (uint64_t)P * nblk, sizeof(uint64_t),
+                                cudaMemcpyDeviceToHost, st));
+        CC_CUDA(cudaStreamSynchronize(st));
+        if (M_keys) {
+            CC_TRY(cc_bufs_get(&B, (void **)&mkeys, (size_t)M_keys * sizeof(uint64_t)));
+            CC_KLAUNCH(ctx, CCK_DIST_PAIRS_BITMAP, k_mask_write, mb, kB, 0, st, E, nblk,
+                       (const uint64_t *)moff, mkeys);
+            if (R > 0) {
+                CC_TRY(cc_bufs_get(&B, (void **)&merged, (size_t)(R + M_keys) * sizeof(uint64_t)));
+                const uint64_t tiles = (R + M_keys + kMergeTile - 1) / kMergeTile;
+                CC_KLAUNCH(ctx, CCK_DIST_MERGE_KEYS, k_merge,
+                           cc_blocks(tiles, 1, (unsigned)ctx->sm_count * 8), kB, 0, st, sorted, R,
+                           mkeys, M_keys, merged);
+                sorted = merged;
+            } else {
+                sorted = mkeys;
+            }
+            R_all = R + M_keys;
+        }
     }
     CC_TRY(clock_mark(clk, st)); /* 4 */
 
@@ -1392,20 +1526,20 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
     DedupParams D;
     memset(&D, 0, sizeof(D));
     D.keys = sorted;
-    D.count = R;
+    D.count = R_all;
     D.rb = rb;
     D.gb = gb;
     D.bounds = bounds;
     D.parts = P;
     uint64_t U = 0, G = 0;
     std::vector<uint64_t> gfirst(P, ~0ull);
-    const uint64_t T = (R + kDedupTile - 1) / kDedupTile;
+    const uint64_t T = (R_all + kDedupTile - 1) / kDedupTile;
     uint64_t *gh_off = nullptr, *segs = nullptr;
     CC_TRY(cc_bufs_get(&B, (void **)&gh_off, (P + 1) * sizeof(uint64_t)));
     CC_TRY(cc_bufs_get(&B, (void **)&segs, (size_t)P * (P + 1) * sizeof(uint64_t)));
     CC_TRY(cc_bufs_get(&B, (void **)&D.gh_first, P * sizeof(uint64_t)));
     CC_CUDA(cudaMemsetAsync(D.gh_first, 0xff, P * sizeof(uint64_t), st));
-    if (R > 0) {
+    if (R_all > 0) {
         uint64_t *u_off = nullptr, *g_off = nullptr;
         CC_TRY(cc_bufs_get(&B, (void **)&D.tile_u, T * sizeof(uint32_t)));
         CC_TRY(cc_bufs_get(&B, (void **)&D.tile_g, T * sizeof(uint32_t)));
@@ -1431,7 +1565,7 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
     CC_TRY(cc_bufs_get(&B, (void **)&D.ghost_pairs, (size_t)(G + 1) * sizeof(uint64_t)));
     CC_TRY(cc_bufs_get(&B, (void **)&D.ghost_labels, (size_t)(G ? G : 1) * sizeof(uint32_t)));
     CC_TRY(cc_bufs_get(&B, (void **)&D.prev_sent, (size_t)(G ? G : 1) * sizeof(uint32_t)));
-    if (R > 0) {
+    if (R_all > 0) {
         CC_KLAUNCH(ctx, CCK_DIST_GHOSTS, k_dedup_write, (unsigned)T, kB, 0, st, D);
         CC_CUDA(cudaMemcpyAsync(D.ghost_pairs + G, &U, sizeof(uint64_t), cudaMemcpyHostToDevice,
                                 st));
@@ -1456,7 +1590,8 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
         for (int p = 0; p < P; ++p)
             printf("[part %d] ghost_count=%llu\n", p, (unsigned long long)(hoff[p + 1] - hoff[p]));
         printf("[all] boundary_edges raw=%llu dedup=%llu reps=%llu sort_passes=%d\n",
-               (unsigned long long)R, (unsigned long long)U, (unsigned long long)S.rep_count,
+               (unsigned long long)S.boundary_raw, (unsigned long long)U,
+               (unsigned long long)S.rep_count,
                S.sort_passes);
     }
 

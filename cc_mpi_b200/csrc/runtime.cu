@@ -191,7 +191,7 @@ static const char *const kKernelNames[CCK_NUM] = {
     "dist_labels", "dist_bounds", "scan", "batch", "misc", "dist_pairs_heavy",
     "dist_pairs_bitmap", "batch_init", "batch_sample", "batch_compress", "batch_giant",
     "batch_link", "batch_heavy", "batch_final", "dist_local_count", "dist_local_fill",
-    "dist_tiles", "dist_gflag"};
+    "dist_tiles", "dist_gflag", "dist_merge_keys"};
 
 struct cc_prof {
     std::vector<cudaEvent_t> pool;
