@@ -665,6 +665,7 @@ __global__ void __launch_bounds__(kB) k_local_fill(LocalParams L)
     __shared__ uint32_t s_excl[kB + 1];
     __shared__ uint32_t s_mask[kB];
     __shared__ uint32_t s_w[kW];
+    __shared__ uint32_t s_out[kTile]; /* the tile's kept entries, compacted */
     for (int i = threadIdx.x; i <= L.parts; i += kB) {
         s_b[i] = L.bounds[i];
         s_pcol[i] = L.pcol[i];
@@ -701,8 +702,11 @@ __global__ void __launch_bounds__(kB) k_local_fill(LocalParams L)
 #pragma unroll
         for (int q = 0; q < kTileE; ++q)
             if (mask & (1u << q))
-                L.lcol[base + k++] = u[q];
+                s_out[k++] = u[q];
         __syncthreads();
+        /* coalesced write-out of the compacted tile */
+        for (uint32_t i = threadIdx.x; i < total; i += kB)
+            L.lcol[base + i] = s_out[i];
         /* local row pointers of the rows starting in (tile start, tile end] */
         const uint64_t lo = t * kTile;
         const uint32_t v0 = L.tile_first[t], v1 = L.tile_first[t + 1];
