@@ -1401,7 +1401,7 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
         tile_first = Lp.tile_first;
         col_tiles = Lp.tiles;
     }
-    LocalCCArgs a = {l_rp, l_col, n, l_m, label, seg64, (uint32_t)P, {}, 0};
+    LocalCCArgs a = {l_rp, l_col, n, l_m, label, seg64, (uint32_t)P, {}, 0, 1};
     ccgpu_cc_opts lo;
     ccgpu_cc_opts_default(&lo);
     lo.chunk_size = o.chunk_size;

@@ -185,6 +185,34 @@ __global__ void __launch_bounds__(kBlock) k_sample_min(const uint64_t *__restric
     }
 }
 
+/* k_sample_min for rounds 0 and 1 with a stash of each vertex's second
+ * neighbour: round 0 reads entries 0 and 1 of the row (one column sector)
+ * and keeps entry 1 in stash[v]; round 1 links v with stash[v] without
+ * touching the row.  UINT32_MAX in the stash means no second entry. */
+__global__ void __launch_bounds__(kBlock) k_sample_stash(const uint64_t *__restrict__ row_ptr,
+                                                         const uint32_t *__restrict__ col,
+                                                         uint32_t n, uint64_t m,
+                                                         uint32_t *parent, uint32_t *stash,
+                                                         int round)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * kBlock;
+    for (uint64_t v = (uint64_t)blockIdx.x * kBlock + threadIdx.x; v < n; v += stride) {
+        uint32_t u;
+        if (round == 0) {
+            Rows r = row_of(row_ptr, (uint32_t)v, m);
+            u = r.beg < r.end ? __ldg(col + r.beg) : 0xffffffffu;
+            stash[v] = r.beg + 1 < r.end ? __ldg(col + r.beg + 1) : 0xffffffffu;
+        } else {
+            u = stash[v];
+        }
+        if (u >= n)
+            continue;
+        uint32_t rv = cc_find(parent, (uint32_t)v), ru = cc_find(parent, u);
+        if (rv != ru)
+            atomicMin(parent + (rv > ru ? rv : ru), rv < ru ? rv : ru);
+    }
+}
+
 __global__ void __launch_bounds__(kBlock) k_compress(uint32_t *parent, uint32_t n)
 {
     const uint64_t stride = (uint64_t)gridDim.x * kBlock;
@@ -603,6 +631,7 @@ void cc_local_carve(cc_carve *c, LocalCCScratch *s, const LocalCCArgs &a)
     s->giants = (uint32_t *)cc_take(c, (size_t)(a.nseg ? a.nseg : 1) * sizeof(uint32_t));
     s->heavy_list = (uint32_t *)cc_take(c, cap * sizeof(uint32_t));
     s->heavy_cap = (uint32_t)cap;
+    s->stash = a.stash ? (uint32_t *)cc_take(c, (size_t)a.n * sizeof(uint32_t)) : nullptr;
 }
 
 int cc_local_init(ccgpu_ctx *ctx, const LocalCCArgs &a, const LocalCCScratch &s, cudaStream_t st)
@@ -647,11 +676,20 @@ int cc_local_run(ccgpu_ctx *ctx, const LocalCCArgs &a, const LocalCCScratch &s, 
             /* with MINHOOK the finish pass relinks entry 0, so the init
              * pass's first hook is all round 0 needs */
             const int r_start = (minhook && (a.o.hook_mode & CCGPU_HOOK_FIRST)) ? 1 : 0;
+            /* rounds 0 and 1 through the stash when the scratch has one and
+             * rows are long enough (>= 8 entries per vertex on average) for
+             * the saved column gathers to outweigh the stash traffic */
+            const bool use_stash = s.stash && minhook && !a.seg_filter && r_start == 0 &&
+                                   k >= 2 && a.m >= 8ull * a.n;
             if (a.o.hook_mode & CCGPU_HOOK_CADENCE) {
                 if (r_start > 0 && r_start < k)
                     CC_KLAUNCH(ctx, CCK_COMPRESS, k_compress, sb, kBlock, 0, st, a.labels, a.n);
                 for (int r = r_start; r < k; ++r) {
-                    CC_TRY(launch_sample_any(ctx, a, 0, a.n, r, r + 1, st, sb));
+                    if (use_stash && r < 2)
+                        CC_KLAUNCH(ctx, CCK_SAMPLE, k_sample_stash, sb, kBlock, 0, st, a.row_ptr,
+                                   a.col, a.n, a.m, a.labels, s.stash, r);
+                    else
+                        CC_TRY(launch_sample_any(ctx, a, 0, a.n, r, r + 1, st, sb));
                     if (r + 1 < k)
                         CC_KLAUNCH(ctx, CCK_COMPRESS, k_compress, sb, kBlock, 0, st, a.labels,
                                    a.n);
@@ -744,7 +782,7 @@ extern "C" int ccgpu_local_cc(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const u
         memset(stats, 0, sizeof(*stats));
     if (n == 0)
         return CCGPU_OK;
-    LocalCCArgs a = {d_row_ptr, d_col_idx, n, m, d_labels, nullptr, 1, {}};
+    LocalCCArgs a = {d_row_ptr, d_col_idx, n, m, d_labels, nullptr, 1, {}, 0, 1};
     CC_TRY(cc_local_resolve_opts(opts, &a.o));
     CC_TRY(ccgpu_ctx_resolve(&ctx));
     cudaStream_t st = (cudaStream_t)stream;

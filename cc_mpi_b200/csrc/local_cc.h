@@ -26,6 +26,10 @@ struct LocalCCArgs {
                                * different segments (the local subgraph
                                * of each partition, reference
                                * src/cc_mpi.c:252-297)                  */
+    int stash;                /* 1: scratch holds each vertex's second
+                               * neighbour, written by sampling round 0
+                               * (same sector as the first) and read by
+                               * round 1 instead of its row            */
 };
 
 /* Device counters a solve leaves behind (for stats). */
@@ -42,6 +46,7 @@ struct LocalCCScratch {
     uint32_t *heavy_list;
     uint32_t heavy_cap;
     uint32_t *giants; /* [nseg] */
+    uint32_t *stash;  /* [n] second neighbours, NULL unless args.stash */
 };
 
 /* Resolves defaults (NULL in -> defaults); CCGPU_ERR_INVALID on bad values. */

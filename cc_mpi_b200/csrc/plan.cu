@@ -37,7 +37,7 @@ extern "C" int ccgpu_local_cc_plan(const uint64_t *d_row_ptr, const uint32_t *d_
     *out = nullptr;
     if (n == 0 || !d_row_ptr || !d_labels || (m > 0 && !d_col_idx))
         return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_local_cc_plan: empty graph or NULL");
-    LocalCCArgs a = {d_row_ptr, d_col_idx, n, m, d_labels, nullptr, 1, {}, 0};
+    LocalCCArgs a = {d_row_ptr, d_col_idx, n, m, d_labels, nullptr, 1, {}, 0, 1};
     CC_TRY(cc_local_resolve_opts(opts, &a.o));
     ccgpu_plan *p = (ccgpu_plan *)calloc(1, sizeof(ccgpu_plan));
     if (!p)
