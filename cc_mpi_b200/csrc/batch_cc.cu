@@ -72,6 +72,7 @@ struct BatchK {
     uint32_t heavy_deg;
     uint32_t warp_deg;
     int skip;                 /* finish pass skips giant trees   */
+    uint32_t *stash;          /* second neighbours (like labels), NULL = off */
 };
 
 struct Tile {
@@ -121,12 +122,18 @@ __global__ void __launch_bounds__(kB) kb_sample(BatchK K, int r)
 {
     for (uint32_t t = blockIdx.x; t < K.tiles; t += gridDim.x) {
         const Tile T = tile_of(K, t);
+        uint32_t *stash = K.stash ? K.stash + (T.parent - K.labels) : nullptr;
         for (uint32_t v = T.v0 + threadIdx.x; v < T.v1; v += kB) {
-            uint64_t b, e;
-            row_bounds(T, v, b, e);
-            if (b + (uint64_t)r >= e)
-                continue;
-            const uint32_t u = __ldg(T.col + b + r);
+            uint32_t u;
+            if (stash && r == 1) {
+                u = stash[v]; /* written by round 0 */
+            } else {
+                uint64_t b, e;
+                row_bounds(T, v, b, e);
+                u = b + (uint64_t)r < e ? __ldg(T.col + b + r) : 0xffffffffu;
+                if (stash && r == 0)
+                    stash[v] = b + 1 < e ? __ldg(T.col + b + 1) : 0xffffffffu;
+            }
             if (u >= T.n)
                 continue;
             const uint32_t rv = cc_find(T.parent, v), ru = cc_find(T.parent, u);
@@ -439,6 +446,8 @@ BatchK kargs(BatchCore *c, int k)
     K.heavy_deg = (uint32_t)c->tune.heavy_degree;
     K.warp_deg = (uint32_t)C.o.warp_degree;
     K.skip = C.o.sample_rounds > 0;
+    K.stash = (c->stash && C.o.sample_rounds >= 2 && C.entries >= 8ull * C.vertices) ? c->stash
+                                                                                    : nullptr;
     return K;
 }
 
@@ -543,7 +552,13 @@ void batch_core_free(BatchCore *c)
     cudaFree(c->d_done);
     if (c->h_stage)
         cudaFreeHost(c->h_stage);
+    cudaFree(c->stash);
     *c = BatchCore();
+}
+
+int batch_core_stash(BatchCore *c, size_t entries)
+{
+    return grow(&c->stash, &c->stash_cap, entries ? entries : 1);
 }
 
 int batch_core_reserve(BatchCore *c, size_t graphs, size_t tiles, size_t heavy)
@@ -872,6 +887,8 @@ extern "C" int ccgpu_batch_plan_create(ccgpu_ctx *ctx, const ccgpu_batch *b,
     p->G = G;
     p->vtx_off.assign(vo, vo + G + 1);
     int rc = batch_core_init(&p->core, ctx, &t);
+    if (rc == CCGPU_OK)
+        rc = batch_core_stash(&p->core, (size_t)vo[G]);
     if (rc == CCGPU_OK)
         rc = batch_core_set(&p->core, b->d_row_ptr, b->d_col, b->d_labels, gr.data(), G,
                             nullptr, 1);

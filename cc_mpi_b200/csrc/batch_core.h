@@ -56,6 +56,8 @@ struct BatchCore {
     cudaEvent_t fork = nullptr;
     void *h_stage = nullptr; /* pinned staging of the uploads */
     size_t stage_cap = 0;
+    uint32_t *stash = nullptr; /* second-neighbour stash, indexed like labels */
+    size_t stash_cap = 0;      /* entries (0: no stash)                      */
 };
 
 /* Validates and stores the tuning, creates the class streams and events. */
@@ -73,6 +75,11 @@ int batch_core_set(BatchCore *c, const uint64_t *row_ptr, const uint32_t *col, u
 /* Rebuilds and uploads class k's tile list after its options changed
  * (synchronous). */
 int batch_core_retile(BatchCore *c, int k);
+/* Gives the batch a second-neighbour stash of `entries` u32 (the extent of
+ * the label array): sampling round 0 keeps each vertex's second neighbour
+ * there and round 1 reads it instead of the row, in classes whose rows
+ * average at least 8 entries. */
+int batch_core_stash(BatchCore *c, size_t entries);
 /* Enqueues the whole solve on st: per-graph outputs cleared, every class
  * on its own stream forked from st and joined back. */
 int batch_core_enqueue(BatchCore *c, cudaStream_t st, int *kernels);
