@@ -848,12 +848,11 @@ extern "C" void ccgpu_batch_tuning_default(ccgpu_batch_tuning *t)
     }
 }
 
-extern "C" int ccgpu_batch_plan_create(ccgpu_ctx *ctx, const ccgpu_batch *b,
-                                       const ccgpu_batch_tuning *tuning, ccgpu_batch_plan **out)
+namespace {
+
+/* Checks a batch and builds its per-graph descriptors. */
+int batch_descs(const ccgpu_batch *b, std::vector<BGraph> &gr)
 {
-    if (!b || !out || !b->h_vtx_off || !b->h_edge_off)
-        return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_batch_plan_create: NULL argument");
-    *out = nullptr;
     if (b->graphs == 0)
         return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_batch_plan_create: empty batch");
     if (!b->d_row_ptr || !b->d_labels || (b->h_edge_off[b->graphs] && !b->d_col))
@@ -862,7 +861,7 @@ extern "C" int ccgpu_batch_plan_create(ccgpu_ctx *ctx, const ccgpu_batch *b,
     const uint64_t *vo = b->h_vtx_off, *eo = b->h_edge_off;
     if (vo[0] != 0 || eo[0] != 0)
         return ccgpu_set_error(CCGPU_ERR_INVALID, "batch: offsets must start at 0");
-    std::vector<BGraph> gr(G);
+    gr.resize(G);
     for (uint32_t g = 0; g < G; ++g) {
         if (vo[g + 1] < vo[g] || eo[g + 1] < eo[g])
             return ccgpu_set_error(CCGPU_ERR_INVALID, "batch: offsets of graph %u decrease", g);
@@ -876,6 +875,35 @@ extern "C" int ccgpu_batch_plan_create(ccgpu_ctx *ctx, const ccgpu_batch *b,
         gr[g].m = eo[g + 1] - eo[g];
         gr[g].pad = 0;
     }
+    return CCGPU_OK;
+}
+
+/* Points an initialised plan at a batch: tuning, descriptors, tiles and a
+ * stash covering its labels.  Device arrays only grow. */
+int plan_set(ccgpu_batch_plan *p, const ccgpu_batch *b, const ccgpu_batch_tuning &t,
+             const std::vector<BGraph> &gr)
+{
+    drop_graph(p);
+    p->G = b->graphs;
+    p->vtx_off.assign(b->h_vtx_off, b->h_vtx_off + b->graphs + 1);
+    p->core.tune = t;
+    for (int k = 0; k < CCGPU_BATCH_CLASSES; ++k)
+        p->core.cls[k].o = t.cls[k];
+    CC_TRY(batch_core_stash(&p->core, (size_t)p->vtx_off[p->G]));
+    return batch_core_set(&p->core, b->d_row_ptr, b->d_col, b->d_labels, gr.data(), p->G,
+                          nullptr, 1);
+}
+
+} // namespace
+
+extern "C" int ccgpu_batch_plan_create(ccgpu_ctx *ctx, const ccgpu_batch *b,
+                                       const ccgpu_batch_tuning *tuning, ccgpu_batch_plan **out)
+{
+    if (!b || !out || !b->h_vtx_off || !b->h_edge_off)
+        return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_batch_plan_create: NULL argument");
+    *out = nullptr;
+    std::vector<BGraph> gr;
+    CC_TRY(batch_descs(b, gr));
     ccgpu_batch_tuning t;
     if (tuning)
         t = *tuning;
@@ -884,14 +912,9 @@ extern "C" int ccgpu_batch_plan_create(ccgpu_ctx *ctx, const ccgpu_batch *b,
     CC_TRY(batch_check_tuning(&t));
     CC_TRY(ccgpu_ctx_resolve(&ctx));
     ccgpu_batch_plan *p = new ccgpu_batch_plan();
-    p->G = G;
-    p->vtx_off.assign(vo, vo + G + 1);
     int rc = batch_core_init(&p->core, ctx, &t);
     if (rc == CCGPU_OK)
-        rc = batch_core_stash(&p->core, (size_t)vo[G]);
-    if (rc == CCGPU_OK)
-        rc = batch_core_set(&p->core, b->d_row_ptr, b->d_col, b->d_labels, gr.data(), G,
-                            nullptr, 1);
+        rc = plan_set(p, b, t, gr);
     if (rc != CCGPU_OK) {
         ccgpu_batch_plan_destroy(p);
         return rc;
@@ -1029,17 +1052,49 @@ extern "C" void ccgpu_batch_plan_destroy(ccgpu_batch_plan *p)
     delete p;
 }
 
+/* One-shot solve.  The context keeps the plan of its last call and points
+ * it at the next batch, so repeated calls allocate only when a batch
+ * outgrows what earlier ones needed (a context serves one host thread at a
+ * time). */
 extern "C" int ccgpu_batch_cc(ccgpu_ctx *ctx, const ccgpu_batch *b,
                               const ccgpu_batch_tuning *tuning, uint32_t *h_components,
                               void *stream)
 {
-    ccgpu_batch_plan *p = nullptr;
-    CC_TRY(ccgpu_batch_plan_create(ctx, b, tuning, &p));
+    if (!b || !b->h_vtx_off || !b->h_edge_off)
+        return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_batch_cc: NULL argument");
+    CC_TRY(ccgpu_ctx_resolve(&ctx));
+    ccgpu_batch_plan *p = ctx->batch_cache;
+    if (p) {
+        std::vector<BGraph> gr;
+        CC_TRY(batch_descs(b, gr));
+        ccgpu_batch_tuning t;
+        if (tuning)
+            t = *tuning;
+        else
+            ccgpu_batch_tuning_default(&t);
+        CC_TRY(batch_check_tuning(&t));
+        int rc = plan_set(p, b, t, gr);
+        if (rc != CCGPU_OK) {
+            ctx->batch_cache = nullptr;
+            ccgpu_batch_plan_destroy(p);
+            return rc;
+        }
+    } else {
+        CC_TRY(ccgpu_batch_plan_create(ctx, b, tuning, &p));
+        ctx->batch_cache = p;
+    }
     int rc = ccgpu_batch_plan_run(p, stream);
     if (rc == CCGPU_OK)
         rc = ccgpu_batch_plan_results(p, h_components, nullptr, stream);
     else
         cudaStreamSynchronize((cudaStream_t)stream);
-    ccgpu_batch_plan_destroy(p);
     return rc;
+}
+
+void cc_batch_cache_free(ccgpu_ctx *ctx)
+{
+    if (ctx && ctx->batch_cache) {
+        ccgpu_batch_plan_destroy(ctx->batch_cache);
+        ctx->batch_cache = nullptr;
+    }
 }

@@ -92,6 +92,7 @@ extern "C" void ccgpu_ctx_destroy(ccgpu_ctx *ctx)
     int prev = -1;
     cudaGetDevice(&prev);
     cudaSetDevice(ctx->device);
+    cc_batch_cache_free(ctx);
     if (ctx->base)
         cudaFree(ctx->base);
     if (ctx->host_pinned)
@@ -191,7 +192,8 @@ static const char *const kKernelNames[CCK_NUM] = {
     "dist_labels", "dist_bounds", "scan", "batch", "misc", "dist_pairs_heavy",
     "dist_pairs_bitmap", "batch_init", "batch_sample", "batch_compress", "batch_giant",
     "batch_link", "batch_heavy", "batch_final", "dist_local_count", "dist_local_fill",
-    "dist_tiles", "dist_gflag", "dist_merge_keys"};
+    "dist_tiles", "dist_gflag", "dist_merge_keys", "merge_exch_pull",
+    "dist_pairs_local"};
 
 struct cc_prof {
     std::vector<cudaEvent_t> pool;

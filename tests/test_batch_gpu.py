@@ -107,19 +107,24 @@ def test_schedules_match_oracle(torch, sched):
 
 
 def test_one_shot_call(torch):
+    """ccgpu_batch_cc reuses its context's plan from call to call: batches
+    that grow, shrink and change tuning all get the oracle's labels."""
     import ctypes as C
-    gs = small_batch(seed=5, count=20)
-    vo, eo, d_rp, d_col, d_lab = to_device(torch, gs)
     L = batch._bind()
-    b = batch.Batch()
-    b.graphs = len(gs)
-    b.h_vtx_off = vo.ctypes.data_as(C.POINTER(C.c_uint64))
-    b.h_edge_off = eo.ctypes.data_as(C.POINTER(C.c_uint64))
-    b.d_row_ptr, b.d_col, b.d_labels = d_rp.data_ptr(), d_col.data_ptr(), d_lab.data_ptr()
-    comps = np.zeros(len(gs), np.uint32)
-    _lib.check(L.ccgpu_batch_cc(None, C.byref(b), None, comps.ctypes.data,
-                                torch.cuda.current_stream().cuda_stream))
-    check_oracle(torch, gs, vo, d_lab, comps)
+    cases = [(5, 20, None), (6, 70, tuning_with(sample_rounds=3, cadence=1)),
+             (7, 10, None), (8, 90, tuning_with(sample_rounds=0))]
+    for seed, count, tun in cases:
+        gs = small_batch(seed=seed, count=count)
+        vo, eo, d_rp, d_col, d_lab = to_device(torch, gs)
+        b = batch.Batch()
+        b.graphs = len(gs)
+        b.h_vtx_off = vo.ctypes.data_as(C.POINTER(C.c_uint64))
+        b.h_edge_off = eo.ctypes.data_as(C.POINTER(C.c_uint64))
+        b.d_row_ptr, b.d_col, b.d_labels = d_rp.data_ptr(), d_col.data_ptr(), d_lab.data_ptr()
+        comps = np.zeros(len(gs), np.uint32)
+        _lib.check(L.ccgpu_batch_cc(None, C.byref(b), C.byref(tun) if tun else None,
+                                    comps.ctypes.data, torch.cuda.current_stream().cuda_stream))
+        check_oracle(torch, gs, vo, d_lab, comps)
 
 
 def test_rejects_bad_offsets(torch):
