@@ -299,6 +299,7 @@ def dist_bytes(n, m, st):
     R, U, G, reps = int(st.sorted_keys), int(st.pair_count), int(st.ghost_count), \
         int(st.rep_count)
     lm = int(st.local_entries)
+    sorted_rows = bool(st.sorted_rows)
     return {
         "init": 4 * n, "sample": 8 * (n + 1) + 8 * n, "compress": 8 * n,
         "final_compress": 8 * n, "link_rows": 4 * n + 8 * n, "giant": 4096,
@@ -306,10 +307,13 @@ def dist_bytes(n, m, st):
         "dist_local_fill": 4 * m + 4 * lm + 16 * (n + 1),
         "dist_gflag": 4 * n + n // 8, "dist_pairs_bitmap": 4 * n + 4 * G,
         "dist_merge_keys": 16 * (R + G),
-        "dist_reps": 4 * n + 12 * reps, "dist_pairs": 8 * (n + 1) + 4 * m + n // 8 + 8 * R,
+        "dist_reps": 4 * n + 12 * reps,
+        "dist_pairs": 8 * (n + 1) + 4 * m + (m // 8 if sorted_rows else n // 8 + 8 * R),
+        "dist_pairs_local": n // 8 + 8 * R,
         "sort_hist": 8 * R, "sort_scatter": 16 * R, "dist_dedup": 8 * R,
         "dist_ghosts": 8 * R + 8 * U + 24 * G, "merge_hook": 12 * U,
         "merge_upd": 12 * reps, "merge_exch_pack": 16 * G, "merge_exch_scatter": 16 * G,
+        "merge_exch_pull": 12 * U,
         "dist_labels": 12 * n, "dist_plan": 0, "dist_bounds": 0, "scan": 0,
         "dist_pairs_heavy": 0,
     }
@@ -449,6 +453,7 @@ def run_dist(args, torch, dist_mod, rank, world, dev):
                    bounds=[int(x) for x in bounds], components=int(st.roots),
                    rounds=int(st.rounds), exchanges=int(st.exchanges),
                    boundary_raw=int(st.boundary_raw), sorted_keys=int(st.sorted_keys),
+                   sorted_rows=bool(st.sorted_rows),
                    boundary_dedup=int(st.pair_count),
                    ghosts=int(st.ghost_count), reps=int(st.rep_count),
                    sent_pairs=int(st.sent_pairs), sort_passes=int(st.sort_passes),

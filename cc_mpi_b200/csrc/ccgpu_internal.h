@@ -49,7 +49,11 @@ struct ccgpu_ctx {
     unsigned long long *cell; /* 256-byte device cell for small reductions */
     unsigned long long launches; /* kernels this context has launched */
     struct cc_prof *prof;        /* per-kernel event timing, NULL = off */
+    struct ccgpu_batch_plan *batch_cache; /* the plan ccgpu_batch_cc reuses */
 };
+
+/* Frees the context's cached batch plan (batch_cc.cu). */
+void cc_batch_cache_free(ccgpu_ctx *ctx);
 
 /* Kernel ids for the launch profiler (names in runtime.cu). */
 enum {
@@ -96,6 +100,8 @@ enum {
     CCK_DIST_TILES,
     CCK_DIST_GFLAG,
     CCK_DIST_MERGE_KEYS,
+    CCK_MERGE_EXCH_PULL,
+    CCK_DIST_PAIRS_LOCAL,
     CCK_NUM
 };
 

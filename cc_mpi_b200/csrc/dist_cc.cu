@@ -42,7 +42,6 @@ namespace {
 
 constexpr int kB = 256;
 constexpr int kW = kB / 32;
-constexpr int kEmitBuf = 256;           /* keys per warp buffer           */
 constexpr int kTileE = 16;              /* column entries per thread in a tile */
 constexpr int kTile = kB * kTileE;      /* column entries per tile             */
 constexpr int kDedupItems = 16;
@@ -136,37 +135,47 @@ struct EmitParams {
     const uint32_t *giants;  /* [parts] giant root of each partition, NULL = no masks */
     uint64_t tiles;          /* column tiles of kTile entries     */
     const uint32_t *tile_first; /* [tiles+1] first row starting after each tile's first entry */
+    int vec;                 /* col is 16-byte aligned: 16-byte loads */
+    uint32_t *ngbits;        /* [m/32] bit j: entry j points to a vertex outside its
+                              * partition's giant tree (sorted-row mode), NULL = gather gflag */
+    unsigned long long *bad; /* set when a row is not strictly ascending or a
+                              * mirror entry is missing: sorted-row mode invalid */
 };
 
-struct WarpBuf {
-    uint64_t *buf;
-    uint32_t cnt;
+/* Plain keys are rare (most cut entries fall in a giant tree), so a block
+ * collects them in shared memory through a shared counter and writes them
+ * out with one global reservation when the buffer is half full.  A key
+ * arriving at a full buffer reserves its own slot. */
+constexpr uint32_t kKeyBuf = 2048;
+
+struct KeyBuf {
+    uint64_t *keys;
+    uint32_t *cnt;
+    unsigned long long *base;
 };
 
-__device__ __noinline__ void wb_flush(WarpBuf &w, const EmitParams &E, int lane)
+__device__ __forceinline__ void kb_put(const KeyBuf &kb, const EmitParams &E, uint64_t key)
 {
-    __syncwarp();
-    unsigned long long base = 0;
-    if (lane == 0 && w.cnt)
-        base = atomicAdd(E.count, (unsigned long long)w.cnt);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    for (uint32_t i = lane; i < w.cnt; i += 32)
-        E.out[base + i] = w.buf[i];
-    w.cnt = 0;
-    __syncwarp();
+    const uint32_t pos = atomicAdd(kb.cnt, 1u);
+    if (pos < kKeyBuf)
+        kb.keys[pos] = key;
+    else
+        E.out[atomicAdd(E.count, 1ull)] = key;
 }
 
-__device__ __forceinline__ void wb_append(WarpBuf &w, const EmitParams &E, int lane, bool pred,
-                                          uint64_t key)
+/* Block-uniform: every thread passes the count it read after a barrier. */
+__device__ __noinline__ void kb_flush(const KeyBuf &kb, const EmitParams &E, uint32_t kc)
 {
-    unsigned mask = __ballot_sync(0xffffffffu, pred);
-    if (!mask)
-        return;
-    if (w.cnt + 32 > kEmitBuf)
-        wb_flush(w, E, lane);
-    if (pred)
-        w.buf[w.cnt + __popc(mask & ((1u << lane) - 1u))] = key;
-    w.cnt += __popc(mask);
+    const uint32_t nk = kc < kKeyBuf ? kc : kKeyBuf;
+    if (threadIdx.x == 0)
+        *kb.base = atomicAdd(E.count, (unsigned long long)nk);
+    __syncthreads();
+    const unsigned long long base = *kb.base;
+    for (uint32_t i = threadIdx.x; i < nk; i += blockDim.x)
+        E.out[base + i] = kb.keys[i];
+    __syncthreads();
+    if (threadIdx.x == 0)
+        *kb.cnt = 0;
 }
 
 __device__ __forceinline__ uint64_t make_key(const EmitParams &E, int p, uint32_t u, uint32_t rep)
@@ -235,17 +244,17 @@ __global__ void __launch_bounds__(kB) k_giant_flags(EmitParams E)
  * marks over the tile (rows are laid out in vertex order, so the last row
  * start at or before a position is its row).  Long rows need no special
  * path. */
-/* Partition of v: compares against bounds held in registers when there
- * are at most 8 partitions, else a binary search in shared memory. */
+/* Partition of v < n: compares against bounds held in registers when
+ * there are at most 8 partitions, else a binary search in shared memory. */
 template <int PMAX>
 __device__ __forceinline__ int part_fast(const uint32_t *s_b, const uint32_t *rb, int parts,
                                          uint32_t v)
 {
-    if (PMAX <= 8) {
+    if (PMAX <= 8) { /* rb[parts] = n and rb[i > parts] = ~0: exact for v < n */
         int p = 0;
 #pragma unroll
         for (int i = 1; i < PMAX; ++i)
-            p += (i < parts) & (v >= rb[i]);
+            p += v >= rb[i];
         return p;
     }
     return part_of(s_b, parts, v);
@@ -262,70 +271,58 @@ __device__ __forceinline__ void mask_or(uint32_t *w, uint32_t bits)
         atomicOr(w, bits);
 }
 
-/* Position i of a tile's row-start array, padded by one word per 32 so
- * that thread t reading its 16 consecutive positions (t * 16 + k) hits 32
- * distinct banks across a warp. */
-#define HP(i) ((i) + ((i) >> 5))
+/* Position i of a tile's row-start array, padded by four words per 32 so
+ * that thread t's 16 consecutive positions (t * 16 + k) start on a 16-byte
+ * boundary and a quarter-warp's 16-byte reads cover 32 distinct banks. */
+#define HP(i) ((i) + 4 * ((i) >> 5))
+constexpr int kHeadWords = kTile + 4 * (kTile / 32);
 
-template <int PMAX>
+/* Boundary pairs from the remote end over one column tile per block
+ * iteration.  SORTED (sorted-row mode): rows ascend, so along a row the
+ * entries' partition is stepped forward against the next bound; an
+ * unmarked cut entry sets bit pv in the row's mask (marked ones had their
+ * keys written by the local end, k_ng_*), and a row that is not strictly
+ * ascending sets *bad.  Otherwise each cut entry gathers its giant flag and
+ * non-giant ones emit their key here. */
+template <int PMAX, bool SORTED>
 __global__ void __launch_bounds__(kB, 4) k_emit(EmitParams E)
 {
-    __shared__ uint64_t s_buf[kW][kEmitBuf];
-    __shared__ uint32_t s_b[CCGPU_MAX_PARTS + 1];
-    __shared__ uint32_t s_head[kTile + kTile / 32]; /* padded: see HP() */
+    __shared__ uint64_t s_keys[kKeyBuf];
+    __shared__ __align__(16) uint32_t s_head[kHeadWords];
+    __shared__ uint32_t s_b[CCGPU_MAX_PARTS + 2]; /* bounds, then ~0 */
     __shared__ uint32_t s_w[kW];
-    for (int i = threadIdx.x; i <= E.parts; i += kB)
-        s_b[i] = E.bounds[i];
+    __shared__ uint32_t s_last[kW]; /* each warp's last entry */
+    __shared__ uint32_t s_kcnt;
+    __shared__ unsigned long long s_kbase;
+    for (int i = threadIdx.x; i < CCGPU_MAX_PARTS + 2; i += kB)
+        s_b[i] = i <= E.parts ? E.bounds[i] : 0xffffffffu;
+    if (threadIdx.x == 0)
+        s_kcnt = 0;
+    /* Row-start marks are not cleared between tiles: a block's tiles come
+     * in column order, so a stale mark names a row before the current
+     * tile's first row (v0 - 1, stored at position 0) and never raises the
+     * max-scan. */
+    uint4 *h4 = reinterpret_cast<uint4 *>(s_head);
+    for (int i = threadIdx.x; i < kHeadWords / 4; i += kB)
+        h4[i] = make_uint4(0u, 0u, 0u, 0u);
     unsigned long long raw = 0;
     __syncthreads();
     uint32_t sb[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i)
-        sb[i] = i <= E.parts ? s_b[i] : 0xffffffffu;
+        sb[i] = s_b[i];
+    const uint64_t allp = E.parts >= 32 ? 0xffffffffull : (1ull << E.parts) - 1;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    WarpBuf w = {s_buf[warp], 0};
+    const KeyBuf kbuf = {s_keys, &s_kcnt, &s_kbase};
+    const uint4 *mine = reinterpret_cast<const uint4 *>(s_head + HP(threadIdx.x * kTileE));
+    bool unsorted = false;
     for (uint64_t t = blockIdx.x; t < E.tiles; t += gridDim.x) {
         const uint64_t lo = t * kTile;
         const uint32_t v0 = E.tile_first[t], v1 = E.tile_first[t + 1];
-        for (int i = threadIdx.x; i < kTile + kTile / 32; i += kB)
-            s_head[i] = 0;
-        __syncthreads();
-        if (threadIdx.x == 0)
-            s_head[0] = v0 > 0 ? v0 - 1 : 0; /* the row holding the tile's first entry */
-        __syncthreads();
-        for (uint64_t v = (uint64_t)v0 + threadIdx.x; v < v1 && v < E.n; v += kB) {
-            const uint64_t rp = __ldg(E.row_ptr + v);
-            if (rp < lo + kTile)
-                atomicMax(s_head + HP(rp - lo), (uint32_t)v);
-        }
-        __syncthreads();
-        /* inclusive max-scan of s_head: 16 positions per thread */
-        uint32_t run = 0;
-#pragma unroll
-        for (int k = 0; k < kTileE; ++k) {
-            const uint32_t h = s_head[HP(threadIdx.x * kTileE + k)];
-            run = h > run ? h : run;
-        }
-        uint32_t incl = run;
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o)
-                incl = y > incl ? y : incl;
-        }
-        if (lane == 31)
-            s_w[warp] = incl;
-        __syncthreads();
-        uint32_t pre = 0;
-        for (int k = 0; k < warp; ++k)
-            pre = s_w[k] > pre ? s_w[k] : pre;
-        uint32_t before = __shfl_up_sync(0xffffffffu, incl, 1);
-        if (lane == 0)
-            before = 0;
-        before = before > pre ? before : pre; /* max over earlier threads */
-        /* this thread's 16 entries */
+        /* this thread's 16 entries; positions past m read as no vertex */
         const uint64_t j0 = lo + (uint64_t)threadIdx.x * kTileE;
         uint32_t c[kTileE];
-        if (j0 + kTileE <= E.m) {
+        if (E.vec && j0 + kTileE <= E.m) {
             const uint4 *c4 = reinterpret_cast<const uint4 *>(E.col + j0);
 #pragma unroll
             for (int q = 0; q < kTileE / 4; ++q) {
@@ -338,43 +335,286 @@ __global__ void __launch_bounds__(kB, 4) k_emit(EmitParams E)
         } else {
 #pragma unroll
             for (int k = 0; k < kTileE; ++k)
-                c[k] = j0 + k < E.m ? __ldg(E.col + j0 + k) : 0u;
+                c[k] = j0 + k < E.m ? __ldg(E.col + j0 + k) : 0xffffffffu;
         }
-        uint32_t row = 0xffffffffu, bits = 0;
-        int pu = 0;
-        uint32_t cur = before;
+        /* sorted-row mode: marks of the 16 entries (j0 is a multiple of 16) */
+        const uint32_t ng = SORTED && j0 < E.m ? __ldg(E.ngbits + (j0 >> 5)) >> (j0 & 31) : 0u;
+        const int kv = j0 >= E.m ? 0 : (E.m - j0 < kTileE ? (int)(E.m - j0) : kTileE);
+        /* position 0 holds the row of the tile's first entry; no row in
+         * [v0, v1) starts there */
+        if (threadIdx.x == 0)
+            s_head[0] = v0 > 0 ? v0 - 1 : 0u;
+        for (uint64_t v = (uint64_t)v0 + threadIdx.x; v < v1 && v < E.n; v += kB) {
+            const uint64_t rp = __ldg(E.row_ptr + v);
+            if (rp >= lo && rp < lo + kTile)
+                atomicMax(s_head + HP(rp - lo), (uint32_t)v);
+        }
+        __syncthreads();
+        /* inclusive max-scan of the row starts: 16 positions per thread */
+        uint32_t run = 0;
 #pragma unroll
-        for (int k = 0; k < kTileE; ++k) {
-            const uint32_t h = s_head[HP(threadIdx.x * kTileE + k)];
-            cur = h > cur ? h : cur;
-            const uint32_t v = c[k];
-            const bool ok = j0 + k < E.m && cur < E.n && v < E.n;
-            if (ok && cur != row) {
-                if (bits)
-                    mask_or(E.pmask + row, bits);
-                bits = 0;
-                row = cur;
-                pu = part_fast<PMAX>(s_b, sb, E.parts, row);
+        for (int q = 0; q < kTileE / 4; ++q) {
+            const uint4 x = mine[q];
+            run = max(max(run, max(x.x, x.y)), max(x.z, x.w));
+        }
+        uint32_t incl = run;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o)
+                incl = y > incl ? y : incl;
+        }
+        if (lane == 31) {
+            s_w[warp] = incl;
+            s_last[warp] = c[kTileE - 1];
+        }
+        __syncthreads();
+        uint32_t pre = 0;
+        for (int k = 0; k < warp; ++k)
+            pre = s_w[k] > pre ? s_w[k] : pre;
+        uint32_t before = __shfl_up_sync(0xffffffffu, incl, 1);
+        if (lane == 0)
+            before = 0;
+        before = before > pre ? before : pre; /* max over earlier threads */
+        /* the row of the entry before j0 (none: ~0), and that entry */
+        uint32_t prow = before, prev = __shfl_up_sync(0xffffffffu, c[kTileE - 1], 1);
+        if (lane == 0)
+            prev = warp > 0 ? s_last[warp - 1] : 0u;
+        if (threadIdx.x == 0) {
+            prow = 0xffffffffu;
+            if (SORTED && lo > 0 && v0 > 0 && __ldg(E.row_ptr + v0 - 1) < lo) {
+                prow = v0 - 1; /* the tile's first row began in an earlier tile */
+                prev = __ldg(E.col + lo - 1);
             }
-            const int pv = ok ? part_fast<PMAX>(s_b, sb, E.parts, v) : 0;
-            const bool bnd = ok && pv != pu;
-            bool gnt = false;
-            if (bnd && E.gflag)
-                gnt = (__ldg(E.gflag + (v >> 5)) >> (v & 31)) & 1u;
-            if (gnt)
-                bits |= 1u << pv;
-            raw += bnd;
-            uint64_t key = 0;
-            if (bnd && !gnt)
-                key = make_key(E, pv, row, __ldg(E.label + v) - s_b[pv]);
-            wb_append(w, E, lane, bnd && !gnt, key);
+        }
+        uint32_t row = prow, bits = 0, rawc = 0;
+        int pu = row < E.n ? part_fast<PMAX>(s_b, sb, E.parts, row) : -1;
+        uint32_t cur = before; /* running max of the row starts: the row of entry k */
+        if (SORTED) {
+            /* Entries >= n are clamped to n, which steps to partition P
+             * (none).  cutm: bit p set when p is a valid partition other
+             * than the row's. */
+            uint64_t cutm = pu >= 0 ? allp & ~(1ull << pu) : 0ull;
+            uint32_t v = c[0] < E.n ? c[0] : E.n;
+            int pv = part_fast<PMAX>(s_b, sb, E.parts, v < E.n ? v : E.n - 1);
+            uint32_t nb = s_b[pv + 1];
+#pragma unroll
+            for (int q = 0; q < kTileE / 4; ++q) {
+                const uint4 x = mine[q];
+                const uint32_t hs[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int k = 4 * q + e;
+                    cur = hs[e] > cur ? hs[e] : cur;
+                    v = c[k] < E.n ? c[k] : E.n;
+                    if (cur != row) {
+                        if (bits)
+                            mask_or(E.pmask + row, bits);
+                        bits = 0;
+                        row = cur;
+                        pu = row < E.n ? part_fast<PMAX>(s_b, sb, E.parts, row) : -1;
+                        cutm = pu >= 0 ? allp & ~(1ull << pu) : 0ull;
+                        pv = part_fast<PMAX>(s_b, sb, E.parts, v < E.n ? v : E.n - 1);
+                        nb = s_b[pv + 1];
+                    } else {
+                        unsorted |= c[k] <= prev && k < kv;
+                    }
+                    while (v >= nb) {
+                        ++pv;
+                        nb = s_b[pv + 1];
+                    }
+                    prev = c[k];
+                    const uint32_t cut = (uint32_t)(cutm >> pv) & 1u;
+                    rawc += cut;
+                    bits |= (cut & ~(ng >> k)) << (pv & 31);
+                }
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < kTileE / 4; ++q) {
+                const uint4 x = mine[q];
+                const uint32_t hs[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int k = 4 * q + e;
+                    cur = hs[e] > cur ? hs[e] : cur;
+                    const uint32_t v = c[k];
+                    if (cur != row) {
+                        if (bits)
+                            mask_or(E.pmask + row, bits);
+                        bits = 0;
+                        row = cur;
+                        pu = row < E.n ? part_fast<PMAX>(s_b, sb, E.parts, row) : -1;
+                    }
+                    const int pv = part_fast<PMAX>(s_b, sb, E.parts, v);
+                    if (pv != pu && v < E.n && pu >= 0) { /* a cut edge */
+                        ++rawc;
+                        bool gnt = false;
+                        if (E.gflag)
+                            gnt = (__ldg(E.gflag + (v >> 5)) >> (v & 31)) & 1u;
+                        if (gnt)
+                            bits |= 1u << pv;
+                        else
+                            kb_put(kbuf, E, make_key(E, pv, row, __ldg(E.label + v) - s_b[pv]));
+                    }
+                }
+            }
         }
         if (bits)
             mask_or(E.pmask + row, bits);
+        raw += rawc;
         __syncthreads();
+        const uint32_t kc = s_kcnt;
+        if (kc >= kKeyBuf / 2)
+            kb_flush(kbuf, E, kc);
     }
-    wb_flush(w, E, lane);
+    if (unsorted)
+        *E.bad = 1ull;
+    __syncthreads();
+    const uint32_t kc = s_kcnt;
+    if (kc)
+        kb_flush(kbuf, E, kc);
     add_raw(E, raw, lane);
+}
+
+/* Sorted-row mode, local end: the rows of vertices outside their
+ * partition's giant tree (few, mostly short).  For every cut entry u of
+ * such a row v the key (p, u, rep(v)) is written here, and the mirror entry
+ * v of row u is marked in ngbits, so the remote-end pass (k_emit) sends
+ * every unmarked cut entry to the giant mask without reading gflag.  Three
+ * passes: cut entries per such row (k_ng_count), after a scan their keys
+ * and (u, v) work items at the row's offset (k_ng_emit), then one search
+ * per item (k_ng_mark); a mirror that is not found sets *bad. */
+template <int PMAX>
+__device__ __forceinline__ bool ng_row(const EmitParams &E, const uint32_t *s_b,
+                                       const uint32_t *sb, uint32_t v, uint64_t &b, uint64_t &e,
+                                       int &pv)
+{
+    if ((__ldg(E.gflag + (v >> 5)) >> (v & 31)) & 1u)
+        return false;
+    b = __ldg(E.row_ptr + v);
+    e = __ldg(E.row_ptr + v + 1);
+    e = e > E.m ? E.m : e;
+    b = b > e ? e : b;
+    pv = part_fast<PMAX>(s_b, sb, E.parts, v);
+    return b < e;
+}
+
+#define NG_PROLOGUE                                                    \
+    __shared__ uint32_t s_b[CCGPU_MAX_PARTS + 1];                      \
+    for (int i = threadIdx.x; i <= E.parts; i += kB)                   \
+        s_b[i] = E.bounds[i];                                          \
+    __syncthreads();                                                   \
+    uint32_t sb[8];                                                    \
+    _Pragma("unroll") for (int i = 0; i < 8; ++i) sb[i] =              \
+        i <= E.parts ? s_b[i] : 0xffffffffu;                           \
+    const uint64_t stride = (uint64_t)gridDim.x * kB
+
+template <int PMAX>
+__global__ void __launch_bounds__(kB) k_ng_count(EmitParams E, uint32_t *cnt)
+{
+    NG_PROLOGUE;
+    for (uint64_t v = (uint64_t)blockIdx.x * kB + threadIdx.x; v < E.n; v += stride) {
+        uint64_t b, e;
+        int pv;
+        uint32_t c = 0;
+        if (ng_row<PMAX>(E, s_b, sb, (uint32_t)v, b, e, pv))
+            for (uint64_t j = b; j < e; ++j) {
+                const uint32_t u = __ldg(E.col + j);
+                c += u < E.n && part_fast<PMAX>(s_b, sb, E.parts, u) != pv;
+            }
+        cnt[v] = c;
+    }
+}
+
+template <int PMAX>
+__global__ void __launch_bounds__(kB) k_ng_emit(EmitParams E, const uint64_t *off,
+                                                uint64_t *work)
+{
+    NG_PROLOGUE;
+    for (uint64_t v = (uint64_t)blockIdx.x * kB + threadIdx.x; v < E.n; v += stride) {
+        uint64_t b, e;
+        int pv;
+        if (!ng_row<PMAX>(E, s_b, sb, (uint32_t)v, b, e, pv))
+            continue;
+        uint64_t o = off[v];
+        const uint64_t o_end = off[v + 1];
+        const uint32_t rep = __ldg(E.label + v) - s_b[pv];
+        for (uint64_t j = b; j < e && o < o_end; ++j) {
+            const uint32_t u = __ldg(E.col + j);
+            if (u >= E.n || part_fast<PMAX>(s_b, sb, E.parts, u) == pv)
+                continue;
+            E.out[o] = make_key(E, pv, u, rep);
+            work[o] = ((uint64_t)u << 32) | (uint32_t)v;
+            ++o;
+        }
+    }
+}
+
+/* Position of v in the strictly ascending col[lo, hi), or ~0.  Up to four
+ * interpolation probes (ids spread evenly, so each lands close to v), then
+ * a binary search of what is left.  Probes differ from search to search,
+ * where plain bisection would send every search of a long row through the
+ * same few middle entries. */
+__device__ __forceinline__ uint64_t find_sorted(const uint32_t *col, uint64_t lo, uint64_t hi,
+                                                uint32_t v)
+{
+    constexpr uint64_t kNone = ~0ull;
+    if (lo >= hi)
+        return kNone;
+    uint32_t a = __ldg(col + lo), z = __ldg(col + hi - 1);
+    if (v == a)
+        return lo;
+    if (v == z)
+        return hi - 1;
+    if (v < a || v > z)
+        return kNone;
+    /* col[lo] = a < v < z = col[hi - 1] */
+    for (int it = 0; it < 4 && hi - lo > 16; ++it) {
+        const uint64_t span = hi - 1 - lo;
+        uint64_t p = lo + (uint64_t)((double)(v - a) / (double)(z - a) * (double)span);
+        p = p <= lo ? lo + 1 : (p >= hi - 1 ? hi - 2 : p);
+        const uint32_t x = __ldg(col + p);
+        if (x == v)
+            return p;
+        if (x < v) {
+            lo = p;
+            a = x;
+        } else {
+            hi = p + 1;
+            z = x;
+        }
+    }
+    uint64_t l = lo + 1, h = hi - 1; /* first entry >= v in (lo, hi - 1) */
+    while (l < h) {
+        const uint64_t mid = l + (h - l) / 2;
+        if (__ldg(col + mid) < v)
+            l = mid + 1;
+        else
+            h = mid;
+    }
+    return l < hi - 1 && __ldg(col + l) == v ? l : kNone;
+}
+
+__global__ void __launch_bounds__(kB) k_ng_mark(EmitParams E, const uint64_t *work,
+                                                const uint64_t *total)
+{
+    const uint64_t items = *total;
+    const uint64_t stride = (uint64_t)gridDim.x * kB;
+    bool missing = false;
+    for (uint64_t i = (uint64_t)blockIdx.x * kB + threadIdx.x; i < items; i += stride) {
+        const uint64_t w = work[i];
+        const uint32_t u = (uint32_t)(w >> 32), v = (uint32_t)w;
+        uint64_t lo = __ldg(E.row_ptr + u), hi = __ldg(E.row_ptr + u + 1);
+        hi = hi > E.m ? E.m : hi;
+        lo = lo > hi ? hi : lo;
+        const uint64_t pos = find_sorted(E.col, lo, hi, v);
+        if (pos != ~0ull)
+            atomicOr(E.ngbits + (pos >> 5), 1u << (pos & 31));
+        else
+            missing = true;
+    }
+    if (missing)
+        *E.bad = 1ull;
 }
 
 /* The mask keys in sorted order: key (p, u, giant rep of p) for every bit
@@ -545,6 +785,7 @@ struct LocalParams {
     uint32_t *tile_first;       /* [tiles+1] first row starting after the tile's first entry */
     uint64_t *lrp;              /* [n+1] local row pointers           */
     uint32_t *lcol;             /* [tile_off[tiles]] kept entries     */
+    int vec;                    /* col is 16-byte aligned: 16-byte loads */
 };
 
 /* tile_first[t] = smallest v with row_ptr[v] > t * kTile (v in [0, n]),
@@ -598,7 +839,7 @@ __device__ __forceinline__ uint32_t tile_keep(const LocalParams &L, const uint32
                                               uint32_t *u)
 {
     const uint64_t j0 = tile * kTile + (uint64_t)threadIdx.x * kTileE;
-    if (j0 + kTileE <= L.m) {
+    if (L.vec && j0 + kTileE <= L.m) {
         const uint4 *c4 = reinterpret_cast<const uint4 *>(L.col + j0);
 #pragma unroll
         for (int q = 0; q < kTileE / 4; ++q) {
@@ -993,7 +1234,17 @@ struct MergeParams {
     uint32_t *msg_count;          /* [parts*parts], [q*parts+p] */
     int *changed;                 /* [parts] */
     unsigned long long *sent;
+    uint32_t *ghost_rep;          /* [ghosts] local rep of each ghost vertex */
+    int ghost_rep_ready;          /* 0: k_pack fills ghost_rep from label[] */
 };
+
+/* An exchange lowers the hook minima by one pass over every pair (pull)
+ * when it carries more than one message per 8 pairs; below that, the
+ * receiver walks the pairs of each received ghost (push). */
+__device__ __forceinline__ bool pull_hooks(const MergeParams &M, uint64_t messages)
+{
+    return messages * 8 > M.pairs;
+}
 
 /* hook[rep] = min over the rep's cut pairs of the ghost labels. */
 __global__ void __launch_bounds__(kB) k_hook_init(MergeParams M)
@@ -1092,7 +1343,14 @@ __global__ void __launch_bounds__(kB) k_pack(MergeParams M)
                     hi = mid;
             }
             int p = lo;
-            lbl = M.cur[__ldg(M.label + u)];
+            uint32_t rep;
+            if (M.ghost_rep_ready) {
+                rep = __ldg(M.ghost_rep + g);
+            } else {
+                rep = __ldg(M.label + u); /* fixed by the local solve */
+                M.ghost_rep[g] = rep;
+            }
+            lbl = M.cur[rep];
             if (lbl < M.prev_sent[g]) {
                 M.prev_sent[g] = lbl;
                 send = true;
@@ -1184,6 +1442,7 @@ __global__ void __launch_bounds__(kB) k_scatter_sent(MergeParams M)
     }
     __syncthreads();
     const uint32_t total = s_pre[R];
+    const bool push = !pull_hooks(M, total);
     const int lane = threadIdx.x & 31;
     const uint64_t stride = (uint64_t)gridDim.x * kB;
     for (uint64_t base = (uint64_t)blockIdx.x * kB; base < total; base += stride) {
@@ -1205,8 +1464,10 @@ __global__ void __launch_bounds__(kB) k_scatter_sent(MergeParams M)
             const uint64_t g = rstart + (pr >> 32);
             lbl = (uint32_t)pr;
             M.ghost_labels[g] = lbl;
-            k0 = M.ghost_pairs[g];
-            k1 = M.ghost_pairs[g + 1];
+            if (push) {
+                k0 = M.ghost_pairs[g];
+                k1 = M.ghost_pairs[g + 1];
+            }
         }
         /* hook minima, one pair per lane per step: lanes whose pairs share a
          * rep (most cut pairs of a partition carry its giant rep) combine
@@ -1230,6 +1491,37 @@ __global__ void __launch_bounds__(kB) k_scatter_sent(MergeParams M)
         const unsigned got = __popc(__ballot_sync(0xffffffffu, has));
         if (lane == 0 && got)
             atomicAdd(M.sent, (unsigned long long)got);
+    }
+}
+
+/* Pull side of an exchange with many messages: after k_scatter_sent wrote
+ * the received ghost labels, one pass over every pair lowers the hook
+ * minima.  Ghost labels only decrease and hook[r] already bounds the old
+ * labels of r's ghosts, so the minima equal the push side's.  Does nothing
+ * when the exchange used the push side. */
+__global__ void __launch_bounds__(kB) k_hook_pull(MergeParams M)
+{
+    __shared__ uint64_t s_total;
+    if (threadIdx.x == 0) {
+        uint64_t t = 0;
+        for (int r = 0; r < M.parts * M.parts; ++r)
+            t += M.msg_count[r];
+        s_total = t;
+    }
+    __syncthreads();
+    if (!pull_hooks(M, s_total))
+        return;
+    const int lane = threadIdx.x & 31;
+    const uint64_t stride = (uint64_t)gridDim.x * kB;
+    for (uint64_t base = (uint64_t)blockIdx.x * kB; base < M.pairs; base += stride) {
+        const uint64_t k = base + threadIdx.x;
+        const bool ok = k < M.pairs;
+        const uint32_t r = ok ? M.pair_rep[k] : 0xffffffffu;
+        const uint32_t l = ok ? M.ghost_labels[M.pair_g[k]] : 0xffffffffu;
+        const unsigned peers = __match_any_sync(0xffffffffu, r);
+        const uint32_t mn = __reduce_min_sync(peers, l);
+        if (ok && (__ffs(peers) - 1) == lane && mn < M.hook[r])
+            atomicMin(M.hook + r, mn);
     }
 }
 
@@ -1371,6 +1663,7 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
         LocalParams Lp;
         Lp.row_ptr = d_row_ptr;
         Lp.col = d_col;
+        Lp.vec = ((uintptr_t)d_col & 15) == 0;
         Lp.n = n;
         Lp.m = m;
         Lp.bounds = bounds;
@@ -1440,6 +1733,7 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
     EmitParams E;
     E.row_ptr = d_row_ptr;
     E.col = d_col;
+    E.vec = ((uintptr_t)d_col & 15) == 0;
     E.label = label;
     E.bounds = bounds;
     E.n = n;
@@ -1465,19 +1759,83 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
         CC_KLAUNCH(ctx, CCK_DIST_GFLAG, k_giant_flags,
                    cc_blocks(n, kB, (unsigned)ctx->sm_count * 8), kB, 0, st, E);
     }
-    if (P > 1 && col_tiles) {
+    /* Sorted-row mode (giant masks on): the local end writes the plain keys
+     * and marks their mirror entries, the remote end reads the marks
+     * instead of gathering gflag.  Both passes check that rows are strictly
+     * ascending and symmetric; if not, the pairs are made again by the
+     * gather pass alone. */
+    E.ngbits = nullptr;
+    E.bad = counters + 6;
+    const bool sorted_mode = use_mask && P > 1 && col_tiles > 0;
+    auto emit = [&]() -> int {
         const unsigned eb = cc_blocks(col_tiles, 1, (unsigned)ctx->sm_count * 4);
-        if (P <= 4)
-            CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit<4>, eb, kB, 0, st, E);
-        else if (P <= 8)
-            CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit<8>, eb, kB, 0, st, E);
-        else
-            CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit<CCGPU_MAX_PARTS>, eb, kB, 0, st, E);
+        const unsigned lb = cc_blocks(n, kB, (unsigned)ctx->sm_count * 8);
+        if (E.ngbits) {
+            uint32_t *cnt = nullptr;
+            uint64_t *off = nullptr, *work = nullptr;
+            CC_TRY(cc_bufs_get(&B, (void **)&cnt, (size_t)n * sizeof(uint32_t)));
+            CC_TRY(cc_bufs_get(&B, (void **)&off, ((size_t)n + 1) * sizeof(uint64_t)));
+            if (P <= 4)
+                CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_count<4>, lb, kB, 0, st, E, cnt);
+            else if (P <= 8)
+                CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_count<8>, lb, kB, 0, st, E, cnt);
+            else
+                CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_count<CCGPU_MAX_PARTS>, lb, kB, 0, st,
+                           E, cnt);
+            CC_TRY(cc_scan_u32(ctx, cnt, off, n, &B, st));
+            unsigned long long items = 0;
+            CC_CUDA(cudaMemcpyAsync(&items, off + n, sizeof(items), cudaMemcpyDeviceToHost, st));
+            CC_CUDA(cudaStreamSynchronize(st));
+            CC_TRY(cc_bufs_get(&B, (void **)&work, (size_t)(items ? items : 1) * sizeof(uint64_t)));
+            if (P <= 4)
+                CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_emit<4>, lb, kB, 0, st, E, off, work);
+            else if (P <= 8)
+                CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_emit<8>, lb, kB, 0, st, E, off, work);
+            else
+                CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_emit<CCGPU_MAX_PARTS>, lb, kB, 0, st,
+                           E, off, work);
+            CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_mark, lb, kB, 0, st, E, work, off + n);
+            CC_CUDA(cudaMemcpyAsync(E.count, off + n, sizeof(unsigned long long),
+                                    cudaMemcpyDeviceToDevice, st));
+            if (P <= 4)
+                CC_KLAUNCH(ctx, CCK_DIST_PAIRS, (k_emit<4, true>), eb, kB, 0, st, E);
+            else if (P <= 8)
+                CC_KLAUNCH(ctx, CCK_DIST_PAIRS, (k_emit<8, true>), eb, kB, 0, st, E);
+            else
+                CC_KLAUNCH(ctx, CCK_DIST_PAIRS, (k_emit<CCGPU_MAX_PARTS, true>), eb, kB, 0, st, E);
+        } else {
+            if (P <= 4)
+                CC_KLAUNCH(ctx, CCK_DIST_PAIRS, (k_emit<4, false>), eb, kB, 0, st, E);
+            else if (P <= 8)
+                CC_KLAUNCH(ctx, CCK_DIST_PAIRS, (k_emit<8, false>), eb, kB, 0, st, E);
+            else
+                CC_KLAUNCH(ctx, CCK_DIST_PAIRS, (k_emit<CCGPU_MAX_PARTS, false>), eb, kB, 0, st,
+                           E);
+        }
+        return CCGPU_OK;
+    };
+    if (sorted_mode) {
+        const size_t words = (size_t)((m + 31) / 32);
+        CC_TRY(cc_bufs_get(&B, (void **)&E.ngbits, words * 4));
+        CC_CUDA(cudaMemsetAsync(E.ngbits, 0, words * 4, st));
     }
-    unsigned long long hc[5];
-    CC_CUDA(cudaMemcpyAsync(hc, counters, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+    if (P > 1 && col_tiles)
+        CC_TRY(emit());
+    unsigned long long hc[7];
+    CC_CUDA(cudaMemcpyAsync(hc, counters, 7 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                             st));
     CC_CUDA(cudaStreamSynchronize(st));
+    if (sorted_mode && hc[6]) {
+        E.ngbits = nullptr;
+        CC_CUDA(cudaMemsetAsync(counters, 0, sizeof(unsigned long long), st));
+        CC_CUDA(cudaMemsetAsync(counters + 4, 0, sizeof(unsigned long long), st));
+        CC_CUDA(cudaMemsetAsync(E.pmask, 0, (size_t)n * 4, st));
+        CC_TRY(emit());
+        CC_CUDA(cudaMemcpyAsync(hc, counters, 7 * sizeof(unsigned long long),
+                                cudaMemcpyDeviceToHost, st));
+        CC_CUDA(cudaStreamSynchronize(st));
+    }
+    S.sorted_rows = sorted_mode && !hc[6];
     const uint64_t R = hc[0];
     S.boundary_raw = hc[4];
     S.sorted_keys = R;
@@ -1639,6 +1997,8 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
     CC_TRY(cc_bufs_get(&B, (void **)&M.msg, (size_t)(G ? G : 1) * sizeof(uint64_t)));
     CC_TRY(cc_bufs_get(&B, (void **)&M.msg_count, (size_t)P * P * sizeof(uint32_t)));
     CC_TRY(cc_bufs_get(&B, (void **)&M.changed, P * sizeof(int)));
+    CC_TRY(cc_bufs_get(&B, (void **)&M.ghost_rep, (size_t)(G ? G : 1) * sizeof(uint32_t)));
+    M.ghost_rep_ready = 0;
     CC_CUDA(cudaMemsetAsync(M.msg_count, 0, (size_t)P * P * sizeof(uint32_t), st));
     const unsigned gbk = (unsigned)ctx->sm_count * 8;
     if (U > 0) {
@@ -1684,10 +2044,13 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
         if (steps >= interval || !any_changed) {
             M.cur = pc;
             CC_KLAUNCH(ctx, CCK_MERGE_EXCH_PACK, k_pack, cc_blocks(G, kB, gbk), kB, 0, st, M);
-            if (P <= kSmallParts)
+            M.ghost_rep_ready = 1;
+            if (P <= kSmallParts) {
                 CC_KLAUNCH(ctx, CCK_MERGE_EXCH_SCATTER, k_scatter_sent, cc_blocks(G, kB, gbk), kB,
                            0, st, M);
-            else
+                CC_KLAUNCH(ctx, CCK_MERGE_EXCH_PULL, k_hook_pull, cc_blocks(U, kB, gbk), kB, 0,
+                           st, M);
+            } else
                 CC_KLAUNCH(ctx, CCK_MERGE_EXCH_SCATTER, k_scatter, cc_blocks(G, kB, gbk), kB, 0,
                            st, M);
             CC_CUDA(cudaMemsetAsync(M.msg_count, 0, (size_t)P * P * sizeof(uint32_t), st));

@@ -24,7 +24,8 @@ class DistStats(C.Structure):
                 ("sent_pairs", C.c_uint64), ("ms_bounds", C.c_double), ("ms_local", C.c_double),
                 ("ms_pairs", C.c_double), ("ms_sort", C.c_double), ("ms_ghosts", C.c_double),
                 ("ms_merge", C.c_double), ("ms_total", C.c_double),
-                ("sorted_keys", C.c_uint64), ("local_entries", C.c_uint64)]
+                ("sorted_keys", C.c_uint64), ("local_entries", C.c_uint64),
+                ("sorted_rows", C.c_int), ("pad2", C.c_int)]
 
 
 _bound = False

@@ -215,6 +215,10 @@ typedef struct {
     double ms_bounds, ms_local, ms_pairs, ms_sort, ms_ghosts, ms_merge, ms_total;
     uint64_t sorted_keys;   /* boundary keys the radix sort ordered         */
     uint64_t local_entries; /* entries of the partitions' local subgraphs   */
+    int sorted_rows;        /* 1: the boundary pairs came from the sorted-row
+                             * passes (rows strictly ascending), 0: from the
+                             * gather pass                                  */
+    int pad2;
 } ccgpu_dist_stats;
 
 void ccgpu_dist_opts_default(ccgpu_dist_opts *opts);

@@ -101,6 +101,57 @@ def test_rmat_partition_widths(torch, parts):
         check_against_oracle(torch, rp, col, parts, 1, interval)
 
 
+def test_unaligned_columns(torch):
+    """A column array that starts 4 bytes past a 16-byte boundary takes the
+    scalar column loads and gives the same labels and counts."""
+    rp, col = graphs.rmat_csr(13, 16, seed=77)
+    n, m = len(rp) - 1, len(col)
+    d_rp = torch.from_numpy(rp.astype(np.int64)).cuda()
+    buf = torch.zeros(m + 4, dtype=torch.int32, device="cuda")
+    buf[1:m + 1] = torch.from_numpy(col.astype(np.int32)).cuda()
+    d_col = buf[1:m + 1]
+    assert d_col.data_ptr() % 16 == 4
+    lab = torch.empty(n, dtype=torch.int32, device="cuda")
+    st, bounds = dist.dist_cc_device(d_rp, d_col, n, m, 4, 1, 2048, 1, d_labels=lab)
+    want, obounds, ost = oracle.dist_cc(rp, col, 4, 1, 1)
+    assert (lab.cpu().numpy().view(np.uint32) == want).all()
+    assert (bounds == obounds).all()
+    assert st.boundary_raw == ost.boundary_raw and st.pair_count == ost.pair_count
+    assert st.rounds == ost.rounds and st.sent_pairs == ost.sent_pairs
+
+
+def test_sorted_row_mode_and_its_fallback(torch):
+    """Strictly ascending rows take the sorted-row boundary passes; the same
+    graph with its rows shuffled, or with a duplicated (mirrored) entry,
+    falls back to the gather pass.  Every variant matches the oracle."""
+    rp, col = graphs.rmat_csr(12, 16, seed=91)
+    st = check_against_oracle(torch, rp, col, 4, 1, 1)
+    assert st.sorted_rows == 1
+    rng = np.random.default_rng(3)
+    shuffled = col.copy()
+    for v in range(len(rp) - 1):
+        a, b = int(rp[v]), int(rp[v + 1])
+        shuffled[a:b] = rng.permutation(shuffled[a:b])
+    st = check_against_oracle(torch, rp, shuffled, 4, 1, 1)
+    assert st.sorted_rows == 0
+    # duplicate the first cut edge found (both directions): rows stay
+    # ascending but not strictly
+    n = len(rp) - 1
+    bounds = np.array(oracle.weighted_bounds(rp, 4), dtype=np.int64)
+    part = np.searchsorted(bounds, np.arange(n), side="right") - 1
+    src = np.repeat(np.arange(n), np.diff(rp.astype(np.int64)))
+    cut = np.nonzero(part[src] != part[col])[0][0]
+    u, v = int(src[cut]), int(col[cut])
+    rows = [list(col[int(rp[x]):int(rp[x + 1])]) for x in range(n)]
+    for a, b in ((u, v), (v, u)):
+        rows[a].insert(rows[a].index(b), b)
+    rp2 = np.zeros(n + 1, np.uint64)
+    rp2[1:] = np.cumsum([len(r) for r in rows])
+    col2 = np.array([x for r in rows for x in r], np.uint32)
+    st = check_against_oracle(torch, rp2, col2, 4, 1, 1)
+    assert st.sorted_rows == 0
+
+
 def test_bounds_match_reference_restatement(torch):
     rp, col = graphs.rmat_csr(12, 8, seed=6)
     d_rp, _ = dev(torch, rp, col)
