@@ -277,25 +277,158 @@ __device__ __forceinline__ void mask_or(uint32_t *w, uint32_t bits)
 #define HP(i) ((i) + 4 * ((i) >> 5))
 constexpr int kHeadWords = kTile + 4 * (kTile / 32);
 
+/* Sorted-row mode, remote end: one warp per tile of kWarpTile entries (16
+ * per lane), with no block barriers.  Row starts are marked in the warp's
+ * slice of shared memory (stale marks from the warp's earlier tiles name
+ * earlier rows and never raise the max-scan) and a warp max-scan gives
+ * each entry its row.  Rows ascend, so along a row the entries' partition
+ * is stepped forward against the next bound (entries >= n are clamped to
+ * n, which steps to partition P: none); cutm has bit p set for every valid
+ * partition other than the row's.  An unmarked cut entry sets bit pv in
+ * the row's mask (marked ones had their keys written by the local end,
+ * k_ng_*); a row that is not strictly ascending sets *bad. */
+constexpr int kWarpTile = 32 * kTileE;
+constexpr int kWarpHead = kWarpTile + 4 * (kWarpTile / 32);
+
+template <int PMAX>
+__global__ void __launch_bounds__(kB) k_emit_sorted(EmitParams E, const uint32_t *wt_first,
+                                                    uint64_t wtiles)
+{
+    __shared__ __align__(16) uint32_t s_head[kW][kWarpHead];
+    __shared__ uint32_t s_b[CCGPU_MAX_PARTS + 2]; /* bounds, then ~0 */
+    for (int i = threadIdx.x; i < CCGPU_MAX_PARTS + 2; i += kB)
+        s_b[i] = i <= E.parts ? E.bounds[i] : 0xffffffffu;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t *head = s_head[warp];
+    uint4 *h4 = reinterpret_cast<uint4 *>(head);
+    for (int i = lane; i < kWarpHead / 4; i += 32)
+        h4[i] = make_uint4(0u, 0u, 0u, 0u);
+    __syncthreads();
+    uint32_t sb[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+        sb[i] = s_b[i];
+    const uint64_t allp = E.parts >= 32 ? 0xffffffffull : (1ull << E.parts) - 1;
+    const uint4 *mine = reinterpret_cast<const uint4 *>(head + HP(lane * kTileE));
+    unsigned long long raw = 0;
+    bool unsorted = false;
+    const uint64_t nwarps = (uint64_t)gridDim.x * kW;
+    for (uint64_t t = (uint64_t)blockIdx.x * kW + warp; t < wtiles; t += nwarps) {
+        const uint64_t lo = t * kWarpTile;
+        const uint32_t v0 = wt_first[t], v1 = wt_first[t + 1];
+        const uint64_t j0 = lo + (uint64_t)lane * kTileE;
+        uint32_t c[kTileE];
+        if (E.vec && j0 + kTileE <= E.m) {
+            const uint4 *c4 = reinterpret_cast<const uint4 *>(E.col + j0);
+#pragma unroll
+            for (int q = 0; q < kTileE / 4; ++q) {
+                const uint4 x = __ldg(c4 + q);
+                c[4 * q] = x.x;
+                c[4 * q + 1] = x.y;
+                c[4 * q + 2] = x.z;
+                c[4 * q + 3] = x.w;
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < kTileE; ++k)
+                c[k] = j0 + k < E.m ? __ldg(E.col + j0 + k) : 0xffffffffu;
+        }
+        /* marks of the 16 entries (j0 is a multiple of 16) */
+        const uint32_t ng = j0 < E.m ? __ldg(E.ngbits + (j0 >> 5)) >> (j0 & 31) : 0u;
+        const int kv = j0 >= E.m ? 0 : (E.m - j0 < kTileE ? (int)(E.m - j0) : kTileE);
+        __syncwarp(); /* the previous tile's reads of the slice are done */
+        if (lane == 0)
+            head[0] = v0 > 0 ? v0 - 1 : 0u; /* no row in [v0, v1) starts at 0 */
+        for (uint64_t v = (uint64_t)v0 + lane; v < v1 && v < E.n; v += 32) {
+            const uint64_t rp = __ldg(E.row_ptr + v);
+            if (rp >= lo && rp < lo + kWarpTile)
+                atomicMax(head + HP(rp - lo), (uint32_t)v);
+        }
+        __syncwarp();
+        uint32_t run = 0;
+#pragma unroll
+        for (int q = 0; q < kTileE / 4; ++q) {
+            const uint4 x = mine[q];
+            run = max(max(run, max(x.x, x.y)), max(x.z, x.w));
+        }
+        uint32_t incl = run;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o)
+                incl = y > incl ? y : incl;
+        }
+        uint32_t before = __shfl_up_sync(0xffffffffu, incl, 1);
+        uint32_t prev = __shfl_up_sync(0xffffffffu, c[kTileE - 1], 1);
+        uint32_t row = before; /* the row of entry j0 - 1 (lane 0: ~0 or the tile's first row) */
+        if (lane == 0) {
+            before = 0;
+            row = 0xffffffffu;
+            if (lo > 0 && v0 > 0 && __ldg(E.row_ptr + v0 - 1) < lo) {
+                row = v0 - 1; /* the tile's first row began in an earlier tile */
+                prev = __ldg(E.col + lo - 1);
+            }
+        }
+        uint32_t bits = 0, rawc = 0, cur = before;
+        int pu = row < E.n ? part_fast<PMAX>(s_b, sb, E.parts, row) : -1;
+        uint64_t cutm = pu >= 0 ? allp & ~(1ull << pu) : 0ull;
+        uint32_t v = c[0] < E.n ? c[0] : E.n;
+        int pv = part_fast<PMAX>(s_b, sb, E.parts, v < E.n ? v : E.n - 1);
+        uint32_t nb = s_b[pv + 1];
+#pragma unroll
+        for (int q = 0; q < kTileE / 4; ++q) {
+            const uint4 x = mine[q];
+            const uint32_t hs[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int k = 4 * q + e;
+                cur = hs[e] > cur ? hs[e] : cur;
+                v = c[k] < E.n ? c[k] : E.n;
+                if (cur != row) {
+                    if (bits)
+                        mask_or(E.pmask + row, bits);
+                    bits = 0;
+                    row = cur;
+                    pu = row < E.n ? part_fast<PMAX>(s_b, sb, E.parts, row) : -1;
+                    cutm = pu >= 0 ? allp & ~(1ull << pu) : 0ull;
+                    pv = part_fast<PMAX>(s_b, sb, E.parts, v < E.n ? v : E.n - 1);
+                    nb = s_b[pv + 1];
+                } else {
+                    unsorted |= c[k] <= prev && k < kv;
+                }
+                while (v >= nb) {
+                    ++pv;
+                    nb = s_b[pv + 1];
+                }
+                prev = c[k];
+                const uint32_t cut = (uint32_t)(cutm >> pv) & 1u;
+                rawc += cut;
+                bits |= (cut & ~(ng >> k)) << (pv & 31);
+            }
+        }
+        if (bits)
+            mask_or(E.pmask + row, bits);
+        raw += rawc;
+    }
+    if (unsorted)
+        *E.bad = 1ull;
+    add_raw(E, raw, lane);
+}
+
 /* Boundary pairs from the remote end over one column tile per block
- * iteration.  SORTED (sorted-row mode): rows ascend, so along a row the
- * entries' partition is stepped forward against the next bound; an
- * unmarked cut entry sets bit pv in the row's mask (marked ones had their
- * keys written by the local end, k_ng_*), and a row that is not strictly
- * ascending sets *bad.  Otherwise each cut entry gathers its giant flag and
- * non-giant ones emit their key here. */
-template <int PMAX, bool SORTED>
+ * iteration (the gather pass, used when rows are not strictly ascending or
+ * the giant masks are off): each cut entry gathers its giant flag; giant
+ * ones set bit pv in the row's mask, the others emit their key. */
+template <int PMAX>
 __global__ void __launch_bounds__(kB, 4) k_emit(EmitParams E)
 {
     __shared__ uint64_t s_keys[kKeyBuf];
     __shared__ __align__(16) uint32_t s_head[kHeadWords];
-    __shared__ uint32_t s_b[CCGPU_MAX_PARTS + 2]; /* bounds, then ~0 */
+    __shared__ uint32_t s_b[CCGPU_MAX_PARTS + 1];
     __shared__ uint32_t s_w[kW];
-    __shared__ uint32_t s_last[kW]; /* each warp's last entry */
     __shared__ uint32_t s_kcnt;
     __shared__ unsigned long long s_kbase;
-    for (int i = threadIdx.x; i < CCGPU_MAX_PARTS + 2; i += kB)
-        s_b[i] = i <= E.parts ? E.bounds[i] : 0xffffffffu;
+    for (int i = threadIdx.x; i <= E.parts; i += kB)
+        s_b[i] = E.bounds[i];
     if (threadIdx.x == 0)
         s_kcnt = 0;
     /* Row-start marks are not cleared between tiles: a block's tiles come
@@ -310,12 +443,10 @@ __global__ void __launch_bounds__(kB, 4) k_emit(EmitParams E)
     uint32_t sb[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i)
-        sb[i] = s_b[i];
-    const uint64_t allp = E.parts >= 32 ? 0xffffffffull : (1ull << E.parts) - 1;
+        sb[i] = i <= E.parts ? s_b[i] : 0xffffffffu;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const KeyBuf kbuf = {s_keys, &s_kcnt, &s_kbase};
     const uint4 *mine = reinterpret_cast<const uint4 *>(s_head + HP(threadIdx.x * kTileE));
-    bool unsorted = false;
     for (uint64_t t = blockIdx.x; t < E.tiles; t += gridDim.x) {
         const uint64_t lo = t * kTile;
         const uint32_t v0 = E.tile_first[t], v1 = E.tile_first[t + 1];
@@ -337,9 +468,6 @@ __global__ void __launch_bounds__(kB, 4) k_emit(EmitParams E)
             for (int k = 0; k < kTileE; ++k)
                 c[k] = j0 + k < E.m ? __ldg(E.col + j0 + k) : 0xffffffffu;
         }
-        /* sorted-row mode: marks of the 16 entries (j0 is a multiple of 16) */
-        const uint32_t ng = SORTED && j0 < E.m ? __ldg(E.ngbits + (j0 >> 5)) >> (j0 & 31) : 0u;
-        const int kv = j0 >= E.m ? 0 : (E.m - j0 < kTileE ? (int)(E.m - j0) : kTileE);
         /* position 0 holds the row of the tile's first entry; no row in
          * [v0, v1) starts there */
         if (threadIdx.x == 0)
@@ -363,10 +491,8 @@ __global__ void __launch_bounds__(kB, 4) k_emit(EmitParams E)
             if (lane >= o)
                 incl = y > incl ? y : incl;
         }
-        if (lane == 31) {
+        if (lane == 31)
             s_w[warp] = incl;
-            s_last[warp] = c[kTileE - 1];
-        }
         __syncthreads();
         uint32_t pre = 0;
         for (int k = 0; k < warp; ++k)
@@ -375,87 +501,35 @@ __global__ void __launch_bounds__(kB, 4) k_emit(EmitParams E)
         if (lane == 0)
             before = 0;
         before = before > pre ? before : pre; /* max over earlier threads */
-        /* the row of the entry before j0 (none: ~0), and that entry */
-        uint32_t prow = before, prev = __shfl_up_sync(0xffffffffu, c[kTileE - 1], 1);
-        if (lane == 0)
-            prev = warp > 0 ? s_last[warp - 1] : 0u;
-        if (threadIdx.x == 0) {
-            prow = 0xffffffffu;
-            if (SORTED && lo > 0 && v0 > 0 && __ldg(E.row_ptr + v0 - 1) < lo) {
-                prow = v0 - 1; /* the tile's first row began in an earlier tile */
-                prev = __ldg(E.col + lo - 1);
-            }
-        }
-        uint32_t row = prow, bits = 0, rawc = 0;
-        int pu = row < E.n ? part_fast<PMAX>(s_b, sb, E.parts, row) : -1;
+        uint32_t row = 0xffffffffu, bits = 0, rawc = 0;
+        int pu = -1;
         uint32_t cur = before; /* running max of the row starts: the row of entry k */
-        if (SORTED) {
-            /* Entries >= n are clamped to n, which steps to partition P
-             * (none).  cutm: bit p set when p is a valid partition other
-             * than the row's. */
-            uint64_t cutm = pu >= 0 ? allp & ~(1ull << pu) : 0ull;
-            uint32_t v = c[0] < E.n ? c[0] : E.n;
-            int pv = part_fast<PMAX>(s_b, sb, E.parts, v < E.n ? v : E.n - 1);
-            uint32_t nb = s_b[pv + 1];
 #pragma unroll
-            for (int q = 0; q < kTileE / 4; ++q) {
-                const uint4 x = mine[q];
-                const uint32_t hs[4] = {x.x, x.y, x.z, x.w};
+        for (int q = 0; q < kTileE / 4; ++q) {
+            const uint4 x = mine[q];
+            const uint32_t hs[4] = {x.x, x.y, x.z, x.w};
 #pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                    const int k = 4 * q + e;
-                    cur = hs[e] > cur ? hs[e] : cur;
-                    v = c[k] < E.n ? c[k] : E.n;
-                    if (cur != row) {
-                        if (bits)
-                            mask_or(E.pmask + row, bits);
-                        bits = 0;
-                        row = cur;
-                        pu = row < E.n ? part_fast<PMAX>(s_b, sb, E.parts, row) : -1;
-                        cutm = pu >= 0 ? allp & ~(1ull << pu) : 0ull;
-                        pv = part_fast<PMAX>(s_b, sb, E.parts, v < E.n ? v : E.n - 1);
-                        nb = s_b[pv + 1];
-                    } else {
-                        unsorted |= c[k] <= prev && k < kv;
-                    }
-                    while (v >= nb) {
-                        ++pv;
-                        nb = s_b[pv + 1];
-                    }
-                    prev = c[k];
-                    const uint32_t cut = (uint32_t)(cutm >> pv) & 1u;
-                    rawc += cut;
-                    bits |= (cut & ~(ng >> k)) << (pv & 31);
+            for (int e = 0; e < 4; ++e) {
+                const int k = 4 * q + e;
+                cur = hs[e] > cur ? hs[e] : cur;
+                const uint32_t v = c[k];
+                if (cur != row) {
+                    if (bits)
+                        mask_or(E.pmask + row, bits);
+                    bits = 0;
+                    row = cur;
+                    pu = row < E.n ? part_fast<PMAX>(s_b, sb, E.parts, row) : -1;
                 }
-            }
-        } else {
-#pragma unroll
-            for (int q = 0; q < kTileE / 4; ++q) {
-                const uint4 x = mine[q];
-                const uint32_t hs[4] = {x.x, x.y, x.z, x.w};
-#pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                    const int k = 4 * q + e;
-                    cur = hs[e] > cur ? hs[e] : cur;
-                    const uint32_t v = c[k];
-                    if (cur != row) {
-                        if (bits)
-                            mask_or(E.pmask + row, bits);
-                        bits = 0;
-                        row = cur;
-                        pu = row < E.n ? part_fast<PMAX>(s_b, sb, E.parts, row) : -1;
-                    }
-                    const int pv = part_fast<PMAX>(s_b, sb, E.parts, v);
-                    if (pv != pu && v < E.n && pu >= 0) { /* a cut edge */
-                        ++rawc;
-                        bool gnt = false;
-                        if (E.gflag)
-                            gnt = (__ldg(E.gflag + (v >> 5)) >> (v & 31)) & 1u;
-                        if (gnt)
-                            bits |= 1u << pv;
-                        else
-                            kb_put(kbuf, E, make_key(E, pv, row, __ldg(E.label + v) - s_b[pv]));
-                    }
+                const int pv = part_fast<PMAX>(s_b, sb, E.parts, v);
+                if (pv != pu && v < E.n && pu >= 0) { /* a cut edge */
+                    ++rawc;
+                    bool gnt = false;
+                    if (E.gflag)
+                        gnt = (__ldg(E.gflag + (v >> 5)) >> (v & 31)) & 1u;
+                    if (gnt)
+                        bits |= 1u << pv;
+                    else
+                        kb_put(kbuf, E, make_key(E, pv, row, __ldg(E.label + v) - s_b[pv]));
                 }
             }
         }
@@ -467,8 +541,6 @@ __global__ void __launch_bounds__(kB, 4) k_emit(EmitParams E)
         if (kc >= kKeyBuf / 2)
             kb_flush(kbuf, E, kc);
     }
-    if (unsorted)
-        *E.bad = 1ull;
     __syncthreads();
     const uint32_t kc = s_kcnt;
     if (kc)
@@ -788,23 +860,24 @@ struct LocalParams {
     int vec;                    /* col is 16-byte aligned: 16-byte loads */
 };
 
-/* tile_first[t] = smallest v with row_ptr[v] > t * kTile (v in [0, n]),
- * tile_first[tiles] = n + 1. */
-__global__ void __launch_bounds__(kB) k_tile_first(LocalParams L)
+/* first[t] = smallest v with row_ptr[v] > t * width (v in [0, n]),
+ * first[tiles] = n + 1. */
+__global__ void __launch_bounds__(kB) k_tile_first(LocalParams L, uint64_t width,
+                                                   uint64_t tiles, uint32_t *first)
 {
     const uint64_t stride = (uint64_t)gridDim.x * kB;
     for (uint64_t v = (uint64_t)blockIdx.x * kB + threadIdx.x; v <= L.n; v += stride) {
         if (v == 0) {
             /* tiles before the first row or after the last one hold no row
              * start (only for a row_ptr that does not span [0, m]) */
-            L.tile_first[L.tiles] = L.n + 1;
+            first[tiles] = L.n + 1;
             uint64_t r0 = __ldg(L.row_ptr), rn = __ldg(L.row_ptr + L.n);
             r0 = r0 > L.m ? L.m : r0;
             rn = rn > L.m ? L.m : rn;
-            for (uint64_t t = 0; t * kTile < r0; ++t)
-                L.tile_first[t] = 0;
-            for (uint64_t t = (rn + kTile - 1) / kTile; t < L.tiles; ++t)
-                L.tile_first[t] = L.n + 1;
+            for (uint64_t t = 0; t * width < r0; ++t)
+                first[t] = 0;
+            for (uint64_t t = (rn + width - 1) / width; t < tiles; ++t)
+                first[t] = L.n + 1;
             continue;
         }
         uint64_t a = __ldg(L.row_ptr + v - 1), b = __ldg(L.row_ptr + v);
@@ -812,9 +885,9 @@ __global__ void __launch_bounds__(kB) k_tile_first(LocalParams L)
             b = L.m;
         if (a > b)
             a = b;
-        /* tiles whose first entry t*kTile lies in [a, b) */
-        for (uint64_t t = (a + kTile - 1) / kTile; t * kTile < b; ++t)
-            L.tile_first[t] = (uint32_t)v;
+        /* tiles whose first entry t*width lies in [a, b) */
+        for (uint64_t t = (a + width - 1) / width; t * width < b; ++t)
+            first[t] = (uint32_t)v;
     }
 }
 
@@ -1657,8 +1730,8 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
     const uint64_t *l_rp = d_row_ptr;
     const uint32_t *l_col = d_col;
     uint64_t l_m = m;
-    uint32_t *tile_first = nullptr;
-    uint64_t col_tiles = 0;
+    uint32_t *tile_first = nullptr, *wt_first = nullptr;
+    uint64_t col_tiles = 0, wtiles = 0;
     if (P > 1 && m > 0) {
         LocalParams Lp;
         Lp.row_ptr = d_row_ptr;
@@ -1681,8 +1754,13 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
         Lp.lcol = nullptr;
         const unsigned tb = cc_blocks(Lp.tiles, 1, (unsigned)ctx->sm_count * 8);
         CC_KLAUNCH(ctx, CCK_DIST_LOCAL_COUNT, k_local_count, tb, kB, 0, st, Lp);
-        CC_KLAUNCH(ctx, CCK_DIST_TILES, k_tile_first,
-                   cc_blocks((uint64_t)n + 1, kB, (unsigned)ctx->sm_count * 8), kB, 0, st, Lp);
+        const unsigned vb = cc_blocks((uint64_t)n + 1, kB, (unsigned)ctx->sm_count * 8);
+        CC_KLAUNCH(ctx, CCK_DIST_TILES, k_tile_first, vb, kB, 0, st, Lp, (uint64_t)kTile, Lp.tiles,
+                   Lp.tile_first);
+        wtiles = (m + kWarpTile - 1) / kWarpTile;
+        CC_TRY(cc_bufs_get(&B, (void **)&wt_first, (wtiles + 1) * sizeof(uint32_t)));
+        CC_KLAUNCH(ctx, CCK_DIST_TILES, k_tile_first, vb, kB, 0, st, Lp, (uint64_t)kWarpTile,
+                   wtiles, wt_first);
         CC_TRY(cc_scan_u32(ctx, Lp.tile_cnt, tile_off, Lp.tiles, &B, st));
         CC_CUDA(cudaMemcpyAsync(&l_m, tile_off + Lp.tiles, sizeof(uint64_t),
                                 cudaMemcpyDeviceToHost, st));
@@ -1797,19 +1875,23 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
             CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_mark, lb, kB, 0, st, E, work, off + n);
             CC_CUDA(cudaMemcpyAsync(E.count, off + n, sizeof(unsigned long long),
                                     cudaMemcpyDeviceToDevice, st));
+            const unsigned wb = cc_blocks(wtiles, kW, (unsigned)ctx->sm_count * 8);
             if (P <= 4)
-                CC_KLAUNCH(ctx, CCK_DIST_PAIRS, (k_emit<4, true>), eb, kB, 0, st, E);
+                CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit_sorted<4>, wb, kB, 0, st, E, wt_first,
+                           wtiles);
             else if (P <= 8)
-                CC_KLAUNCH(ctx, CCK_DIST_PAIRS, (k_emit<8, true>), eb, kB, 0, st, E);
+                CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit_sorted<8>, wb, kB, 0, st, E, wt_first,
+                           wtiles);
             else
-                CC_KLAUNCH(ctx, CCK_DIST_PAIRS, (k_emit<CCGPU_MAX_PARTS, true>), eb, kB, 0, st, E);
+                CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit_sorted<CCGPU_MAX_PARTS>, wb, kB, 0, st, E,
+                           wt_first, wtiles);
         } else {
             if (P <= 4)
-                CC_KLAUNCH(ctx, CCK_DIST_PAIRS, (k_emit<4, false>), eb, kB, 0, st, E);
+                CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit<4>, eb, kB, 0, st, E);
             else if (P <= 8)
-                CC_KLAUNCH(ctx, CCK_DIST_PAIRS, (k_emit<8, false>), eb, kB, 0, st, E);
+                CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit<8>, eb, kB, 0, st, E);
             else
-                CC_KLAUNCH(ctx, CCK_DIST_PAIRS, (k_emit<CCGPU_MAX_PARTS, false>), eb, kB, 0, st,
+                CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit<CCGPU_MAX_PARTS>, eb, kB, 0, st,
                            E);
         }
         return CCGPU_OK;
