@@ -357,7 +357,10 @@ int ccgpu_batch_plan_class_graphs(const ccgpu_batch_plan *p, uint32_t *counts);
 int ccgpu_batch_plan_results(ccgpu_batch_plan *p, uint32_t *h_components, uint32_t *h_done,
                              void *stream);
 void ccgpu_batch_plan_destroy(ccgpu_batch_plan *p);
-/* One-shot: plan, solve, per-graph component counts (may be NULL), destroy. */
+/* One-shot: plan, solve, per-graph component counts (may be NULL).  The
+ * context keeps the plan (and its device arrays, which only grow) for its
+ * next call, and frees it in ccgpu_ctx_destroy; a context serves one host
+ * thread at a time.  Synchronous on `stream`. */
 int ccgpu_batch_cc(ccgpu_ctx *ctx, const ccgpu_batch *b, const ccgpu_batch_tuning *tuning,
                    uint32_t *h_components, void *stream);
 
