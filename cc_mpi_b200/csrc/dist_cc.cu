@@ -927,20 +927,31 @@ __device__ __forceinline__ uint32_t tile_keep(const LocalParams &L, const uint32
         for (int k = 0; k < kTileE; ++k)
             u[k] = j0 + k < L.m ? __ldg(L.col + j0 + k) : 0u;
     }
-    int p = j0 < L.m ? part_at(s_pcol, L.parts, j0) : 0;
+    if (j0 >= L.m)
+        return 0u;
+    const int kn = L.m - j0 < kTileE ? (int)(L.m - j0) : kTileE; /* entries before m */
+    /* The partition of entry k is p until entry kc, where the next
+     * partition's columns begin (rare inside 16 entries); its vertex range
+     * [lo_b, hi_b) stays in registers. */
+    int p = part_at(s_pcol, L.parts, j0);
     uint64_t pend = s_pcol[p + 1];
+    int kc = pend <= j0 || pend - j0 >= kTileE ? kTileE : (int)(pend - j0);
+    uint32_t lo_b = s_b[p], hi_b = s_b[p + 1];
     uint32_t mask = 0;
 #pragma unroll
     for (int k = 0; k < kTileE; ++k) {
-        const uint64_t j = j0 + k;
-        if (j >= L.m)
-            break;
-        while (j >= pend && p < L.parts - 1) { /* crossed into the next partition */
-            ++p;
-            pend = s_pcol[p + 1];
+        if (k == kc) {
+            const uint64_t j = j0 + k;
+            while (j >= pend && p < L.parts - 1) {
+                ++p;
+                pend = s_pcol[p + 1];
+            }
+            kc = pend <= j || pend - j0 >= kTileE ? kTileE : (int)(pend - j0);
+            lo_b = s_b[p];
+            hi_b = s_b[p + 1];
         }
-        if (u[k] >= s_b[p] && u[k] < s_b[p + 1])
-            mask |= 1u << k;
+        const bool keep = k < kn && u[k] - lo_b < hi_b - lo_b; /* lo_b <= u < hi_b */
+        mask |= (uint32_t)keep << k;
     }
     return mask;
 }
