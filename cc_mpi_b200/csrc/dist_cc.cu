@@ -286,7 +286,8 @@ constexpr int kHeadWords = kTile + 4 * (kTile / 32);
  * n, which steps to partition P: none); cutm has bit p set for every valid
  * partition other than the row's.  An unmarked cut entry sets bit pv in
  * the row's mask (marked ones had their keys written by the local end,
- * k_ng_*); a row that is not strictly ascending sets *bad. */
+ * k_ng_*); a row that is not strictly ascending sets *bad.  Runs with
+ * fewer than 32 partitions, so partition masks and shifts fit 32 bits. */
 constexpr int kWarpTile = 32 * kTileE;
 constexpr int kWarpHead = kWarpTile + 4 * (kWarpTile / 32);
 
@@ -308,7 +309,7 @@ __global__ void __launch_bounds__(kB) k_emit_sorted(EmitParams E, const uint32_t
 #pragma unroll
     for (int i = 0; i < 8; ++i)
         sb[i] = s_b[i];
-    const uint64_t allp = E.parts >= 32 ? 0xffffffffull : (1ull << E.parts) - 1;
+    const uint32_t allp = (1u << E.parts) - 1u; /* sorted-row mode: parts < 32 */
     const uint4 *mine = reinterpret_cast<const uint4 *>(head + HP(lane * kTileE));
     unsigned long long raw = 0;
     bool unsorted = false;
@@ -370,7 +371,7 @@ __global__ void __launch_bounds__(kB) k_emit_sorted(EmitParams E, const uint32_t
         }
         uint32_t bits = 0, rawc = 0, cur = before;
         int pu = row < E.n ? part_fast<PMAX>(s_b, sb, E.parts, row) : -1;
-        uint64_t cutm = pu >= 0 ? allp & ~(1ull << pu) : 0ull;
+        uint32_t cutm = pu >= 0 ? allp & ~(1u << pu) : 0u;
         uint32_t v = c[0] < E.n ? c[0] : E.n;
         int pv = part_fast<PMAX>(s_b, sb, E.parts, v < E.n ? v : E.n - 1);
         uint32_t nb = s_b[pv + 1];
@@ -389,7 +390,7 @@ __global__ void __launch_bounds__(kB) k_emit_sorted(EmitParams E, const uint32_t
                     bits = 0;
                     row = cur;
                     pu = row < E.n ? part_fast<PMAX>(s_b, sb, E.parts, row) : -1;
-                    cutm = pu >= 0 ? allp & ~(1ull << pu) : 0ull;
+                    cutm = pu >= 0 ? allp & ~(1u << pu) : 0u;
                     pv = part_fast<PMAX>(s_b, sb, E.parts, v < E.n ? v : E.n - 1);
                     nb = s_b[pv + 1];
                 } else {
@@ -400,9 +401,9 @@ __global__ void __launch_bounds__(kB) k_emit_sorted(EmitParams E, const uint32_t
                     nb = s_b[pv + 1];
                 }
                 prev = c[k];
-                const uint32_t cut = (uint32_t)(cutm >> pv) & 1u;
+                const uint32_t cut = (cutm >> pv) & 1u; /* pv <= parts < 32 */
                 rawc += cut;
-                bits |= (cut & ~(ng >> k)) << (pv & 31);
+                bits |= (cut & ~(ng >> k)) << pv;
             }
         }
         if (bits)
@@ -1855,7 +1856,7 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
      * gather pass alone. */
     E.ngbits = nullptr;
     E.bad = counters + 6;
-    const bool sorted_mode = use_mask && P > 1 && col_tiles > 0;
+    const bool sorted_mode = use_mask && P > 1 && P < 32 && col_tiles > 0;
     auto emit = [&]() -> int {
         const unsigned eb = cc_blocks(col_tiles, 1, (unsigned)ctx->sm_count * 4);
         const unsigned lb = cc_blocks(n, kB, (unsigned)ctx->sm_count * 8);
