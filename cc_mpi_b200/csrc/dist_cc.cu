@@ -1212,6 +1212,11 @@ __global__ void __launch_bounds__(kB) k_dedup_count(DedupParams D)
     }
 }
 
+/* Writes pairs and ghosts with coalesced stores: warp w walks tile
+ * positions [w * 512, (w + 1) * 512) 32 consecutive keys per step, and a
+ * step's new pairs (and new ghosts) go to consecutive slots found by
+ * ballots.  A first sweep counts each warp's pairs and ghosts for the
+ * block's offsets. */
 __global__ void __launch_bounds__(kB) k_dedup_write(DedupParams D)
 {
     __shared__ uint64_t s_keys[kDedupSmem];
@@ -1222,49 +1227,60 @@ __global__ void __launch_bounds__(kB) k_dedup_write(DedupParams D)
         s_b[i] = D.bounds[i];
     dedup_stage(D, s_keys, &s_prev);
     const uint64_t tile = (uint64_t)blockIdx.x * kDedupTile;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int wbase = warp * 32 * kDedupItems;
     uint32_t cu = 0, cg = 0;
     for (int j = 0; j < kDedupItems; ++j) {
-        int li = threadIdx.x * kDedupItems + j;
+        const int li = wbase + j * 32 + lane;
+        bool u = false, g = false;
         if (tile + li < D.count) {
             uint64_t k;
-            bool u, g;
             dedup_flags(D, s_keys, s_prev, li, tile + li, k, u, g);
-            cu += u;
-            cg += g;
         }
+        cu += __popc(__ballot_sync(0xffffffffu, u));
+        cg += __popc(__ballot_sync(0xffffffffu, g));
     }
-    uint32_t iu = cc_block_incl_scan256<uint32_t>(cu, s_wu, nullptr);
-    uint32_t ig = cc_block_incl_scan256<uint32_t>(cg, s_wg, nullptr);
-    uint64_t up = D.u_off[blockIdx.x] + iu - cu; /* first unique index of this thread */
-    uint64_t gp = D.g_off[blockIdx.x] + ig - cg; /* ghosts started before this thread */
+    if (lane == 0) {
+        s_wu[warp] = cu;
+        s_wg[warp] = cg;
+    }
+    __syncthreads();
+    uint64_t up = D.u_off[blockIdx.x], gp = D.g_off[blockIdx.x]; /* before this warp */
+    for (int w = 0; w < warp; ++w) {
+        up += s_wu[w];
+        gp += s_wg[w];
+    }
     const uint64_t pmask = (1ull << D.gb) - 1ull;
     const uint64_t rmask = (1ull << D.rb) - 1ull;
     const int pshift = D.rb + D.gb;
+    const uint32_t lt = (1u << lane) - 1u, le = (lt << 1) | 1u;
     for (int j = 0; j < kDedupItems; ++j) {
-        int li = threadIdx.x * kDedupItems + j;
-        uint64_t gi = tile + li;
-        if (gi >= D.count)
-            break;
-        uint64_t k;
-        bool u, g;
-        dedup_flags(D, s_keys, s_prev, li, gi, k, u, g);
+        const int li = wbase + j * 32 + lane;
+        const uint64_t gi = tile + li;
+        uint64_t k = 0;
+        bool u = false, g = false;
+        if (gi < D.count)
+            dedup_flags(D, s_keys, s_prev, li, gi, k, u, g);
+        const uint32_t bu = __ballot_sync(0xffffffffu, u), bg = __ballot_sync(0xffffffffu, g);
         const int p = (int)(k >> pshift);
         if (g) {
-            uint32_t remote = (uint32_t)((k >> D.rb) & pmask);
-            uint64_t prev = gi == 0 ? ~0ull : (li > 0 ? s_keys[DD_PAD(li - 1)] : s_prev);
+            const uint64_t my = gp + __popc(bg & lt);
+            const uint32_t remote = (uint32_t)((k >> D.rb) & pmask);
+            const uint64_t prev = gi == 0 ? ~0ull : (li > 0 ? s_keys[DD_PAD(li - 1)] : s_prev);
             if (gi == 0 || (int)(prev >> pshift) != p)
-                D.gh_first[p] = gp; /* first ghost of partition p */
-            D.ghost_v[gp] = remote;
-            D.ghost_pairs[gp] = up;
-            D.ghost_labels[gp] = remote;   /* src/cc_mpi.c:456-457 */
-            D.prev_sent[gp] = 0xffffffffu; /* src/cc_mpi.c:480-487 */
-            gp++;
+                D.gh_first[p] = my; /* first ghost of partition p */
+            D.ghost_v[my] = remote;
+            D.ghost_pairs[my] = up + __popc(bu & lt);
+            D.ghost_labels[my] = remote;   /* src/cc_mpi.c:456-457 */
+            D.prev_sent[my] = 0xffffffffu; /* src/cc_mpi.c:480-487 */
         }
         if (u) {
-            D.pair_rep[up] = s_b[p] + (uint32_t)(k & rmask);
-            D.pair_g[up] = (uint32_t)(gp - 1);
-            up++;
+            const uint64_t my = up + __popc(bu & lt);
+            D.pair_rep[my] = s_b[p] + (uint32_t)(k & rmask);
+            D.pair_g[my] = (uint32_t)(gp + __popc(bg & le) - 1); /* the latest ghost */
         }
+        up += __popc(bu);
+        gp += __popc(bg);
     }
 }
 
