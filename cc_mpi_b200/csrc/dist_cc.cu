@@ -1094,19 +1094,12 @@ __global__ void __launch_bounds__(kB) k_reps(const uint32_t *__restrict__ label,
     }
 }
 
-/* Reps that own at least one boundary pair.  A rep without one has no hook
- * and its own label as its only jump target, so a merge round never
- * changes it (src/cc_mpi.c:575-622): the rounds walk only the others. */
-__global__ void __launch_bounds__(kB) k_mark_pair_reps(const uint32_t *__restrict__ pair_rep,
-                                                       uint64_t pairs, uint8_t *flag)
-{
-    const uint64_t stride = (uint64_t)gridDim.x * kB;
-    for (uint64_t k = (uint64_t)blockIdx.x * kB + threadIdx.x; k < pairs; k += stride)
-        flag[__ldg(pair_rep + k)] = 1;
-}
-
+/* Reps that own at least one boundary pair (their hook minimum is set).  A
+ * rep without one has no hook and its own label as its only jump target,
+ * so a merge round never changes it (src/cc_mpi.c:575-622): the rounds
+ * walk only the others. */
 __global__ void __launch_bounds__(kB) k_active_reps(const uint32_t *__restrict__ rep_list,
-                                                    uint64_t reps, const uint8_t *flag,
+                                                    uint64_t reps, const uint32_t *hook,
                                                     uint32_t *act, unsigned long long *act_count)
 {
     const int lane = threadIdx.x & 31;
@@ -1114,7 +1107,7 @@ __global__ void __launch_bounds__(kB) k_active_reps(const uint32_t *__restrict__
     for (uint64_t base = (uint64_t)blockIdx.x * kB; base < reps; base += stride) {
         const uint64_t i = base + threadIdx.x;
         const uint32_t r = i < reps ? __ldg(rep_list + i) : 0u;
-        const bool a = i < reps && flag[r];
+        const bool a = i < reps && hook[r] != 0xffffffffu;
         const unsigned mask = __ballot_sync(0xffffffffu, a);
         unsigned long long slot = 0;
         if (lane == 0 && mask)
@@ -2068,30 +2061,12 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
     }
 
     /* 6. merge rounds, over the reps that own boundary pairs */
-    uint32_t *act = nullptr;
-    uint64_t act_count = 0;
-    if (U > 0) {
-        uint8_t *flag = nullptr;
-        CC_TRY(cc_bufs_get(&B, (void **)&flag, (size_t)n));
-        CC_TRY(cc_bufs_get(&B, (void **)&act, (size_t)S.rep_count * sizeof(uint32_t) + 4));
-        CC_CUDA(cudaMemsetAsync(flag, 0, (size_t)n, st));
-        CC_CUDA(cudaMemsetAsync(counters + 5, 0, sizeof(unsigned long long), st));
-        const unsigned gb2 = (unsigned)ctx->sm_count * 8;
-        CC_KLAUNCH(ctx, CCK_MERGE_INIT, k_mark_pair_reps, cc_blocks(U, kB, gb2), kB, 0, st,
-                   D.pair_rep, U, flag);
-        CC_KLAUNCH(ctx, CCK_MERGE_INIT, k_active_reps, cc_blocks(S.rep_count, kB, gb2), kB, 0,
-                   st, rep_list, S.rep_count, flag, act, counters + 5);
-        unsigned long long ac = 0;
-        CC_CUDA(cudaMemcpyAsync(&ac, counters + 5, sizeof(ac), cudaMemcpyDeviceToHost, st));
-        CC_CUDA(cudaStreamSynchronize(st));
-        act_count = ac;
-    }
     MergeParams M;
     M.label = label;
     M.bounds = bounds;
     M.parts = P;
-    M.rep_list = act;
-    M.rep_count = act_count;
+    M.rep_list = nullptr;
+    M.rep_count = 0;
     M.hook = hook;
     M.pair_rep = D.pair_rep;
     M.pair_g = D.pair_g;
@@ -2111,10 +2086,24 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
     M.ghost_rep_ready = 0;
     CC_CUDA(cudaMemsetAsync(M.msg_count, 0, (size_t)P * P * sizeof(uint32_t), st));
     const unsigned gbk = (unsigned)ctx->sm_count * 8;
+    uint64_t act_count = 0;
     if (U > 0) {
+        /* hook minima first: a rep owns a pair exactly when its hook left ~0
+         * (ghost labels start as vertex ids) */
         M.cur = cur;
         M.next = nxt;
         CC_KLAUNCH(ctx, CCK_MERGE_HOOK, k_hook_init, cc_blocks(U, kB, gbk), kB, 0, st, M);
+        uint32_t *act = nullptr;
+        CC_TRY(cc_bufs_get(&B, (void **)&act, (size_t)S.rep_count * sizeof(uint32_t) + 4));
+        CC_CUDA(cudaMemsetAsync(counters + 5, 0, sizeof(unsigned long long), st));
+        CC_KLAUNCH(ctx, CCK_MERGE_INIT, k_active_reps, cc_blocks(S.rep_count, kB, gbk), kB, 0,
+                   st, rep_list, S.rep_count, hook, act, counters + 5);
+        unsigned long long ac = 0;
+        CC_CUDA(cudaMemcpyAsync(&ac, counters + 5, sizeof(ac), cudaMemcpyDeviceToHost, st));
+        CC_CUDA(cudaStreamSynchronize(st));
+        act_count = ac;
+        M.rep_list = act;
+        M.rep_count = act_count;
     }
     /* src/cc_mpi.c:538: merge only when some partition has ghosts, pairs
      * and reps; a partition with none joins the rounds and exchanges
