@@ -190,7 +190,8 @@ __device__ __forceinline__ uint64_t make_key(const EmitParams &E, int p, uint32_
  * as entry v of row u.  When v lies in p's giant tree (one bit per vertex,
  * gflag, small enough to stay in L2) the row only records partition p in a
  * mask it owns (pmask[u], one atomicOr per row segment of a thread);
- * k_mask_keys then writes one (p, u, giant rep) key per mask bit.  Every
+ * k_mask_count / k_mask_write then write one (p, u, giant rep) key per
+ * mask bit.  Every
  * other cut edge emits its key, so the sorted, deduplicated pair list is
  * the reference's. */
 
