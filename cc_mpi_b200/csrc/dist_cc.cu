@@ -191,9 +191,10 @@ __device__ __forceinline__ uint64_t make_key(const EmitParams &E, int p, uint32_
  * gflag, small enough to stay in L2) the row only records partition p in a
  * mask it owns (pmask[u], one atomicOr per row segment of a thread);
  * k_mask_count / k_mask_write then write one (p, u, giant rep) key per
- * mask bit.  Every
- * other cut edge emits its key, so the sorted, deduplicated pair list is
- * the reference's. */
+ * mask bit.  Every other cut edge emits its key, so the sorted,
+ * deduplicated pair list is the reference's.  With strictly ascending rows
+ * the giant test of each cut entry comes from mirror marks instead of gflag
+ * gathers (k_ng_* and k_emit_sorted below). */
 
 /* Giant label (global min id) of every partition, ~0 when it has none or the
  * mask path is off. */
