@@ -2,11 +2,10 @@
  * ccgpu_local_cc_noalloc: the local CC solve for callers that cannot
  * allocate device memory.
  *
- * Some callers cannot call cudaMalloc: code that runs while another library
- * holds a stream capture open (allocation calls are not capturable), serving
- * processes whose memory manager reserved the whole HBM budget up front,
- * and latency-critical loops that must not take the device-wide
- * synchronisation cudaMalloc/cudaFree imply.  This variant keeps the solve's
+ * Some callers cannot call cudaMalloc: serving processes whose memory
+ * manager reserved the whole HBM budget up front, plug-ins that must not own
+ * device memory of their own, and latency-critical loops that must not take
+ * the device-wide synchronisation cudaMalloc/cudaFree imply.  This variant keeps the solve's
  * scratch - the work counters, the giant root and the heavy-row queue - in a
  * file-scope device array of fixed size, so the caller only passes the graph
  * and the label buffer.
@@ -17,8 +16,12 @@
  * reuses the same array, which keeps the previous call's contents; the init
  * kernel clears the counters each call, everything else is written before it
  * is read.  Calls whose kernels overlap on the GPU (two streams, or two host
- * threads) share the array and race: serialise them.
+ * threads) share the array and race: serialise them.  The cached address
+ * belongs to the device's current context: after cudaDeviceReset the module
+ * may be loaded elsewhere, so the call must not be used after a reset in
+ * the same process.
  */
+#include <cstdint>
 #include <cstring>
 #include <mutex>
 
@@ -82,7 +85,7 @@ extern "C" size_t ccgpu_local_cc_noalloc_required(uint32_t n, uint64_t m,
 {
     LocalCCArgs a = {nullptr, nullptr, n, m, nullptr, nullptr, 1, {}, 0};
     if (cc_local_resolve_opts(opts, &a.o) != CCGPU_OK)
-        return 0;
+        return SIZE_MAX; /* invalid options: never fits (the error is set) */
     return required_bytes(a);
 }
 

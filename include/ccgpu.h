@@ -270,17 +270,18 @@ int ccgpu_plan_kernels(const ccgpu_plan *plan);
 void ccgpu_plan_destroy(ccgpu_plan *plan);
 
 /* ccgpu_local_cc without any device allocation.  No counterpart in the
- * reference: it exists for callers that cannot allocate device memory (code
- * running inside another library's stream capture, where allocation calls
- * are not capturable; processes whose allocator reserved all of HBM up
- * front; loops that must not take the device-wide synchronisation of
- * cudaMalloc/cudaFree).  Scratch lives in a fixed file-scope device array of
+ * reference: it exists for callers that cannot allocate device memory
+ * (processes whose allocator reserved all of HBM up front; plug-ins that
+ * must not own device memory; loops that must not take the device-wide
+ * synchronisation of cudaMalloc/cudaFree).  Scratch lives in a fixed file-scope device array of
  * ccgpu_local_cc_noalloc_capacity() bytes (1 MiB), held by every GPU that
  * loads the library until the process exits; a solve needs
  * ccgpu_local_cc_noalloc_required(n, m, opts) bytes (about 4 bytes per
  * m/heavy_degree row of the heavy queue) and larger graphs are rejected
- * with CCGPU_ERR_LIMIT.  The first call on a device looks up the array with
- * cudaGetSymbolAddress; make it before any stream capture.  Calls share the
+ * with CCGPU_ERR_LIMIT; _required returns SIZE_MAX for invalid options.
+ * The first call on a device looks up the array with cudaGetSymbolAddress
+ * and keeps the address; make it before any stream capture, and do not use
+ * the call after cudaDeviceReset in the same process.  Calls share the
  * array: calls whose kernels overlap on the GPU race.  Asynchronous on
  * `stream`; no stats. */
 int ccgpu_local_cc_noalloc(const uint64_t *d_row_ptr, const uint32_t *d_col_idx, uint32_t n,

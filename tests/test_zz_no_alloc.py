@@ -1,6 +1,6 @@
 """ccgpu_local_cc_noalloc: the local CC solve for callers that cannot allocate
-device memory (inside another library's stream capture, under an allocator
-that already reserved all of HBM, or where cudaMalloc's device-wide
+device memory (under an allocator that already reserved all of HBM, plug-ins
+that must not own device memory, or where cudaMalloc's device-wide
 synchronisation is not acceptable).  Its scratch is a fixed device array
 inside the library, so the call allocates nothing; its labels must be the
 same as the allocating entry point's, call after call.
@@ -82,3 +82,25 @@ def test_noalloc_rejects_graphs_beyond_its_scratch(L):
     assert rc == 5  # CCGPU_ERR_LIMIT
     assert b"scratch" in L.ccgpu_last_error()
     assert L.ccgpu_local_cc_noalloc_required(1 << 24, 1 << 29, None) <= cap
+    bad = _lib.opts(sample_rounds=9)  # above the limit of 8: invalid, never fits
+    assert L.ccgpu_local_cc_noalloc_required(1000, 1000, C.byref(bad)) == C.c_size_t(-1).value
+
+
+def test_noalloc_leaves_free_device_memory_unchanged(L, torch):
+    """After the first call on the device (its set-up), a call takes no
+    device memory: the free bytes the driver reports do not move."""
+    rp, col = graphs.rmat_csr(15, 16, seed=23)
+    n, m = len(rp) - 1, int(rp[-1])
+    d_rp = torch.from_numpy(rp.astype(np.int64)).cuda()
+    d_col = torch.from_numpy(col.astype(np.int32)).cuda()
+    got = torch.empty(n, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    assert noalloc(L, d_rp, d_col, n, m, got, None, stream) == 0  # set-up call
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(3):
+        assert noalloc(L, d_rp, d_col, n, m, got, None, stream) == 0, L.ccgpu_last_error()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    assert (got.cpu().numpy().view(np.uint32) == oracle.uf_labels(rp, col)).all()
