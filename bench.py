@@ -41,7 +41,10 @@ WORKLOADS = {
     "grid2048": dict(kind="grid", rows=2048, cols=2048, p=0.1),
     # partitioned path (compute_connected_components_mpi_advanced)
     "c3": dict(kind="rmat_big", scale=26, n=65_600_000, undirected=1_800_000_000, parts=4,
-               dist=True),
+               dist=True, ref_runs=1),
+    # the reference's own CPU-runnable case: R-MAT scale 18 as a .mat file,
+    # mpirun -np 2 -t 8 -c 8192 -e 1 -r 3
+    "c1": dict(kind="rmat", scale=18, ef=16, parts=2, dist=True, mat=True, ref_runs=3),
     "rmat24p4": dict(kind="rmat", scale=24, ef=16, parts=4, dist=True),
     "rmat22p4": dict(kind="rmat", scale=22, ef=16, parts=4, dist=True),
     # batched path (ccgpu_batch_*): graphs of log-uniform size, a third each
@@ -159,22 +162,53 @@ def read_peaks():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def algorithmic_bytes(torch, rp_d, n, m, k, st):
-    """Bytes each kernel must move per launch (see the roofline section of
-    the design notes): row pointers, the column entries actually read and
-    the own-label read/write; neighbour-label gathers are cache-served and
-    not counted."""
-    deg = rp_d[1:] - rp_d[:-1]
-    sampled = int(torch.clamp(deg, max=k).sum().item()) if k > 0 else 0
-    return {
-        "init": 4 * n,
-        "sample": 8 * (n + 1) + 4 * sampled + 4 * n,
-        "compress": 8 * n,
-        "giant": 4 * 1024,
-        "link_rows": 4 * n + 8 * int(st.finish_rows) + 4 * int(st.finish_edges),
-        "link_heavy": 4 * 0,
-        "final_compress": 8 * n,
-    }
+def local_cc_bytes(torch, deg, n, m, opts, finish_rows=None, finish_edges=None, row_bytes=8):
+    """Algorithmic bytes of each launch of one local CC solve, by kernel name
+    (a list when the launches of one kernel move different bytes).  Per
+    launch, what the kernel must move at least: row pointers it reads
+    (8 bytes per row), the column entries it reads (4 each), its own label
+    read and write (4 each per vertex); neighbour-label gathers are counted
+    as cache-served, so the figure is conservative.
+
+    ``deg`` is the device tensor of row lengths of the graph the local CC
+    runs on.  Sampling round r reads entry r of every row longer than r.
+    With the second-neighbour stash (sampling with min-hooks and a shortcut
+    between rounds, at least two rounds, and 8 or more entries per vertex)
+    round 0 reads entries 0 and 1 of each row and writes the stash (4n),
+    and round 1 reads only the stash (4n).  ``row_bytes``: bytes of row
+    bounds per row (8 for a CSR's row pointers, 16 for begin/end pairs)."""
+    k = opts.sample_rounds if opts.sample_rounds >= 0 else 2
+    hook = opts.hook_mode if opts.hook_mode >= 0 else 12
+    stash = (hook & 12) == 12 and k >= 2 and m >= 8 * n
+
+    def longer(r):
+        return int((deg > r).sum().item())
+
+    sample = []
+    r = 0
+    if stash:
+        two = int(torch.clamp(deg, max=2).sum().item())
+        sample += [row_bytes * n + 4 * two + 4 * n + 4 * n, 4 * n + 4 * n]
+        r = 2
+    sample += [row_bytes * n + 4 * longer(q) + 4 * n for q in range(r, k)]
+    link = 4 * n + row_bytes * n
+    if finish_rows is not None:
+        link = 4 * n + 8 * int(finish_rows) + 4 * int(finish_edges)
+    return {"init": [4 * n], "sample": sample or [0], "compress": [8 * n], "giant": [4 * 1024],
+            "link_rows": [link], "link_heavy": [0], "final_compress": [8 * n]}
+
+
+def per_launch(bytes_lists):
+    """Mean bytes per launch of each kernel."""
+    return {kk: sum(v) / len(v) for kk, v in bytes_lists.items()}
+
+
+def step_bytes_of(bytes_lists, per, steps):
+    """Algorithmic bytes of one step: every launch the profiler saw, each
+    charged its own bytes (kernels launched more than once per step with
+    different bytes, like the sampling rounds, are charged their mean)."""
+    mean = per_launch(bytes_lists)
+    return sum(mean.get(kk, 0) * cnt / steps for kk, (_, cnt) in per.items())
 
 
 def run_reference_graphs(args, world, spec_w):
@@ -227,7 +261,11 @@ def run_reference_graphs(args, world, spec_w):
 
 
 def run_reference(args, rank, world):
-    """--impl reference: the reference's own CPU code on this host."""
+    """--impl reference: the reference's own CPU code on this host.  Plain
+    single-graph workloads time compute_connected_components_pthreads with
+    every host thread; partitioned workloads time the reference's own MPI
+    path (mpi_cc_benchmark at the workload's rank count, its CLI's per-run
+    time) - a bounded number of full solves, ``--ref-runs``."""
     if rank != 0:
         return 0
     spec_w = WORKLOADS[args.workload]
@@ -241,8 +279,34 @@ def run_reference(args, rank, world):
     rp = rp_d.cpu().numpy().view(np.uint64)
     col = col_d.cpu().numpy().view(np.uint32)
     del rp_d, col_d
+    torch.cuda.empty_cache()
     n, m = len(rp) - 1, int(rp[-1])
     threads = os.cpu_count() or 1
+    cfg = workload_config(args.workload, n, m)
+    if spec_w.get("dist"):
+        parts = args.parts or spec_w["parts"]
+        runs = args.ref_runs or spec_w.get("ref_runs", 1)
+        base, why = ref_mpi_baseline(rp, col, parts, args.chunk, args.exchange, runs,
+                                     mat=spec_w.get("mat", False))
+        if base is None:
+            print(json.dumps({"impl": "reference", "unavailable": why}), flush=True)
+            return 0
+        gteps = base["value"]
+        cfg.update(partitions=parts, chunk_size=args.chunk, exchange_interval=args.exchange,
+                   components=base["components"], rounds=base["rounds"])
+        line = {
+            "impl": "reference", "metric": "CC GTEPS", "value": gteps, "unit": "GTEPS",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": base["seconds_per_solve"] * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": cfg, "cpu_baseline": base,
+            "e2e": {"value": gteps, "unit": "GTEPS", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "timing": f"the reference CLI's own per-run times of {runs} full solve(s); the "
+                      f"--steps/--warmup counts are not repeated on the CPU (minutes per solve)",
+        }
+        print(json.dumps(line), flush=True)
+        return 0
     for _ in range(args.warmup):
         oracle.ref_pthreads_labels(rp, col, threads, 8192)
     times = []
@@ -256,8 +320,9 @@ def run_reference(args, rank, world):
         "impl": "reference", "metric": "CC GTEPS", "value": gteps, "unit": "GTEPS",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
-        "data": "synthetic", "config": workload_config(args.workload, n, m),
+        "data": "synthetic", "config": cfg,
         "cpu_baseline": {"value": gteps, "unit": "GTEPS", "cores": threads, "kind": "reference",
+                         "path": "compute_connected_components_pthreads",
                          "sample": f"full graph, {args.steps} solves, chunk 8192"},
         "e2e": {"value": gteps, "unit": "GTEPS", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
@@ -267,71 +332,284 @@ def run_reference(args, rank, world):
 
 
 def cpu_baseline(rp, col, budget_s=20.0):
+    """The reference's compute_connected_components_pthreads (compiled
+    unmodified into oracle/_ref) on all host threads, chunk 8192: up to 3
+    solves within ``budget_s``.  Returns (baseline dict, labels of the last
+    solve) - the labels are the parity check of the GPU result."""
     import oracle
     threads = os.cpu_count() or 1
     m = int(rp[-1])
     times = []
     t_start = time.perf_counter()
+    labels = None
     if oracle.have_ref():
         kind = "reference"
         while len(times) < 3 and time.perf_counter() - t_start < budget_s:
             t0 = time.perf_counter()
-            oracle.ref_pthreads_labels(rp, col, threads, 8192)
+            labels = oracle.ref_pthreads_labels(rp, col, threads, 8192)
             times.append(time.perf_counter() - t0)
         sample = f"full graph, {len(times)} solves, {threads} threads, chunk 8192"
         used = threads
     else:
         kind = "port"
         t0 = time.perf_counter()
-        oracle.lp_labels(rp, col)
+        labels, _ = oracle.lp_labels(rp, col)
         times.append(time.perf_counter() - t0)
         sample = "full graph, 1 solve, 1 thread (oracle label propagation)"
         used = 1
     t = min(times)
-    return {"value": (m / 2) / t / 1e9, "unit": "GTEPS", "cores": used, "kind": kind,
-            "sample": sample, "seconds_per_solve": t}
+    return ({"value": (m / 2) / t / 1e9, "unit": "GTEPS", "cores": used, "kind": kind,
+             "path": "compute_connected_components_pthreads", "sample": sample,
+             "seconds_per_solve": t}, labels)
 
 
-def dist_bytes(n, m, st):
-    """Algorithmic bytes per launch of the partitioned path's kernels (the
-    local-CC kernels are counted as in algorithmic_bytes, without the
-    sampled-entry term)."""
+def host_mem_available():
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    return 0
+
+
+def ref_mpi_memory(n, m, parts, boundary_raw=None, freed=0):
+    """(fits, reason): whether this host can hold the reference's own
+    partitioned run.  Peak host bytes: rank 0 holds the whole CSR while the
+    partitions fill (2x the CSR), then the partitions plus 8 bytes per cut
+    entry of the boundary arrays and ~13 bytes per vertex of per-vertex
+    arrays.  ``freed``: bytes the caller releases before the run."""
+    csr = 8 * (n + 1) + 4 * m
+    raw = boundary_raw if boundary_raw is not None else m
+    need = max(2 * csr, csr + 8 * raw + 13 * n) + (2 << 30)
+    have = host_mem_available() + freed
+    if host_mem_available() and need > have:
+        return False, (f"host has {have / 2**30:.1f} GiB available, the reference's "
+                       f"{parts}-rank run needs about {need / 2**30:.1f} GiB")
+    return True, None
+
+
+def ref_mpi_write(folder, rp, col, mat):
+    """The graph as the reference's CLI input: MAT level 5 (struct Problem,
+    sparse field A) when ``mat``, else the CSR binary format under a .mat
+    name, which the matio shim serves as one sparse variable."""
+    import oracle
+    path = os.path.join(folder, "graph.mat")
+    t0 = time.perf_counter()
+    if mat:
+        oracle.write_mat(path, rp, col)
+    else:
+        oracle.write_csrbin(path, rp, col)
+    return path, time.perf_counter() - t0
+
+
+def ref_mpi_time(path, n, m, parts, chunk, exchange, runs, threads=None, timeout=1500,
+                 mat=False):
+    """Runs the reference's own partitioned path - its mpi_cc_benchmark CLI
+    (src/mpi_cc_benchmark.c, cc_mpi.c, exchange_plan.c, graph_dist.c, ...,
+    compiled unmodified over the fakempi / fakematio shims into oracle/_ref)
+    at ``parts`` ranks x floor(cores / parts) pthreads, -c chunk -e exchange
+    -r runs.  Its time is the CLI's own per-run time (the region around one
+    compute_connected_components_mpi_advanced call)."""
+    import oracle
+    cores = os.cpu_count() or 1
+    threads = threads or max(1, cores // parts)
+    res = oracle.ref_mpi_run(path, parts, threads=threads, chunk=chunk, exchange=exchange,
+                             runs=runs, timeout=timeout)
+    runs_out = res["runs"]
+    secs = [r["seconds"] for r in runs_out if r["seconds"]]
+    t = sum(secs) / len(secs)
+    last = runs_out[-1]
+    return {"value": (m / 2) / t / 1e9, "unit": "GTEPS", "cores": parts * threads,
+            "kind": "reference", "path": "mpi_cc_benchmark (compute_connected_components_"
+            "mpi_advanced over fakempi ranks)",
+            "sample": f"full graph, {len(secs)} solve(s) of -np {parts} -t {threads} "
+                      f"-c {chunk} -e {exchange} -r {runs} ({'MAT v5' if mat else 'CSR binary'}"
+                      f" input, loaded once in {res['graph'].get('load_s', 0):.1f} s)",
+            "seconds_per_solve": t, "ranks": parts, "threads_per_rank": threads,
+            "components": last["components"], "rounds": last["rounds"],
+            "bounds": last["bounds"], "boundary_raw": sum(last["raw"].values()),
+            "boundary_dedup": sum(last["dedup"].values()),
+            "ghosts": sum(last["ghosts"].values())}
+
+
+def ref_mpi_baseline(rp, col, parts, chunk, exchange, runs, boundary_raw=None, mat=False):
+    """ref_mpi_memory + ref_mpi_write + ref_mpi_time on a scratch folder
+    (CCB200_SCRATCH or the system temp folder).  Returns (baseline, None) or
+    (None, reason)."""
+    import tempfile
+    import oracle
+    if not oracle.have_ref_mpi():
+        return None, "reference MPI build (oracle/_ref/mpi_cc_benchmark) absent"
+    n, m = len(rp) - 1, int(rp[-1])
+    fits, why = ref_mpi_memory(n, m, parts, boundary_raw)
+    if not fits:
+        return None, why
+    with tempfile.TemporaryDirectory(dir=os.environ.get("CCB200_SCRATCH")) as tmp:
+        path, write_s = ref_mpi_write(tmp, rp, col, mat)
+        base = ref_mpi_time(path, n, m, parts, chunk, exchange, runs, mat=mat)
+    base["file_write_s"] = write_s
+    return base, None
+
+
+def local_degrees(torch, rp_d, col_d, bounds, chunk=1 << 26):
+    """Row lengths of the partitions' local subgraphs (entries whose target
+    lies in the row's own partition, src/cc_mpi.c:252-275), counted on the
+    device in chunks of entries (setup work, outside any timed region)."""
+    n = rp_d.numel() - 1
+    dev = rp_d.device
+    ldeg = torch.zeros(n, dtype=torch.int32, device=dev)
+    for p in range(len(bounds) - 1):
+        b0, b1 = int(bounds[p]), int(bounds[p + 1])
+        if b1 <= b0:
+            continue
+        rows = rp_d[b0:b1 + 1]
+        e0, e1 = int(rows[0].item()), int(rows[-1].item())
+        for c0 in range(e0, e1, chunk):
+            c1 = min(e1, c0 + chunk)
+            v = col_d[c0:c1]
+            local = (v >= b0) & (v < b1)
+            pos = torch.arange(c0, c1, device=dev, dtype=torch.int64)[local]
+            r = torch.searchsorted(rows, pos, right=True) - 1 + b0
+            ldeg.index_add_(0, r, torch.ones_like(r, dtype=torch.int32))
+            del v, local, pos, r
+    return ldeg
+
+
+def dist_bytes(torch, ldeg, n, m, st, chunk):
+    """Algorithmic bytes per launch of the partitioned path's kernels (lists
+    where one kernel's launches differ).  The local-CC kernels run on the
+    partitions' local subgraphs and are counted as in local_cc_bytes over
+    the local row lengths; the rest as listed per kernel below.  Two layouts
+    of the local subgraphs: read in place as each row's run inside its own
+    partition (row_runs: a row-start bitmap, a row-order check and per-row
+    partition offsets), or a local CSR built by a count and a fill pass."""
+    from cc_mpi_b200 import _lib
     R, U, G, reps = int(st.sorted_keys), int(st.pair_count), int(st.ghost_count), \
         int(st.rep_count)
     lm = int(st.local_entries)
+    P = int(st.parts) if hasattr(st, "parts") else 4
     sorted_rows = bool(st.sorted_rows)
-    return {
-        "init": 4 * n, "sample": 8 * (n + 1) + 8 * n, "compress": 8 * n,
-        "final_compress": 8 * n, "link_rows": 4 * n + 8 * n, "giant": 4096,
-        "dist_local_count": 4 * m, "dist_tiles": 8 * (n + 1),
-        "dist_local_fill": 4 * m + 4 * lm + 16 * (n + 1),
-        "dist_gflag": 4 * n + n // 8, "dist_pairs_bitmap": 4 * n + 4 * G,
-        "dist_merge_keys": 16 * (R + G),
-        "dist_reps": 4 * n + 12 * reps,
-        "dist_pairs": 8 * (n + 1) + 4 * m + (m // 8 if sorted_rows else n // 8 + 8 * R),
-        "dist_pairs_local": n // 8 + 8 * R,
-        "sort_hist": 8 * R, "sort_scatter": 16 * R, "dist_dedup": 8 * R,
-        "dist_ghosts": 8 * R + 8 * U + 24 * G, "merge_hook": 12 * U,
-        "merge_upd": 12 * reps, "merge_exch_pack": 16 * G, "merge_exch_scatter": 16 * G,
-        "merge_exch_pull": 12 * U,
-        "dist_labels": 12 * n, "dist_plan": 0, "dist_bounds": 0, "scan": 0,
-        "dist_pairs_heavy": 0,
-    }
+    runs = bool(getattr(st, "row_runs", 0))
+    out = local_cc_bytes(torch, ldeg, n, lm, _lib.opts(chunk_size=chunk),
+                         row_bytes=16 if runs else 8)
+    tiles, wtiles = (m + 4095) // 4096, (m + 511) // 512
+    if runs:
+        out.update({
+            # k_row_starts: row pointers in, one bit per entry out
+            "dist_tiles": [8 * (n + 1) + m // 8],
+            # k_rows_ascend: every column entry and its row-start bit
+            "dist_local_count": [4 * m + m // 8],
+            # k_row_ranges: row pointers in; P offsets and the own run out
+            "dist_local_fill": [8 * (n + 1) + 4 * P * n + 16 * n],
+            # k_emit_ranges: row pointer and P offsets in, mask out (the
+            # mirror-mark words it reads are not counted)
+            "dist_pairs": [8 * n + 4 * P * n + 4 * n],
+        })
+    else:
+        out.update({
+            # k_part_cols (P+1 searches), k_tile_first over 4096- and
+            # 512-entry tiles
+            "dist_tiles": [0, 8 * (n + 1) + 4 * tiles, 8 * (n + 1) + 4 * wtiles],
+            "dist_local_count": [4 * m + 4 * tiles],
+            "dist_local_fill": [4 * m + 4 * lm + 16 * (n + 1)],
+            "dist_pairs": [8 * (n + 1) + 4 * m + (m // 8 if sorted_rows else n // 8 + 8 * R)],
+        })
+    out.update({
+        "dist_gflag": [4 * n + n // 8],
+        "dist_pairs_bitmap": [4 * n + 4 * G],
+        "dist_merge_keys": [16 * (R + G)],
+        "dist_reps": [4 * n + 12 * reps],
+        "dist_pairs_local": [n // 8 + 8 * R],
+        "sort_hist": [8 * R], "sort_scatter": [16 * R], "dist_dedup": [8 * R],
+        "dist_ghosts": [8 * R + 8 * U + 24 * G], "merge_hook": [12 * U],
+        # an exchange reads each ghost's cached rep and last-sent label (8G)
+        # and writes last-sent, ghost label and delta entry of every changed
+        # ghost (12 per sent pair); the first exchange changes all G ghosts,
+        # so its hook update is the pull pass over all pairs (12U) whenever
+        # G > U/8 - later ones are counted as push (pairs walked not counted)
+        "merge_upd": [12 * reps],
+        "merge_exchange": [8 * G + 12 * int(st.sent_pairs) // max(int(st.exchanges), 1)],
+        "merge_exch_push": [0],
+        "merge_exch_pull": [12 * U * (1 if 8 * G > U else 0) // max(int(st.exchanges), 1)],
+        "dist_labels": [12 * n], "dist_plan": [0], "dist_bounds": [0], "scan": [0],
+        "dist_pairs_heavy": [0], "merge_init": [0],
+    })
+    return out
+
+
+# DRAM bytes per launch measured by ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum) for the kernels that lead a workload's step, per
+# unit of work, so that a capture on a smaller graph scales to the bench's
+# graph: "entry" = CSR entries, "vertex" = vertices.  Each figure comes from
+# the capture summarised in the named profiles/ file.
+NCU_TRAFFIC = {}
+
+
+def ncu_traffic(kernel, n, m):
+    t = NCU_TRAFFIC.get(kernel)
+    if not t:
+        return None
+    units = m if t["per"] == "entry" else n
+    return {"bytes_per_launch": t["bytes_per_unit"] * units, "source": t["source"],
+            "scaled": f"{t['bytes_per_unit']:.3f} bytes per {t['per']} x {units}"}
+
+
+def roofline_dict(dom, achieved, peak, peak_kind, traffic, bytes_per, bytes_lists, per,
+                  step_bytes, whole):
+    """The line's roofline object for the dominant kernel: achieved =
+    algorithmic bytes per launch / mean launch time (CUDA events on the
+    launching stream), frac = achieved / measured peak; traffic = ncu DRAM
+    bytes per launch (scaled from the capture) or null."""
+    b = bytes_per.get(dom, 0)
+    d = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+         "frac": achieved / peak, "peak_source": peak_kind,
+         "traffic": traffic["bytes_per_launch"] if traffic else None,
+         "bytes_per_launch": b, "ms_per_launch": per[dom][0],
+         "whole_solve": {"algorithmic_bytes": step_bytes, "achieved": whole,
+                         "frac": whole / peak}}
+    if len(bytes_lists.get(dom, [])) > 1:
+        d["bytes_per_launch_each"] = bytes_lists[dom]
+    if traffic:
+        d["traffic_over_algorithmic"] = traffic["bytes_per_launch"] / b if b else None
+        d["traffic_source"] = traffic["source"]
+        d["traffic_scaled"] = traffic["scaled"]
+    return d
+
+
+def release_pinned(torch):
+    """Hands torch's cached pinned host blocks back to the system."""
+    fn = getattr(torch._C, "_host_emptyCache", None)
+    if fn:
+        fn()
 
 
 def run_dist(args, torch, dist_mod, rank, world, dev):
     """Partitioned workloads: a step is one ccgpu_dist_cc solve (all
     partitions device-resident) - the timed region of the reference's
-    benchmark, one compute_connected_components_mpi_advanced call."""
+    benchmark, one compute_connected_components_mpi_advanced call.
+
+    Parity, on rank 0: the labels must equal those of the reference's own
+    compute_connected_components_pthreads on the same graph (its labels are
+    the minimum vertex id of each component, the contract of
+    include/cc_mpi.h:26-27), and the component count, partition bounds and
+    boundary / dedup / ghost totals must equal what the reference's own MPI
+    path prints when it runs as the CPU baseline; graphs the oracle finishes
+    in seconds are also checked against its restatement (round and exchange
+    counts included)."""
     import numpy as np
     from cc_mpi_b200 import _lib, cc, dist
     spec = WORKLOADS[args.workload]
     L = _lib.lib()
     parts = args.parts or spec["parts"]
+    t0 = time.perf_counter()
     rp_d, col_d = make_graph(torch, args.workload, args.seed + rank)
     torch.cuda.synchronize()
     torch.cuda.empty_cache()  # hand the generator's cached blocks back for the solver's pool
+    gen_s = time.perf_counter() - t0
     n, m = rp_d.numel() - 1, col_d.numel()
+    log(f"{args.workload}: n={n} m={m} generated in {gen_s:.1f} s")
     lab = torch.empty(n, dtype=torch.int32, device=dev)
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.int32, device=dev)
     stream = torch.cuda.current_stream()
@@ -342,23 +620,20 @@ def run_dist(args, torch, dist_mod, rank, world, dev):
                                    d_labels=lab, stream=sptr)
 
     st, bounds = solve()
-    # verification: the unpartitioned union-find path, the device invariants,
-    # and (for graphs the CPU checks in seconds) the oracle
+    torch.cuda.synchronize()
+    # the unpartitioned union-find solve and the device invariants: a check
+    # that needs no host copy (it cannot tell merged components apart, the
+    # reference comparison below does)
     ref = torch.empty(n, dtype=torch.int32, device=dev)
     cc.local_cc_device(rp_d, col_d, n, m, ref, stream=sptr)
     torch.cuda.synchronize()
-    verified = bool(torch.equal(ref, lab)) and \
+    same_as_unpartitioned = bool(torch.equal(ref, lab)) and \
         cc.check_labels_device(rp_d, col_d, n, m, lab) == 0
-    oracle_checked = False
-    if rank == 0 and not args.no_verify and m < 1_200_000_000:
-        import oracle
-        want, _, ost = oracle.dist_cc(rp_d.cpu().numpy().view(np.uint64),
-                                      col_d.cpu().numpy().view(np.uint32), parts, 1,
-                                      args.exchange)
-        verified = verified and bool((lab.cpu().numpy().view(np.uint32) == want).all()) and \
-            ost.rounds == st.rounds and ost.exchanges == st.exchanges
-        oracle_checked = True
     del ref
+    ldeg = local_degrees(torch, rp_d, col_d, bounds)
+    st.parts = parts
+    bytes_lists = dist_bytes(torch, ldeg, n, m, st, args.chunk)
+    del ldeg
     torch.cuda.empty_cache()
     for _ in range(args.warmup):
         flush.fill_(1)
@@ -368,6 +643,8 @@ def run_dist(args, torch, dist_mod, rank, world, dev):
     def timed_steps():
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
               for _ in range(args.steps)]
+        if world > 1:
+            dist_mod.barrier()
         torch.cuda.synchronize()
         for i in range(args.steps):
             flush.fill_(i)
@@ -382,8 +659,6 @@ def run_dist(args, torch, dist_mod, rank, world, dev):
             t = float(tt.item())
         return t
 
-    if world > 1:
-        dist_mod.barrier()
     launches0 = L.ccgpu_ctx_launches(None)
     with ClockSampler(dev.index or 0) as clk:
         t_ms = timed_steps()
@@ -400,12 +675,13 @@ def run_dist(args, torch, dist_mod, rank, world, dev):
     per = {names[i]: (ms[i] / cnt[i], int(cnt[i])) for i in range(k) if cnt[i]}
     total_kernel_ms = {kk: v[0] * v[1] / args.steps for kk, v in per.items()}
     dom = max(total_kernel_ms, key=total_kernel_ms.get)
-    bytes_per = dist_bytes(n, m, st)
+    bytes_per = per_launch(bytes_lists)
     peak, peak_kind = read_peaks()
     achieved = bytes_per.get(dom, 0) / (per[dom][0] / 1e3) / 1e9
-    step_bytes = sum(bytes_per.get(kk, 0) * v[1] / args.steps for kk, v in per.items())
+    step_bytes = step_bytes_of(bytes_lists, per, args.steps)
     whole = step_bytes / (t_ms / 1e3) / 1e9
     value = (m // 2) * world / (t_ms / 1e3) / 1e9
+    traffic = ncu_traffic(dom, n, m)
 
     # e2e through the reference-facing calls with host buffers
     rp_h = torch.empty(n + 1, dtype=torch.int64, pin_memory=True)
@@ -440,13 +716,69 @@ def run_dist(args, torch, dist_mod, rank, world, dev):
         L.free_dist_csr_view(C.byref(Gd))
         e2e_t.append(time.perf_counter() - t0)
     e2e_s = sum(e2e_t[1:]) / len(e2e_t[1:])
-    e2e_ok = bool((lab_h == lab.cpu().numpy().view(np.uint32)).all())
+    if world > 1:
+        tt = torch.tensor([e2e_s], device=dev)
+        dist_mod.all_reduce(tt, op=dist_mod.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    got = lab.cpu().numpy().view(np.uint32)
+    e2e_ok = bool((lab_h == got).all())
     L.cc_group_free(grp)
 
-    cpu = None
+    # parity with the reference, on rank 0
+    rp_np, col_np = rp_h.numpy().view(np.uint64), col_h.numpy().view(np.uint32)
+    parity = {"same_as_unpartitioned_solve": same_as_unpartitioned}
+    pth = None
+    if rank == 0 and not args.no_verify:
+        pth, ref_labels = cpu_baseline(rp_np, col_np, budget_s=0.0 if world > 1 else 30.0)
+        parity["labels_equal_reference_pthreads"] = bool((got == ref_labels).all())
+        parity["components_equal_reference_pthreads"] = \
+            int(np.count_nonzero(ref_labels == np.arange(n, dtype=np.uint32))) == int(st.roots)
+        del ref_labels
+        if m < 1_200_000_000:
+            import oracle
+            want, obounds, ost = oracle.dist_cc(rp_np, col_np, parts, 1, args.exchange)
+            parity["oracle_labels_rounds_exchanges"] = bool((got == want).all()) and \
+                ost.rounds == st.rounds and ost.exchanges == st.exchanges and \
+                [int(x) for x in obounds] == [int(x) for x in bounds]
+    cpu = pth
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(rp_h.numpy().view(np.uint64), col_h.numpy().view(np.uint32),
-                           budget_s=30.0)
+        # the reference's partitioned path on the same graph, host memory
+        # permitting: the graph file is written from the pinned copies, which
+        # are released before the run
+        import tempfile
+        import oracle
+        base, why = None, None
+        if not oracle.have_ref_mpi():
+            why = "reference MPI build (oracle/_ref/mpi_cc_benchmark) absent"
+        else:
+            fits, why = ref_mpi_memory(n, m, parts, int(st.boundary_raw),
+                                       freed=8 * (n + 1) + 4 * m)
+            if fits:
+                tmp = tempfile.TemporaryDirectory(dir=os.environ.get("CCB200_SCRATCH"))
+                try:
+                    path, write_s = ref_mpi_write(tmp.name, rp_np, col_np, spec.get("mat", False))
+                    del rp_np, col_np, g
+                    rp_h = col_h = None
+                    release_pinned(torch)
+                    base = ref_mpi_time(path, n, m, parts, args.chunk, args.exchange,
+                                        spec.get("ref_runs", 1), mat=spec.get("mat", False))
+                    base["file_write_s"] = write_s
+                except Exception as e:  # the baseline is reported, never the target
+                    base, why = None, f"reference MPI run failed: {e}"
+                finally:
+                    tmp.cleanup()
+        if base is not None:
+            parity["mpi_components_equal"] = base["components"] == int(st.roots)
+            parity["mpi_bounds_equal"] = base["bounds"] == [int(x) for x in bounds]
+            parity["mpi_boundary_counts_equal"] = \
+                base["boundary_raw"] == int(st.boundary_raw) and \
+                base["boundary_dedup"] == int(st.pair_count) and \
+                base["ghosts"] == int(st.ghost_count)
+            base["pthreads_baseline"] = pth
+            cpu = base
+        elif pth is not None:
+            cpu = dict(pth, mpi_unavailable=why)
+    verified = all(parity.values())
     if rank == 0:
         cfg = workload_config(args.workload, n, m)
         cfg.update(partitions=parts, chunk_size=args.chunk, exchange_interval=args.exchange,
@@ -456,6 +788,7 @@ def run_dist(args, torch, dist_mod, rank, world, dev):
                    sorted_rows=bool(st.sorted_rows),
                    boundary_dedup=int(st.pair_count),
                    ghosts=int(st.ghost_count), reps=int(st.rep_count),
+                   local_entries=int(st.local_entries),
                    sent_pairs=int(st.sent_pairs), sort_passes=int(st.sort_passes),
                    phases_ms={"bounds": st.ms_bounds, "local": st.ms_local,
                               "pairs": st.ms_pairs, "sort": st.ms_sort,
@@ -463,19 +796,16 @@ def run_dist(args, torch, dist_mod, rank, world, dev):
                    l2="2x L2 buffer written between timed steps; col_idx > L2",
                    parallelism=f"{parts} partitions on one device" +
                                (f", replicas{world}" if world > 1 else ""),
-                   verified=verified, verified_by_oracle=oracle_checked,
-                   e2e_labels_match=e2e_ok)
+                   generate_s=gen_s, verified=verified, verified_by_reference=bool(
+                       parity.get("labels_equal_reference_pthreads")),
+                   parity=parity, e2e_labels_match=e2e_ok)
         line = {
             "metric": "CC GTEPS", "value": value, "unit": "GTEPS", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic", "config": cfg,
-            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                         "traffic": None, "bytes_per_launch": bytes_per.get(dom, 0),
-                         "ms_per_launch": per[dom][0],
-                         "whole_solve": {"algorithmic_bytes": step_bytes, "achieved": whole,
-                                         "frac": whole / peak}},
+            "roofline": roofline_dict(dom, achieved, peak, peak_kind, traffic, bytes_per,
+                                      bytes_lists, per, step_bytes, whole),
             "kernels": {kk: {"ms": round(v[0], 5), "launches": v[1],
                              "gbs": round(bytes_per.get(kk, 0) / (v[0] / 1e3) / 1e9, 1)}
                         for kk, v in per.items()},
@@ -893,7 +1223,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="rmat24")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c3")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-verify", action="store_true")
@@ -903,6 +1233,8 @@ def main():
     ap.add_argument("--parts", type=int, default=0, help="partitions (partitioned workloads)")
     ap.add_argument("--chunk", type=int, default=8192, help="-c of the partitioned workloads")
     ap.add_argument("--exchange", type=int, default=1, help="-e of the partitioned workloads")
+    ap.add_argument("--ref-runs", type=int, default=0,
+                    help="full solves the partitioned reference arm times (-r of its CLI)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -974,7 +1306,9 @@ def main():
         verified = bool((got == want).all()) and viol == 0
         if not verified:
             log(f"VERIFY FAILED: {int((got != want).sum())} labels differ, {viol} violations")
-    bytes_per = algorithmic_bytes(torch, rp_d, n, m, opts.sample_rounds, st)
+    bytes_lists = local_cc_bytes(torch, rp_d[1:] - rp_d[:-1], n, m, opts, st.finish_rows,
+                                 st.finish_edges)
+    bytes_per = per_launch(bytes_lists)
 
     for _ in range(args.warmup):
         flush.fill_(1)
@@ -1037,9 +1371,8 @@ def main():
     per = {names[i]: (ms[i] / cnt[i], int(cnt[i])) for i in range(k) if cnt[i]}
     dom = max(per, key=lambda kk: per[kk][0] * per[kk][1])
     peak, peak_kind = read_peaks()
-    dom_bytes = bytes_per.get(dom, 0)
-    achieved = dom_bytes / (per[dom][0] / 1e3) / 1e9
-    total_bytes = sum(bytes_per.get(kk, 0) for kk in per)
+    achieved = bytes_per.get(dom, 0) / (per[dom][0] / 1e3) / 1e9
+    total_bytes = step_bytes_of(bytes_lists, per, args.steps)
     whole = total_bytes / (t_ms / 1e3) / 1e9
 
     # e2e through the reference-facing call with pinned host buffers
@@ -1068,8 +1401,11 @@ def main():
     e2e_ok = bool((lab_h.numpy() == lab_d.cpu().numpy()).all())
 
     cpu = None
+    by_reference = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(rp_np, col_np)
+        cpu, ref_labels = cpu_baseline(rp_np, col_np)
+        by_reference = bool((lab_d.cpu().numpy().view(np.uint32) == ref_labels).all())
+        del ref_labels
 
     if rank == 0:
         cfg = workload_config(args.workload, n, m)
@@ -1079,18 +1415,15 @@ def main():
                          "heavy_degree": opts.heavy_degree, "skip_giant": opts.skip_giant,
                          "hook_mode": opts.hook_mode},
                    parallelism=f"replicas{world}" if world > 1 else "single",
-                   verified_vs_oracle=verified, e2e_labels_match=e2e_ok)
+                   verified_vs_oracle=verified, verified_by_reference=by_reference,
+                   e2e_labels_match=e2e_ok)
         line = {
             "metric": "CC GTEPS", "value": value, "unit": "GTEPS", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic", "config": cfg,
-            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                         "traffic": None, "bytes_per_launch": dom_bytes,
-                         "ms_per_launch": per[dom][0],
-                         "whole_solve": {"algorithmic_bytes": total_bytes, "achieved": whole,
-                                         "frac": whole / peak}},
+            "roofline": roofline_dict(dom, achieved, peak, peak_kind, ncu_traffic(dom, n, m),
+                                      bytes_per, bytes_lists, per, total_bytes, whole),
             "kernels": {kk: {"ms": round(v[0], 5), "launches": v[1],
                              "gbs": round(bytes_per.get(kk, 0) / (v[0] / 1e3) / 1e9, 1)}
                         for kk, v in per.items()},

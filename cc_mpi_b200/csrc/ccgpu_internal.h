@@ -271,11 +271,13 @@ __device__ __forceinline__ uint32_t cc_warp_min(uint32_t v)
  * pieces of `chunk` entries: rows are taken 256 at a time, the block scans
  * their piece counts in shared memory, and piece g of the batch goes to
  * warp g mod (all warps).  fn(v, jb, je) is called by all 32 lanes of a
- * warp together.  Rows are [row_ptr[v] + skip, row_ptr[v+1]) clamped to m.
- * Must be called by every thread of a 256-thread block. */
+ * warp together.  Rows are [row_ptr[v] + skip, row_ptr[v+1]) clamped to m,
+ * or [row_ptr[v] + skip, row_end[v]) when row_end is given.  Must be called
+ * by every thread of a 256-thread block. */
 template <typename Fn>
 __device__ __forceinline__ void cc_for_heavy_pieces(const uint32_t *list, uint32_t count,
-                                                    const uint64_t *row_ptr, uint64_t m,
+                                                    const uint64_t *row_ptr,
+                                                    const uint64_t *row_end, uint64_t m,
                                                     uint32_t skip, uint64_t chunk, Fn fn)
 {
     __shared__ uint64_t s_pre[257];
@@ -289,7 +291,7 @@ __device__ __forceinline__ void cc_for_heavy_pieces(const uint32_t *list, uint32
         uint64_t pieces = 0;
         if (h < count) {
             uint32_t v = list[h];
-            uint64_t e = row_ptr[v + 1], b = row_ptr[v];
+            uint64_t e = row_end ? row_end[v] : row_ptr[v + 1], b = row_ptr[v];
             if (e > m)
                 e = m;
             if (b > e)

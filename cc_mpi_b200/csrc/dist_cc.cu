@@ -13,8 +13,9 @@
  *   src/exchange_plan.c:48-225  exchange plan              -> k_plan
  *   src/cc_mpi.c:541-710        merge rounds               -> k_hook_init,
  *                                                             k_upd
- *   src/exchange_plan.c:242-425 delta exchange             -> k_pack,
- *                                                             k_scatter
+ *   src/exchange_plan.c:242-425 delta exchange             -> k_exchange,
+ *                                                             k_delta_push /
+ *                                                             k_hook_pull
  *   src/cc_mpi.c:730-742        roots / labels             -> k_final
  *
  * Layout in HBM: all per-vertex arrays are indexed by global vertex id (a
@@ -27,9 +28,9 @@
  *
  * The reference's HOOK (comp_min = min over cut pairs of the ghost labels)
  * only changes when ghost labels change, i.e. at exchanges; hook[] keeps that
- * minimum per rep and is lowered by the exchange scatter for the pairs of
- * each ghost that received a label, which gives the same comp_min every
- * round without re-reading every pair.
+ * minimum per rep and is lowered by each exchange for the pairs of every
+ * ghost whose label it changed, which gives the same comp_min every round
+ * without re-reading every pair.
  */
 #include <cstdio>
 #include <cstring>
@@ -140,6 +141,8 @@ struct EmitParams {
                               * partition's giant tree (sorted-row mode), NULL = gather gflag */
     unsigned long long *bad; /* set when a row is not strictly ascending or a
                               * mirror entry is missing: sorted-row mode invalid */
+    const uint32_t *roff;    /* [n*parts] partition offsets of sorted rows
+                              * (k_row_ranges), NULL = not computed      */
 };
 
 /* Plain keys are rare (most cut entries fall in a giant tree), so a block
@@ -417,6 +420,237 @@ __global__ void __launch_bounds__(kB) k_emit_sorted(EmitParams E, const uint32_t
     add_raw(E, raw, lane);
 }
 
+/* ---------------------------------------------- sorted-row ranges
+ *
+ * When every row is strictly ascending - what the reference's loader always
+ * builds (the CSC to CSR transposition of src/graph.c:91-117 emits each row
+ * in column order) - a row's entries inside partition q are one contiguous
+ * run, found by binary search on the partition bounds.  The local subgraph
+ * of each partition (src/cc_mpi.c:252-297) is then the own run of every
+ * row, read in place by the local CC (rows as [lb, le) sub-ranges), and the
+ * boundary pairs of a row's run in partition q come from its mirror marks
+ * alone.  The row order is checked first, in one streaming pass. */
+
+/* Bit rp[v] of starts for every non-empty row v (the bitmap is zeroed
+ * first); lanes whose rows start in the same word combine their bits. */
+__global__ void __launch_bounds__(kB) k_row_starts(const uint64_t *__restrict__ row_ptr,
+                                                   uint32_t n, uint64_t m, uint32_t *starts)
+{
+    const int lane = threadIdx.x & 31;
+    const uint64_t stride = (uint64_t)gridDim.x * kB;
+    for (uint64_t base = (uint64_t)blockIdx.x * kB; base < n; base += stride) {
+        const uint64_t v = base + threadIdx.x;
+        uint64_t b = 0;
+        bool ok = false;
+        if (v < n) {
+            b = __ldg(row_ptr + v);
+            const uint64_t e = __ldg(row_ptr + v + 1);
+            ok = b < e && b < m;
+        }
+        const unsigned long long w = ok ? (unsigned long long)(b >> 5) : ~0ull;
+        const unsigned peers = __match_any_sync(0xffffffffu, w);
+        const uint32_t all = __reduce_or_sync(peers, ok ? 1u << (b & 31) : 0u);
+        if (ok && (__ffs(peers) - 1) == lane)
+            atomicOr(starts + w, all);
+    }
+}
+
+/* Row order over the whole column array, 16 entries per lane (16-byte
+ * loads when aligned): an entry that does not start a row is compared with
+ * the one before it.  flags[0] is set when some row descends (its
+ * partition runs are not contiguous), flags[1] when some row repeats an
+ * entry (mirror marks need strictly ascending rows). */
+__global__ void __launch_bounds__(kB) k_rows_ascend(const uint32_t *__restrict__ col, uint64_t m,
+                                                    const uint32_t *__restrict__ starts, int vec,
+                                                    unsigned *flags)
+{
+    const int lane = threadIdx.x & 31;
+    const uint64_t groups = (m + kTileE - 1) / kTileE;
+    const uint64_t wstride = (uint64_t)gridDim.x * kB;
+    bool desc = false, dup = false;
+    for (uint64_t base = (uint64_t)blockIdx.x * kB + (threadIdx.x & ~31u); base < groups;
+         base += wstride) {
+        const uint64_t t = base + lane;
+        const uint64_t j0 = t * kTileE;
+        uint32_t c[kTileE];
+        if (vec && j0 + kTileE <= m) {
+            const uint4 *c4 = reinterpret_cast<const uint4 *>(col + j0);
+#pragma unroll
+            for (int q = 0; q < kTileE / 4; ++q) {
+                const uint4 x = __ldg(c4 + q);
+                c[4 * q] = x.x;
+                c[4 * q + 1] = x.y;
+                c[4 * q + 2] = x.z;
+                c[4 * q + 3] = x.w;
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < kTileE; ++k)
+                c[k] = j0 + k < m ? __ldg(col + j0 + k) : 0u;
+        }
+        /* the entry before j0: the previous lane's last, or a load */
+        uint32_t prev = __shfl_up_sync(0xffffffffu, c[kTileE - 1], 1);
+        if (lane == 0)
+            prev = (j0 > 0 && j0 <= m) ? __ldg(col + j0 - 1) : 0u;
+        if (j0 < m) {
+            const uint32_t sb = __ldg(starts + (j0 >> 5)) >> (j0 & 31); /* j0 % 16 == 0 */
+            const int kv = m - j0 < (uint64_t)kTileE ? (int)(m - j0) : kTileE;
+#pragma unroll
+            for (int k = 0; k < kTileE; ++k) {
+                if (k < kv && !((sb >> k) & 1u)) {
+                    desc |= c[k] < prev;
+                    dup |= c[k] == prev;
+                }
+                prev = c[k];
+            }
+        }
+    }
+    if (__any_sync(0xffffffffu, desc) && lane == 0)
+        atomicOr(flags, 1u);
+    if (__any_sync(0xffffffffu, dup) && lane == 0)
+        atomicOr(flags + 1, 1u);
+}
+
+/* Partition offsets of every (ascending) row: roff[v*P + q-1] = entries of
+ * row v below bounds[q], q = 1..P (bounds[P] = n, so the last is the count
+ * of valid ids).  All P lower bounds of a row advance together (branchless
+ * binary search, one power-of-two step per round), so their loads are
+ * independent.  lb/le: v's own run (its local entries); local_total sums
+ * them. */
+template <int PMAX>
+__global__ void __launch_bounds__(kB) k_row_ranges(const uint64_t *__restrict__ row_ptr,
+                                                   const uint32_t *__restrict__ col, uint32_t n,
+                                                   uint64_t m, const uint32_t *bounds, int parts,
+                                                   uint32_t *roff, uint64_t *lb, uint64_t *le,
+                                                   unsigned long long *local_total)
+{
+    __shared__ uint32_t s_b[PMAX + 1];
+    for (int i = threadIdx.x; i <= PMAX; i += kB)
+        s_b[i] = i <= parts ? bounds[i] : 0xffffffffu;
+    __syncthreads();
+    uint32_t tb[PMAX + 1];
+#pragma unroll
+    for (int i = 0; i <= PMAX; ++i)
+        tb[i] = s_b[i];
+    const uint64_t stride = (uint64_t)gridDim.x * kB;
+    unsigned long long local = 0;
+    for (uint64_t v = (uint64_t)blockIdx.x * kB + threadIdx.x; v < n; v += stride) {
+        uint64_t b = __ldg(row_ptr + v), e = __ldg(row_ptr + v + 1);
+        e = e > m ? m : e;
+        b = b > e ? e : b;
+        const uint64_t len = e - b;
+        int p = 0;
+#pragma unroll
+        for (int i = 1; i < PMAX; ++i)
+            p += (int)((uint32_t)v >= tb[i]);
+        uint64_t pos[PMAX];
+#pragma unroll
+        for (int q = 0; q < PMAX; ++q)
+            pos[q] = 0;
+        if (len) {
+            const uint32_t first = __ldg(col + b), last = __ldg(col + e - 1);
+            bool open[PMAX], any = false;
+#pragma unroll
+            for (int q = 0; q < PMAX; ++q) {
+                const uint32_t t = tb[q + 1];
+                open[q] = q < parts && first < t && last >= t;
+                pos[q] = (q < parts && last < t) ? len : 0;
+                any |= open[q];
+            }
+            uint64_t step = any ? 1ull << (63 - __clzll((long long)len)) : 0ull;
+            for (; step; step >>= 1) {
+#pragma unroll
+                for (int q = 0; q < PMAX; ++q)
+                    if (open[q] && pos[q] + step <= len &&
+                        __ldg(col + b + pos[q] + step - 1) < tb[q + 1])
+                        pos[q] += step;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < PMAX; ++q)
+            if (q < parts)
+                roff[v * (uint64_t)parts + q] = (uint32_t)pos[q];
+        uint64_t lo = 0, hi = 0;
+#pragma unroll
+        for (int q = 0; q < PMAX; ++q) {
+            if (q + 1 == p)
+                lo = pos[q];
+            if (q == p)
+                hi = pos[q];
+        }
+        lb[v] = b + lo;
+        le[v] = b + hi;
+        local += hi - lo;
+    }
+    for (int o = 16; o > 0; o >>= 1)
+        local += __shfl_xor_sync(0xffffffffu, local, o);
+    if ((threadIdx.x & 31) == 0 && local)
+        atomicAdd(local_total, local);
+}
+
+/* True when some entry of [s, e) has no mirror mark. */
+__device__ __forceinline__ bool any_unmarked(const uint32_t *__restrict__ ngbits, uint64_t s,
+                                             uint64_t e)
+{
+    for (uint64_t w = s >> 5; w <= (e - 1) >> 5; ++w) {
+        uint32_t mask = 0xffffffffu;
+        if (w == s >> 5)
+            mask &= 0xffffffffu << (s & 31);
+        if (w == (e - 1) >> 5)
+            mask &= 0xffffffffu >> (31 - ((e - 1) & 31));
+        if (~__ldg(ngbits + w) & mask)
+            return true;
+    }
+    return false;
+}
+
+/* Sorted-row mode, remote end, from the partition offsets: row u's run in
+ * partition q != u's own sets bit q of pmask[u] when it holds an unmarked
+ * entry (a neighbour in q's giant tree; marked ones had their keys written
+ * by the local end, k_ng_*).  The thread owning row u stores pmask[u]
+ * whole.  The raw cut count takes every valid entry outside u's own run. */
+template <int PMAX>
+__global__ void __launch_bounds__(kB) k_emit_ranges(EmitParams E)
+{
+    __shared__ uint32_t s_b[PMAX + 1];
+    for (int i = threadIdx.x; i <= PMAX; i += kB)
+        s_b[i] = i <= E.parts ? E.bounds[i] : 0xffffffffu;
+    __syncthreads();
+    const int P = E.parts;
+    const uint64_t stride = (uint64_t)gridDim.x * kB;
+    unsigned long long raw = 0;
+    for (uint64_t u = (uint64_t)blockIdx.x * kB + threadIdx.x; u < E.n; u += stride) {
+        const uint64_t b = __ldg(E.row_ptr + u);
+        int p = 0;
+#pragma unroll
+        for (int i = 1; i < PMAX; ++i)
+            p += (int)((uint32_t)u >= s_b[i]);
+        uint32_t o[PMAX + 1];
+        o[0] = 0;
+#pragma unroll
+        for (int q = 0; q < PMAX; ++q)
+            o[q + 1] = q < P ? __ldg(E.roff + u * (uint64_t)P + q) : 0u;
+        uint32_t bits = 0, own = 0;
+#pragma unroll
+        for (int q = 0; q < PMAX; ++q) {
+            if (q >= P || o[q + 1] <= o[q])
+                continue;
+            if (q == p) {
+                own = o[q + 1] - o[q];
+                continue;
+            }
+            if (any_unmarked(E.ngbits, b + o[q], b + o[q + 1]))
+                bits |= 1u << q;
+        }
+        raw += (uint64_t)(o[P < PMAX ? P : PMAX] - own);
+        E.pmask[u] = bits;
+    }
+    for (int off = 16; off > 0; off >>= 1)
+        raw += __shfl_xor_sync(0xffffffffu, raw, off);
+    if ((threadIdx.x & 31) == 0 && raw)
+        atomicAdd(E.raw, raw);
+}
+
 /* Boundary pairs from the remote end over one column tile per block
  * iteration (the gather pass, used when rows are not strictly ascending or
  * the giant masks are off): each cut entry gathers its giant flag; giant
@@ -670,9 +904,16 @@ __device__ __forceinline__ uint64_t find_sorted(const uint32_t *col, uint64_t lo
     return l < hi - 1 && __ldg(col + l) == v ? l : kNone;
 }
 
+/* Marks the mirror entry v of row u for every plain key (u, v) of the
+ * local end.  With partition offsets the search covers only row u's run in
+ * v's partition. */
 __global__ void __launch_bounds__(kB) k_ng_mark(EmitParams E, const uint64_t *work,
                                                 const uint64_t *total)
 {
+    __shared__ uint32_t s_b[CCGPU_MAX_PARTS + 1];
+    for (int i = threadIdx.x; i <= E.parts; i += kB)
+        s_b[i] = E.bounds[i];
+    __syncthreads();
     const uint64_t items = *total;
     const uint64_t stride = (uint64_t)gridDim.x * kB;
     bool missing = false;
@@ -682,6 +923,12 @@ __global__ void __launch_bounds__(kB) k_ng_mark(EmitParams E, const uint64_t *wo
         uint64_t lo = __ldg(E.row_ptr + u), hi = __ldg(E.row_ptr + u + 1);
         hi = hi > E.m ? E.m : hi;
         lo = lo > hi ? hi : lo;
+        if (E.roff) {
+            const int pv = part_of(s_b, E.parts, v);
+            const uint64_t base = lo;
+            hi = base + __ldg(E.roff + (uint64_t)u * E.parts + pv);
+            lo = base + (pv ? __ldg(E.roff + (uint64_t)u * E.parts + pv - 1) : 0u);
+        }
         const uint64_t pos = find_sorted(E.col, lo, hi, v);
         if (pos != ~0ull)
             atomicOr(E.ngbits + (pos >> 5), 1u << (pos & 31));
@@ -1326,17 +1573,17 @@ struct MergeParams {
     uint64_t ghosts;
     const uint64_t *gh_off;       /* [parts+1] */
     const uint64_t *seg;          /* [parts*(parts+1)] */
-    uint64_t *msg;                /* [ghosts] */
-    uint32_t *msg_count;          /* [parts*parts], [q*parts+p] */
+    uint32_t *delta;              /* [ghosts] ghosts whose label an exchange lowered */
+    uint32_t *delta_count;        /* entries of delta in the current exchange */
     int *changed;                 /* [parts] */
     unsigned long long *sent;
     uint32_t *ghost_rep;          /* [ghosts] local rep of each ghost vertex */
-    int ghost_rep_ready;          /* 0: k_pack fills ghost_rep from label[] */
+    int ghost_rep_ready;          /* 0: k_exchange fills ghost_rep from label[] */
 };
 
 /* An exchange lowers the hook minima by one pass over every pair (pull)
- * when it carries more than one message per 8 pairs; below that, the
- * receiver walks the pairs of each received ghost (push). */
+ * when it changes more than one ghost label per 8 pairs; below that, the
+ * pairs of each changed ghost are walked (push). */
 __device__ __forceinline__ bool pull_hooks(const MergeParams &M, uint64_t messages)
 {
     return messages * 8 > M.pairs;
@@ -1407,170 +1654,90 @@ __global__ void __launch_bounds__(kB) k_upd(MergeParams M)
     }
 }
 
-/* Delta exchange, sender side (src/exchange_plan.c:325-357): for every
- * ghost g of partition p owned by q, q's current label of the ghost vertex
- * goes out when it fell below what q sent last time; it is written as
- * (position in the need-from range, label) into the (q -> p) region. */
-__global__ void __launch_bounds__(kB) k_pack(MergeParams M)
+/* Delta exchange (src/exchange_plan.c:242-425) on one device.  The
+ * reference's (owner q -> reader p) message region is p's need-from range
+ * for q, which is the index range of p's ghosts owned by q, so a message's
+ * slot at the reader is its ghost.  One pass therefore does the sender's
+ * pack and the reader's scatter: for every ghost g whose owner's current
+ * label fell below what was last sent (prev_sent, ~0 before the first
+ * exchange) the label goes straight into ghost_labels[g], and g is appended
+ * to the exchange's delta list - the in-HBM compaction of the changed
+ * boundary labels - with one slot reservation per block.  The delta list
+ * drives the hook update (k_delta_push) and its length is the reference's
+ * count of sent pairs. */
+__global__ void __launch_bounds__(kB) k_exchange(MergeParams M)
 {
-    __shared__ uint32_t s_b[CCGPU_MAX_PARTS + 1];
-    __shared__ uint64_t s_gh[CCGPU_MAX_PARTS + 1];
-    for (int i = threadIdx.x; i <= M.parts; i += kB) {
-        s_b[i] = M.bounds[i];
-        s_gh[i] = M.gh_off[i];
-    }
-    __syncthreads();
-    const int lane = threadIdx.x & 31;
+    __shared__ uint32_t s_wcnt[kB / 32];
+    __shared__ uint32_t s_base;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint64_t stride = (uint64_t)gridDim.x * kB;
     for (uint64_t base = (uint64_t)blockIdx.x * kB; base < M.ghosts; base += stride) {
-        uint64_t g = base + threadIdx.x;
+        const uint64_t g = base + threadIdx.x;
         bool send = false;
-        uint32_t lbl = 0, region = 0xffffffffu;
-        uint64_t rstart = 0;
         if (g < M.ghosts) {
-            uint32_t u = __ldg(M.ghost_v + g);
-            int q = part_of(s_b, M.parts, u);
-            int lo = 0, hi = M.parts; /* partition p whose ghost range holds g */
-            while (hi - lo > 1) {
-                int mid = (lo + hi) >> 1;
-                if (s_gh[mid] <= g)
-                    lo = mid;
-                else
-                    hi = mid;
-            }
-            int p = lo;
             uint32_t rep;
             if (M.ghost_rep_ready) {
                 rep = __ldg(M.ghost_rep + g);
             } else {
-                rep = __ldg(M.label + u); /* fixed by the local solve */
+                rep = __ldg(M.label + __ldg(M.ghost_v + g)); /* fixed by the local solve */
                 M.ghost_rep[g] = rep;
             }
-            lbl = M.cur[rep];
+            const uint32_t lbl = M.cur[rep];
             if (lbl < M.prev_sent[g]) {
                 M.prev_sent[g] = lbl;
-                send = true;
-                region = (uint32_t)(q * M.parts + p);
-                rstart = M.seg[(uint64_t)p * (M.parts + 1) + q];
-            }
-        }
-        unsigned peers = __match_any_sync(0xffffffffu, region);
-        uint32_t slot = 0;
-        if (send && (__ffs(peers) - 1) == lane)
-            slot = atomicAdd(M.msg_count + region, (uint32_t)__popc(peers));
-        slot = __shfl_sync(peers, slot, __ffs(peers) - 1);
-        if (send) {
-            slot += __popc(peers & ((1u << lane) - 1u));
-            M.msg[rstart + slot] = ((uint64_t)(g - rstart) << 32) | lbl;
-        }
-    }
-}
-
-/* Receiver side (src/exchange_plan.c:390-413): ghost_labels[pos] = label,
- * and the hook minimum of every rep paired with that ghost is lowered. */
-__global__ void __launch_bounds__(kB) k_scatter(MergeParams M)
-{
-    const int lane = threadIdx.x & 31;
-    const uint64_t stride = (uint64_t)gridDim.x * kB;
-    const int regions = M.parts * M.parts;
-    for (uint64_t base = (uint64_t)blockIdx.x * kB; base < M.ghosts; base += stride) {
-        const uint64_t s = base + threadIdx.x;
-        bool has = false;
-        uint64_t g = 0;
-        uint32_t lbl = 0;
-        if (s < M.ghosts) {
-            /* region (p, q) holding slot s: seg is ascending in p-major order */
-            int lo = 0, hi = regions;
-            while (hi - lo > 1) {
-                int mid = (lo + hi) >> 1;
-                int p = mid / M.parts, q = mid % M.parts;
-                if (M.seg[(uint64_t)p * (M.parts + 1) + q] <= s)
-                    lo = mid;
-                else
-                    hi = mid;
-            }
-            int p = lo / M.parts, q = lo % M.parts;
-            uint64_t rstart = M.seg[(uint64_t)p * (M.parts + 1) + q];
-            if (s - rstart < M.msg_count[q * M.parts + p]) {
-                uint64_t pr = M.msg[s];
-                g = rstart + (pr >> 32);
-                lbl = (uint32_t)pr;
                 M.ghost_labels[g] = lbl;
-                has = true;
+                send = true;
             }
         }
-        unsigned got = __popc(__ballot_sync(0xffffffffu, has));
-        if (lane == 0 && got)
-            atomicAdd(M.sent, (unsigned long long)got);
-        if (!has)
-            continue;
-        /* hook values only decrease: a plain read, even a stale one, that is
-         * already <= lbl means the atomicMin would change nothing */
-        for (uint64_t k = M.ghost_pairs[g]; k < M.ghost_pairs[g + 1]; ++k) {
-            uint32_t r = M.pair_rep[k];
-            if (lbl < M.hook[r])
-                atomicMin(M.hook + r, lbl);
+        const unsigned bal = __ballot_sync(0xffffffffu, send);
+        if (lane == 0)
+            s_wcnt[warp] = __popc(bal);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t acc = 0;
+            for (int w = 0; w < kB / 32; ++w) {
+                const uint32_t c = s_wcnt[w];
+                s_wcnt[w] = acc;
+                acc += c;
+            }
+            s_base = acc ? atomicAdd(M.delta_count, acc) : 0u;
+            if (acc)
+                atomicAdd(M.sent, (unsigned long long)acc);
         }
+        __syncthreads();
+        if (send)
+            M.delta[s_base + s_wcnt[warp] + __popc(bal & ((1u << lane) - 1u))] = (uint32_t)g;
+        __syncthreads(); /* s_wcnt / s_base are rewritten by the next tile */
     }
 }
 
-/* Receiver side over the sent messages only, for up to 16 partitions: the
- * (q -> p) region holds msg_count[q*P+p] messages from its start, so a
- * block scans the P*P counts in shared memory and walks the flattened
- * message index; ghost_labels and the hook minima are updated as in
- * k_scatter. */
-constexpr int kSmallParts = 16;
-
-__global__ void __launch_bounds__(kB) k_scatter_sent(MergeParams M)
+/* Hook update of an exchange with few changed ghosts (push side): every
+ * ghost on the delta list lowers the hook minimum of each rep it is paired
+ * with (its pairs are contiguous, [ghost_pairs[g], ghost_pairs[g+1])).
+ * One ghost per lane, one pair per lane per step: lanes whose pairs share a
+ * rep (most cut pairs of a partition carry its giant rep) combine their
+ * labels first and one of them issues the atomicMin.  Hook values only
+ * decrease, so a plain read that is already <= the minimum means the atomic
+ * would change nothing.  Does nothing when the exchange takes the pull
+ * side. */
+__global__ void __launch_bounds__(kB) k_delta_push(MergeParams M)
 {
-    __shared__ uint64_t s_seg[kSmallParts * kSmallParts];   /* region start, p-major */
-    __shared__ uint32_t s_pre[kSmallParts * kSmallParts + 1]; /* messages before region */
-    const int P = M.parts, R = P * P;
-    if (threadIdx.x == 0) {
-        uint32_t acc = 0;
-        for (int r = 0; r < R; ++r) {
-            const int p = r / P, q = r % P;
-            s_seg[r] = M.seg[(uint64_t)p * (P + 1) + q];
-            s_pre[r] = acc;
-            acc += M.msg_count[q * P + p];
-        }
-        s_pre[R] = acc;
-    }
-    __syncthreads();
-    const uint32_t total = s_pre[R];
-    const bool push = !pull_hooks(M, total);
+    const uint32_t total = *M.delta_count;
+    if (pull_hooks(M, total))
+        return;
     const int lane = threadIdx.x & 31;
     const uint64_t stride = (uint64_t)gridDim.x * kB;
     for (uint64_t base = (uint64_t)blockIdx.x * kB; base < total; base += stride) {
         const uint64_t i = base + threadIdx.x;
-        const bool has = i < total;
         uint64_t k0 = 0, k1 = 0;
         uint32_t lbl = 0;
-        if (has) {
-            int lo = 0, hi = R; /* last region with s_pre <= i */
-            while (hi - lo > 1) {
-                const int mid = (lo + hi) >> 1;
-                if (s_pre[mid] <= i)
-                    lo = mid;
-                else
-                    hi = mid;
-            }
-            const uint64_t rstart = s_seg[lo];
-            const uint64_t pr = M.msg[rstart + (i - s_pre[lo])];
-            const uint64_t g = rstart + (pr >> 32);
-            lbl = (uint32_t)pr;
-            M.ghost_labels[g] = lbl;
-            if (push) {
-                k0 = M.ghost_pairs[g];
-                k1 = M.ghost_pairs[g + 1];
-            }
+        if (i < total) {
+            const uint32_t g = M.delta[i];
+            lbl = M.ghost_labels[g];
+            k0 = M.ghost_pairs[g];
+            k1 = M.ghost_pairs[g + 1];
         }
-        /* hook minima, one pair per lane per step: lanes whose pairs share a
-         * rep (most cut pairs of a partition carry its giant rep) combine
-         * their labels first and one of them issues the atomicMin.  Hook
-         * values only decrease, so a plain read that is already <= the
-         * minimum means the atomic would change nothing. */
-        uint64_t nk = k1 - k0;
+        const uint64_t nk = k1 - k0;
         uint64_t steps = nk;
         for (int o = 16; o > 0; o >>= 1) {
             const uint64_t y = __shfl_xor_sync(0xffffffffu, steps, o);
@@ -1584,28 +1751,17 @@ __global__ void __launch_bounds__(kB) k_scatter_sent(MergeParams M)
             if (act && (__ffs(peers) - 1) == lane && mn < M.hook[r])
                 atomicMin(M.hook + r, mn);
         }
-        const unsigned got = __popc(__ballot_sync(0xffffffffu, has));
-        if (lane == 0 && got)
-            atomicAdd(M.sent, (unsigned long long)got);
     }
 }
 
-/* Pull side of an exchange with many messages: after k_scatter_sent wrote
- * the received ghost labels, one pass over every pair lowers the hook
- * minima.  Ghost labels only decrease and hook[r] already bounds the old
- * labels of r's ghosts, so the minima equal the push side's.  Does nothing
- * when the exchange used the push side. */
+/* Hook update of an exchange with many changed ghosts (pull side): after
+ * k_exchange wrote the new ghost labels, one pass over every pair lowers
+ * the hook minima.  Ghost labels only decrease and hook[r] already bounds
+ * the old labels of r's ghosts, so the minima equal the push side's.  Does
+ * nothing when the exchange takes the push side. */
 __global__ void __launch_bounds__(kB) k_hook_pull(MergeParams M)
 {
-    __shared__ uint64_t s_total;
-    if (threadIdx.x == 0) {
-        uint64_t t = 0;
-        for (int r = 0; r < M.parts * M.parts; ++r)
-            t += M.msg_count[r];
-        s_total = t;
-    }
-    __syncthreads();
-    if (!pull_hooks(M, s_total))
+    if (!pull_hooks(M, *M.delta_count))
         return;
     const int lane = threadIdx.x & 31;
     const uint64_t stride = (uint64_t)gridDim.x * kB;
@@ -1747,200 +1903,285 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
             max_local = hb[p + 1] - hb[p];
     CC_TRY(clock_mark(clk, st)); /* 1 */
 
-    /* 2. local CSR of every partition, then local CC on it */
+    /* 2. local subgraph of every partition, then local CC on it.
+     * Ranges mode (2 to 8 partitions): the row order is checked in one
+     * streaming pass and each row's partition runs are found in place; the
+     * local CC reads every row's own run.  If some row turns out to descend
+     * (known after step 3), steps 2-3 run again with the local CSR built
+     * (count + fill), as they do for more partitions. */
     uint32_t *label = nullptr;
     CC_TRY(cc_bufs_get(&B, (void **)&label, (size_t)n * sizeof(uint32_t)));
-    const uint64_t *l_rp = d_row_ptr;
-    const uint32_t *l_col = d_col;
-    uint64_t l_m = m;
-    uint32_t *tile_first = nullptr, *wt_first = nullptr;
-    uint64_t col_tiles = 0, wtiles = 0;
-    if (P > 1 && m > 0) {
-        LocalParams Lp;
-        Lp.row_ptr = d_row_ptr;
-        Lp.col = d_col;
-        Lp.vec = ((uintptr_t)d_col & 15) == 0;
-        Lp.n = n;
-        Lp.m = m;
-        Lp.bounds = bounds;
-        Lp.parts = P;
-        Lp.tiles = (m + kTile - 1) / kTile;
-        uint64_t *pcol = nullptr, *tile_off = nullptr;
-        CC_TRY(cc_bufs_get(&B, (void **)&pcol, (P + 1) * sizeof(uint64_t)));
-        CC_TRY(cc_bufs_get(&B, (void **)&Lp.tile_cnt, Lp.tiles * sizeof(uint32_t)));
-        CC_TRY(cc_bufs_get(&B, (void **)&tile_off, (Lp.tiles + 1) * sizeof(uint64_t)));
-        CC_TRY(cc_bufs_get(&B, (void **)&Lp.tile_first, (Lp.tiles + 1) * sizeof(uint32_t)));
-        CC_TRY(cc_bufs_get(&B, (void **)&Lp.lrp, ((size_t)n + 1) * sizeof(uint64_t)));
-        CC_KLAUNCH(ctx, CCK_DIST_TILES, k_part_cols, 1, 32, 0, st, d_row_ptr, m, bounds, P, pcol);
-        Lp.pcol = pcol;
-        Lp.tile_off = tile_off;
-        Lp.lcol = nullptr;
-        const unsigned tb = cc_blocks(Lp.tiles, 1, (unsigned)ctx->sm_count * 8);
-        CC_KLAUNCH(ctx, CCK_DIST_LOCAL_COUNT, k_local_count, tb, kB, 0, st, Lp);
-        const unsigned vb = cc_blocks((uint64_t)n + 1, kB, (unsigned)ctx->sm_count * 8);
-        CC_KLAUNCH(ctx, CCK_DIST_TILES, k_tile_first, vb, kB, 0, st, Lp, (uint64_t)kTile, Lp.tiles,
-                   Lp.tile_first);
-        wtiles = (m + kWarpTile - 1) / kWarpTile;
-        CC_TRY(cc_bufs_get(&B, (void **)&wt_first, (wtiles + 1) * sizeof(uint32_t)));
-        CC_KLAUNCH(ctx, CCK_DIST_TILES, k_tile_first, vb, kB, 0, st, Lp, (uint64_t)kWarpTile,
-                   wtiles, wt_first);
-        CC_TRY(cc_scan_u32(ctx, Lp.tile_cnt, tile_off, Lp.tiles, &B, st));
-        CC_CUDA(cudaMemcpyAsync(&l_m, tile_off + Lp.tiles, sizeof(uint64_t),
-                                cudaMemcpyDeviceToHost, st));
-        CC_CUDA(cudaStreamSynchronize(st));
-        CC_TRY(cc_bufs_get(&B, (void **)&Lp.lcol, (size_t)(l_m ? l_m : 1) * sizeof(uint32_t)));
-        CC_KLAUNCH(ctx, CCK_DIST_LOCAL_FILL, k_local_fill, tb, kB, 0, st, Lp);
-        l_rp = Lp.lrp;
-        l_col = Lp.lcol;
-        tile_first = Lp.tile_first;
-        col_tiles = Lp.tiles;
-    }
-    LocalCCArgs a = {l_rp, l_col, n, l_m, label, seg64, (uint32_t)P, {}, 0, 1};
     ccgpu_cc_opts lo;
     ccgpu_cc_opts_default(&lo);
     lo.chunk_size = o.chunk_size;
-    CC_TRY(cc_local_resolve_opts(&lo, &a.o));
+    ccgpu_cc_opts ro;
+    CC_TRY(cc_local_resolve_opts(&lo, &ro));
+    const bool use_mask = P > 1 && P <= 32 && ro.sample_rounds > 0 && ro.skip_giant;
+    bool ranges = use_mask && P <= 8 && m > 0;
+    LocalParams Lp;
+    Lp.row_ptr = d_row_ptr;
+    Lp.col = d_col;
+    Lp.vec = ((uintptr_t)d_col & 15) == 0;
+    Lp.n = n;
+    Lp.m = m;
+    Lp.bounds = bounds;
+    Lp.parts = P;
+    Lp.tiles = (m + kTile - 1) / kTile;
+    const unsigned vb = cc_blocks((uint64_t)n + 1, kB, (unsigned)ctx->sm_count * 8);
+    uint32_t *tile_first = nullptr, *wt_first = nullptr;
+    uint64_t col_tiles = 0, wtiles = 0;
+    /* first row starting after each column tile's first entry (the gather
+     * pass and the local CSR build) */
+    auto tiles_of = [&]() -> int {
+        if (tile_first || !(P > 1 && m > 0))
+            return CCGPU_OK;
+        CC_TRY(cc_bufs_get(&B, (void **)&tile_first, (Lp.tiles + 1) * sizeof(uint32_t)));
+        CC_KLAUNCH(ctx, CCK_DIST_TILES, k_tile_first, vb, kB, 0, st, Lp, (uint64_t)kTile, Lp.tiles,
+                   tile_first);
+        col_tiles = Lp.tiles;
+        return CCGPU_OK;
+    };
+    uint64_t l_m = m;
+    unsigned *rflags = nullptr;                     /* [0] a row descends, [1] repeats */
+    unsigned long long *local_total = nullptr;
+    uint32_t *roff = nullptr;
+    uint64_t *rlb = nullptr, *rle = nullptr;
     LocalCCScratch ls;
-    {
-        cc_carve c = {nullptr, 0};
-        cc_local_carve(&c, &ls, a);
-        void *base = nullptr;
-        CC_TRY(cc_bufs_get(&B, &base, c.off));
-        c = {(char *)base, 0};
-        cc_local_carve(&c, &ls, a);
-    }
-    CC_TRY(cc_local_run(ctx, a, ls, st, 0, 0));
-    CC_TRY(clock_mark(clk, st)); /* 2 */
-
-    /* 3. reps and boundary keys */
-    const int rb = bits_for(max_local - 1 ? max_local - 1 : 1);
-    const int gb = bits_for(n - 1 ? n - 1 : 1);
-    const int pb = P > 1 ? bits_for((uint64_t)P - 1) : 0;
-    if (rb + gb + pb > 64)
-        return ccgpu_set_error(CCGPU_ERR_LIMIT, "boundary key needs %d bits", rb + gb + pb);
     uint32_t *rep_list = nullptr, *cur = nullptr, *nxt = nullptr, *hook = nullptr;
-    unsigned long long *counters = nullptr; /* [0] keys [1] reps [2] roots [3] sent [4] raw [5] active reps */
+    unsigned long long *counters = nullptr; /* [0] keys [1] reps [2] roots [3] sent [4] raw [5] active reps [6] bad */
     CC_TRY(cc_bufs_get(&B, (void **)&rep_list, (size_t)n * sizeof(uint32_t)));
     CC_TRY(cc_bufs_get(&B, (void **)&cur, (size_t)n * sizeof(uint32_t)));
     CC_TRY(cc_bufs_get(&B, (void **)&nxt, (size_t)n * sizeof(uint32_t)));
     CC_TRY(cc_bufs_get(&B, (void **)&hook, (size_t)n * sizeof(uint32_t)));
     CC_TRY(cc_bufs_get(&B, (void **)&counters, 8 * sizeof(unsigned long long)));
-    CC_CUDA(cudaMemsetAsync(counters, 0, 8 * sizeof(unsigned long long), st));
-    const unsigned sb = cc_blocks(n, kB, (unsigned)ctx->sm_count * 8);
-    CC_KLAUNCH(ctx, CCK_DIST_REPS, k_reps, sb, kB, 0, st, label, n, rep_list, counters + 1, cur,
-               nxt, hook);
+    CC_TRY(cc_bufs_get(&B, (void **)&rflags, 2 * sizeof(unsigned)));
     uint64_t *keys = nullptr, *alt = nullptr;
     CC_TRY(cc_bufs_get(&B, (void **)&keys, (size_t)(m ? m : 1) * sizeof(uint64_t)));
+    const int rb = bits_for(max_local - 1 ? max_local - 1 : 1);
+    const int gb = bits_for(n - 1 ? n - 1 : 1);
+    const int pb = P > 1 ? bits_for((uint64_t)P - 1) : 0;
+    if (rb + gb + pb > 64)
+        return ccgpu_set_error(CCGPU_ERR_LIMIT, "boundary key needs %d bits", rb + gb + pb);
+    const unsigned sb = cc_blocks(n, kB, (unsigned)ctx->sm_count * 8);
     EmitParams E;
-    E.row_ptr = d_row_ptr;
-    E.col = d_col;
-    E.vec = ((uintptr_t)d_col & 15) == 0;
-    E.label = label;
-    E.bounds = bounds;
-    E.n = n;
-    E.m = m;
-    E.parts = P;
-    E.rb = rb;
-    E.gb = gb;
-    E.out = keys;
-    E.count = counters;
-    E.tiles = col_tiles;
-    E.tile_first = tile_first;
-    E.raw = counters + 4;
-    /* giant flags and per-vertex partition masks (P <= 32) */
-    E.gflag = nullptr;
-    E.pmask = nullptr;
-    E.giants = nullptr;
-    const bool use_mask = P > 1 && P <= 32 && a.o.sample_rounds > 0 && a.o.skip_giant;
-    if (use_mask) {
-        CC_TRY(cc_bufs_get(&B, (void **)&E.gflag, (((size_t)n + 31) / 32) * 4));
-        CC_TRY(cc_bufs_get(&B, (void **)&E.pmask, (size_t)n * 4));
-        CC_CUDA(cudaMemsetAsync(E.pmask, 0, (size_t)n * 4, st));
-        E.giants = ls.giants;
-        CC_KLAUNCH(ctx, CCK_DIST_GFLAG, k_giant_flags,
-                   cc_blocks(n, kB, (unsigned)ctx->sm_count * 8), kB, 0, st, E);
-    }
-    /* Sorted-row mode (giant masks on): the local end writes the plain keys
-     * and marks their mirror entries, the remote end reads the marks
-     * instead of gathering gflag.  Both passes check that rows are strictly
-     * ascending and symmetric; if not, the pairs are made again by the
-     * gather pass alone. */
-    E.ngbits = nullptr;
-    E.bad = counters + 6;
-    const bool sorted_mode = use_mask && P > 1 && P < 32 && col_tiles > 0;
-    auto emit = [&]() -> int {
-        const unsigned eb = cc_blocks(col_tiles, 1, (unsigned)ctx->sm_count * 4);
-        const unsigned lb = cc_blocks(n, kB, (unsigned)ctx->sm_count * 8);
-        if (E.ngbits) {
-            uint32_t *cnt = nullptr;
-            uint64_t *off = nullptr, *work = nullptr;
-            CC_TRY(cc_bufs_get(&B, (void **)&cnt, (size_t)n * sizeof(uint32_t)));
-            CC_TRY(cc_bufs_get(&B, (void **)&off, ((size_t)n + 1) * sizeof(uint64_t)));
-            if (P <= 4)
-                CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_count<4>, lb, kB, 0, st, E, cnt);
-            else if (P <= 8)
-                CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_count<8>, lb, kB, 0, st, E, cnt);
-            else
-                CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_count<CCGPU_MAX_PARTS>, lb, kB, 0, st,
-                           E, cnt);
-            CC_TRY(cc_scan_u32(ctx, cnt, off, n, &B, st));
-            unsigned long long items = 0;
-            CC_CUDA(cudaMemcpyAsync(&items, off + n, sizeof(items), cudaMemcpyDeviceToHost, st));
-            CC_CUDA(cudaStreamSynchronize(st));
-            CC_TRY(cc_bufs_get(&B, (void **)&work, (size_t)(items ? items : 1) * sizeof(uint64_t)));
-            if (P <= 4)
-                CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_emit<4>, lb, kB, 0, st, E, off, work);
-            else if (P <= 8)
-                CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_emit<8>, lb, kB, 0, st, E, off, work);
-            else
-                CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_emit<CCGPU_MAX_PARTS>, lb, kB, 0, st,
-                           E, off, work);
-            CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_mark, lb, kB, 0, st, E, work, off + n);
-            CC_CUDA(cudaMemcpyAsync(E.count, off + n, sizeof(unsigned long long),
-                                    cudaMemcpyDeviceToDevice, st));
-            const unsigned wb = cc_blocks(wtiles, kW, (unsigned)ctx->sm_count * 8);
-            if (P <= 4)
-                CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit_sorted<4>, wb, kB, 0, st, E, wt_first,
-                           wtiles);
-            else if (P <= 8)
-                CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit_sorted<8>, wb, kB, 0, st, E, wt_first,
-                           wtiles);
-            else
-                CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit_sorted<CCGPU_MAX_PARTS>, wb, kB, 0, st, E,
-                           wt_first, wtiles);
-        } else {
-            if (P <= 4)
-                CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit<4>, eb, kB, 0, st, E);
-            else if (P <= 8)
-                CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit<8>, eb, kB, 0, st, E);
-            else
-                CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit<CCGPU_MAX_PARTS>, eb, kB, 0, st,
-                           E);
-        }
-        return CCGPU_OK;
-    };
-    if (sorted_mode) {
-        const size_t words = (size_t)((m + 31) / 32);
-        CC_TRY(cc_bufs_get(&B, (void **)&E.ngbits, words * 4));
-        CC_CUDA(cudaMemsetAsync(E.ngbits, 0, words * 4, st));
-    }
-    if (P > 1 && col_tiles)
-        CC_TRY(emit());
     unsigned long long hc[7];
-    CC_CUDA(cudaMemcpyAsync(hc, counters, 7 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
-                            st));
-    CC_CUDA(cudaStreamSynchronize(st));
-    if (sorted_mode && hc[6]) {
+    bool sorted_mode = false;
+    for (int pass = 0;; ++pass) {
+        clk.n = 2 < clk.n ? 2 : clk.n; /* a second pass re-records phases 2-3 */
+        const uint64_t *l_rp = d_row_ptr, *l_end = nullptr;
+        const uint32_t *l_col = d_col;
+        l_m = m;
+        CC_CUDA(cudaMemsetAsync(rflags, 0, 2 * sizeof(unsigned), st));
+        if (ranges) {
+            if (!roff) {
+                uint32_t *starts = nullptr;
+                const size_t words = (size_t)((m + 31) / 32);
+                CC_TRY(cc_bufs_get(&B, (void **)&starts, words * 4));
+                CC_TRY(cc_bufs_get(&B, (void **)&roff, (size_t)n * P * sizeof(uint32_t)));
+                CC_TRY(cc_bufs_get(&B, (void **)&rlb, (size_t)n * sizeof(uint64_t)));
+                CC_TRY(cc_bufs_get(&B, (void **)&rle, (size_t)n * sizeof(uint64_t)));
+                CC_TRY(cc_bufs_get(&B, (void **)&local_total, sizeof(unsigned long long)));
+                CC_CUDA(cudaMemsetAsync(starts, 0, words * 4, st));
+                CC_CUDA(cudaMemsetAsync(local_total, 0, sizeof(unsigned long long), st));
+                CC_KLAUNCH(ctx, CCK_DIST_TILES, k_row_starts, sb, kB, 0, st, d_row_ptr, n, m,
+                           starts);
+                const uint64_t groups = (m + kTileE - 1) / kTileE;
+                CC_KLAUNCH(ctx, CCK_DIST_LOCAL_COUNT, k_rows_ascend,
+                           cc_blocks(groups, kB, (unsigned)ctx->sm_count * 8), kB, 0, st, d_col, m,
+                           starts, Lp.vec, rflags);
+                if (P <= 4)
+                    CC_KLAUNCH(ctx, CCK_DIST_LOCAL_FILL, k_row_ranges<4>, sb, kB, 0, st,
+                               d_row_ptr, d_col, n, m, bounds, P, roff, rlb, rle, local_total);
+                else
+                    CC_KLAUNCH(ctx, CCK_DIST_LOCAL_FILL, k_row_ranges<8>, sb, kB, 0, st,
+                               d_row_ptr, d_col, n, m, bounds, P, roff, rlb, rle, local_total);
+            }
+            l_rp = rlb;
+            l_end = rle;
+        } else if (P > 1 && m > 0) {
+            uint64_t *pcol = nullptr, *tile_off = nullptr;
+            CC_TRY(cc_bufs_get(&B, (void **)&pcol, (P + 1) * sizeof(uint64_t)));
+            CC_TRY(cc_bufs_get(&B, (void **)&Lp.tile_cnt, Lp.tiles * sizeof(uint32_t)));
+            CC_TRY(cc_bufs_get(&B, (void **)&tile_off, (Lp.tiles + 1) * sizeof(uint64_t)));
+            CC_TRY(cc_bufs_get(&B, (void **)&Lp.lrp, ((size_t)n + 1) * sizeof(uint64_t)));
+            CC_KLAUNCH(ctx, CCK_DIST_TILES, k_part_cols, 1, 32, 0, st, d_row_ptr, m, bounds, P,
+                       pcol);
+            Lp.pcol = pcol;
+            Lp.tile_off = tile_off;
+            Lp.lcol = nullptr;
+            const unsigned tb = cc_blocks(Lp.tiles, 1, (unsigned)ctx->sm_count * 8);
+            CC_KLAUNCH(ctx, CCK_DIST_LOCAL_COUNT, k_local_count, tb, kB, 0, st, Lp);
+            CC_TRY(tiles_of());
+            Lp.tile_first = tile_first;
+            wtiles = (m + kWarpTile - 1) / kWarpTile;
+            CC_TRY(cc_bufs_get(&B, (void **)&wt_first, (wtiles + 1) * sizeof(uint32_t)));
+            CC_KLAUNCH(ctx, CCK_DIST_TILES, k_tile_first, vb, kB, 0, st, Lp, (uint64_t)kWarpTile,
+                       wtiles, wt_first);
+            CC_TRY(cc_scan_u32(ctx, Lp.tile_cnt, tile_off, Lp.tiles, &B, st));
+            CC_CUDA(cudaMemcpyAsync(&l_m, tile_off + Lp.tiles, sizeof(uint64_t),
+                                    cudaMemcpyDeviceToHost, st));
+            CC_CUDA(cudaStreamSynchronize(st));
+            CC_TRY(cc_bufs_get(&B, (void **)&Lp.lcol,
+                               (size_t)(l_m ? l_m : 1) * sizeof(uint32_t)));
+            CC_KLAUNCH(ctx, CCK_DIST_LOCAL_FILL, k_local_fill, tb, kB, 0, st, Lp);
+            l_rp = Lp.lrp;
+            l_col = Lp.lcol;
+        }
+        LocalCCArgs a = {l_rp, l_col, n, ranges ? m : l_m, label, seg64, (uint32_t)P, ro, 0, 1,
+                         l_end};
+        {
+            cc_carve c = {nullptr, 0};
+            cc_local_carve(&c, &ls, a);
+            void *base = nullptr;
+            CC_TRY(cc_bufs_get(&B, &base, c.off));
+            c = {(char *)base, 0};
+            cc_local_carve(&c, &ls, a);
+        }
+        CC_TRY(cc_local_run(ctx, a, ls, st, 0, 0));
+        CC_TRY(clock_mark(clk, st)); /* 2 */
+
+        /* 3. reps and boundary keys */
+        CC_CUDA(cudaMemsetAsync(counters, 0, 8 * sizeof(unsigned long long), st));
+        CC_KLAUNCH(ctx, CCK_DIST_REPS, k_reps, sb, kB, 0, st, label, n, rep_list, counters + 1,
+                   cur, nxt, hook);
+        E.row_ptr = d_row_ptr;
+        E.col = d_col;
+        E.vec = ((uintptr_t)d_col & 15) == 0;
+        E.label = label;
+        E.bounds = bounds;
+        E.n = n;
+        E.m = m;
+        E.parts = P;
+        E.rb = rb;
+        E.gb = gb;
+        E.out = keys;
+        E.count = counters;
+        E.tiles = col_tiles;
+        E.tile_first = tile_first;
+        E.raw = counters + 4;
+        E.roff = ranges ? roff : nullptr;
+        /* giant flags and per-vertex partition masks (P <= 32) */
+        E.gflag = nullptr;
+        E.pmask = nullptr;
+        E.giants = nullptr;
+        if (use_mask) {
+            CC_TRY(cc_bufs_get(&B, (void **)&E.gflag, (((size_t)n + 31) / 32) * 4));
+            CC_TRY(cc_bufs_get(&B, (void **)&E.pmask, (size_t)n * 4));
+            CC_CUDA(cudaMemsetAsync(E.pmask, 0, (size_t)n * 4, st));
+            E.giants = ls.giants;
+            CC_KLAUNCH(ctx, CCK_DIST_GFLAG, k_giant_flags,
+                       cc_blocks(n, kB, (unsigned)ctx->sm_count * 8), kB, 0, st, E);
+        }
+        /* Sorted-row mode (giant masks on): the local end writes the plain
+         * keys and marks their mirror entries, the remote end reads the
+         * marks instead of gathering gflag - from the partition runs
+         * (k_emit_ranges) or by streaming the columns (k_emit_sorted).  The
+         * rows must be strictly ascending and symmetric: the row check (or
+         * k_emit_sorted) and the mirror search report it, and if not, the
+         * pairs are made again by the gather pass alone. */
         E.ngbits = nullptr;
-        CC_CUDA(cudaMemsetAsync(counters, 0, sizeof(unsigned long long), st));
-        CC_CUDA(cudaMemsetAsync(counters + 4, 0, sizeof(unsigned long long), st));
-        CC_CUDA(cudaMemsetAsync(E.pmask, 0, (size_t)n * 4, st));
-        CC_TRY(emit());
+        E.bad = counters + 6;
+        sorted_mode = use_mask && P > 1 && P < 32 && (ranges || col_tiles > 0);
+        auto emit = [&]() -> int {
+            const unsigned lb = cc_blocks(n, kB, (unsigned)ctx->sm_count * 8);
+            if (E.ngbits) {
+                uint32_t *cnt = nullptr;
+                uint64_t *off = nullptr, *work = nullptr;
+                CC_TRY(cc_bufs_get(&B, (void **)&cnt, (size_t)n * sizeof(uint32_t)));
+                CC_TRY(cc_bufs_get(&B, (void **)&off, ((size_t)n + 1) * sizeof(uint64_t)));
+                if (P <= 4)
+                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_count<4>, lb, kB, 0, st, E, cnt);
+                else if (P <= 8)
+                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_count<8>, lb, kB, 0, st, E, cnt);
+                else
+                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_count<CCGPU_MAX_PARTS>, lb, kB, 0,
+                               st, E, cnt);
+                CC_TRY(cc_scan_u32(ctx, cnt, off, n, &B, st));
+                unsigned long long items = 0;
+                CC_CUDA(cudaMemcpyAsync(&items, off + n, sizeof(items), cudaMemcpyDeviceToHost,
+                                        st));
+                CC_CUDA(cudaStreamSynchronize(st));
+                CC_TRY(cc_bufs_get(&B, (void **)&work,
+                                   (size_t)(items ? items : 1) * sizeof(uint64_t)));
+                if (P <= 4)
+                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_emit<4>, lb, kB, 0, st, E, off,
+                               work);
+                else if (P <= 8)
+                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_emit<8>, lb, kB, 0, st, E, off,
+                               work);
+                else
+                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_emit<CCGPU_MAX_PARTS>, lb, kB, 0,
+                               st, E, off, work);
+                CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_mark, lb, kB, 0, st, E, work, off + n);
+                CC_CUDA(cudaMemcpyAsync(E.count, off + n, sizeof(unsigned long long),
+                                        cudaMemcpyDeviceToDevice, st));
+                if (E.roff) {
+                    if (P <= 4)
+                        CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit_ranges<4>, lb, kB, 0, st, E);
+                    else
+                        CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit_ranges<8>, lb, kB, 0, st, E);
+                } else {
+                    const unsigned wb = cc_blocks(wtiles, kW, (unsigned)ctx->sm_count * 8);
+                    if (P <= 4)
+                        CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit_sorted<4>, wb, kB, 0, st, E,
+                                   wt_first, wtiles);
+                    else if (P <= 8)
+                        CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit_sorted<8>, wb, kB, 0, st, E,
+                                   wt_first, wtiles);
+                    else
+                        CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit_sorted<CCGPU_MAX_PARTS>, wb, kB, 0,
+                                   st, E, wt_first, wtiles);
+                }
+            } else {
+                CC_TRY(tiles_of());
+                E.tiles = col_tiles;
+                E.tile_first = tile_first;
+                const unsigned eb = cc_blocks(col_tiles, 1, (unsigned)ctx->sm_count * 4);
+                if (P <= 4)
+                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit<4>, eb, kB, 0, st, E);
+                else if (P <= 8)
+                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit<8>, eb, kB, 0, st, E);
+                else
+                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit<CCGPU_MAX_PARTS>, eb, kB, 0, st, E);
+            }
+            return CCGPU_OK;
+        };
+        if (sorted_mode) {
+            const size_t words = (size_t)((m + 31) / 32);
+            CC_TRY(cc_bufs_get(&B, (void **)&E.ngbits, words * 4));
+            CC_CUDA(cudaMemsetAsync(E.ngbits, 0, words * 4, st));
+        }
+        if (P > 1 && m > 0)
+            CC_TRY(emit());
+        unsigned hf[2] = {0, 0};
         CC_CUDA(cudaMemcpyAsync(hc, counters, 7 * sizeof(unsigned long long),
                                 cudaMemcpyDeviceToHost, st));
+        CC_CUDA(cudaMemcpyAsync(hf, rflags, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+        if (ranges)
+            CC_CUDA(cudaMemcpyAsync(&l_m, local_total, sizeof(l_m), cudaMemcpyDeviceToHost, st));
         CC_CUDA(cudaStreamSynchronize(st));
+        if (ranges && hf[0]) {
+            /* some row descends: its partition runs are not contiguous */
+            ranges = false;
+            continue;
+        }
+        if (sorted_mode && (hc[6] || hf[1])) {
+            E.ngbits = nullptr;
+            E.roff = nullptr;
+            CC_CUDA(cudaMemsetAsync(counters, 0, sizeof(unsigned long long), st));
+            CC_CUDA(cudaMemsetAsync(counters + 4, 0, sizeof(unsigned long long), st));
+            CC_CUDA(cudaMemsetAsync(counters + 6, 0, sizeof(unsigned long long), st));
+            CC_CUDA(cudaMemsetAsync(E.pmask, 0, (size_t)n * 4, st));
+            CC_TRY(emit());
+            CC_CUDA(cudaMemcpyAsync(hc, counters, 7 * sizeof(unsigned long long),
+                                    cudaMemcpyDeviceToHost, st));
+            CC_CUDA(cudaStreamSynchronize(st));
+            sorted_mode = false;
+        }
+        break;
     }
-    S.sorted_rows = sorted_mode && !hc[6];
+    S.sorted_rows = sorted_mode;
+    S.row_runs = ranges;
     const uint64_t R = hc[0];
     S.boundary_raw = hc[4];
     S.sorted_keys = R;
@@ -2081,12 +2322,11 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
     M.gh_off = gh_off;
     M.seg = segs;
     M.sent = counters + 3;
-    CC_TRY(cc_bufs_get(&B, (void **)&M.msg, (size_t)(G ? G : 1) * sizeof(uint64_t)));
-    CC_TRY(cc_bufs_get(&B, (void **)&M.msg_count, (size_t)P * P * sizeof(uint32_t)));
+    CC_TRY(cc_bufs_get(&B, (void **)&M.delta, (size_t)(G ? G : 1) * sizeof(uint32_t)));
+    CC_TRY(cc_bufs_get(&B, (void **)&M.delta_count, sizeof(uint32_t)));
     CC_TRY(cc_bufs_get(&B, (void **)&M.changed, P * sizeof(int)));
     CC_TRY(cc_bufs_get(&B, (void **)&M.ghost_rep, (size_t)(G ? G : 1) * sizeof(uint32_t)));
     M.ghost_rep_ready = 0;
-    CC_CUDA(cudaMemsetAsync(M.msg_count, 0, (size_t)P * P * sizeof(uint32_t), st));
     const unsigned gbk = (unsigned)ctx->sm_count * 8;
     uint64_t act_count = 0;
     if (U > 0) {
@@ -2144,17 +2384,13 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
         steps++;
         if (steps >= interval || !any_changed) {
             M.cur = pc;
-            CC_KLAUNCH(ctx, CCK_MERGE_EXCH_PACK, k_pack, cc_blocks(G, kB, gbk), kB, 0, st, M);
+            CC_CUDA(cudaMemsetAsync(M.delta_count, 0, sizeof(uint32_t), st));
+            CC_KLAUNCH(ctx, CCK_MERGE_EXCH_PACK, k_exchange, cc_blocks(G, kB, gbk), kB, 0, st, M);
             M.ghost_rep_ready = 1;
-            if (P <= kSmallParts) {
-                CC_KLAUNCH(ctx, CCK_MERGE_EXCH_SCATTER, k_scatter_sent, cc_blocks(G, kB, gbk), kB,
-                           0, st, M);
-                CC_KLAUNCH(ctx, CCK_MERGE_EXCH_PULL, k_hook_pull, cc_blocks(U, kB, gbk), kB, 0,
-                           st, M);
-            } else
-                CC_KLAUNCH(ctx, CCK_MERGE_EXCH_SCATTER, k_scatter, cc_blocks(G, kB, gbk), kB, 0,
-                           st, M);
-            CC_CUDA(cudaMemsetAsync(M.msg_count, 0, (size_t)P * P * sizeof(uint32_t), st));
+            CC_KLAUNCH(ctx, CCK_MERGE_EXCH_SCATTER, k_delta_push, cc_blocks(G, kB, gbk), kB, 0,
+                       st, M);
+            CC_KLAUNCH(ctx, CCK_MERGE_EXCH_PULL, k_hook_pull, cc_blocks(U, kB, gbk), kB, 0, st,
+                       M);
             S.exchanges++;
             for (int p = 0; p < P; ++p)
                 pending[p] = 0;

@@ -42,9 +42,13 @@ struct Rows {
     uint64_t beg, end;
 };
 
-__device__ __forceinline__ Rows row_of(const uint64_t *__restrict__ row_ptr, uint32_t v, uint64_t m)
+/* Row v: [row_ptr[v], row_ptr[v+1]), or [row_ptr[v], row_end[v]) when the
+ * rows are sub-ranges of the column array (row_end given). */
+__device__ __forceinline__ Rows row_of(const uint64_t *__restrict__ row_ptr,
+                                       const uint64_t *__restrict__ row_end, uint32_t v,
+                                       uint64_t m)
 {
-    uint64_t b = __ldg(row_ptr + v), e = __ldg(row_ptr + v + 1);
+    uint64_t b = __ldg(row_ptr + v), e = row_end ? __ldg(row_end + v) : __ldg(row_ptr + v + 1);
     if (e > m)
         e = m;
     if (b > e)
@@ -89,6 +93,7 @@ __device__ __forceinline__ bool in_span(Span sp, uint32_t u)
 __global__ void __launch_bounds__(kBlock) k_init(uint32_t *__restrict__ parent, uint32_t n,
                                                  LocalCCCounters *counters, int vec,
                                                  const uint64_t *__restrict__ row_ptr,
+                                                 const uint64_t *__restrict__ row_end,
                                                  const uint32_t *__restrict__ col, uint64_t m,
                                                  int first_hook, const uint64_t *__restrict__ fseg,
                                                  uint32_t nseg)
@@ -101,7 +106,7 @@ __global__ void __launch_bounds__(kBlock) k_init(uint32_t *__restrict__ parent, 
         /* parent[v] = first neighbour if it is smaller: v is still a root
          * and only this thread writes parent[v], so a plain store hooks it */
         for (uint64_t v = tid; v < n; v += stride) {
-            Rows r = row_of(row_ptr, (uint32_t)v, m);
+            Rows r = row_of(row_ptr, row_end, (uint32_t)v, m);
             uint32_t p = (uint32_t)v;
             if (r.beg < r.end) {
                 uint32_t u = __ldg(col + r.beg);
@@ -130,6 +135,7 @@ __global__ void __launch_bounds__(kBlock) k_init(uint32_t *__restrict__ parent, 
  * first hook done by k_init, entry 0 is skipped when it was smaller. */
 template <bool LAZY>
 __global__ void __launch_bounds__(kBlock) k_sample(const uint64_t *__restrict__ row_ptr,
+                                                   const uint64_t *__restrict__ row_end,
                                                    const uint32_t *__restrict__ col, uint32_t n,
                                                    uint64_t m, uint32_t *parent, uint32_t v_lo,
                                                    uint32_t v_hi, int r0, int r1, int first_done,
@@ -138,7 +144,7 @@ __global__ void __launch_bounds__(kBlock) k_sample(const uint64_t *__restrict__ 
     const uint64_t stride = (uint64_t)gridDim.x * kBlock;
     for (uint64_t v = (uint64_t)v_lo + (uint64_t)blockIdx.x * kBlock + threadIdx.x; v < v_hi;
          v += stride) {
-        Rows r = row_of(row_ptr, (uint32_t)v, m);
+        Rows r = row_of(row_ptr, row_end, (uint32_t)v, m);
         const Span sp = span_of(fseg, nseg, n, v);
         for (int k = r0; k < r1; ++k) {
             uint64_t j = r.beg + (uint64_t)k;
@@ -160,6 +166,7 @@ __global__ void __launch_bounds__(kBlock) k_sample(const uint64_t *__restrict__ 
  * outside the giant tree from its first entry, which restores anything
  * lost. */
 __global__ void __launch_bounds__(kBlock) k_sample_min(const uint64_t *__restrict__ row_ptr,
+                                                       const uint64_t *__restrict__ row_end,
                                                        const uint32_t *__restrict__ col,
                                                        uint32_t n, uint64_t m, uint32_t *parent,
                                                        uint32_t v_lo, uint32_t v_hi, int r0,
@@ -169,7 +176,7 @@ __global__ void __launch_bounds__(kBlock) k_sample_min(const uint64_t *__restric
     const uint64_t stride = (uint64_t)gridDim.x * kBlock;
     for (uint64_t v = (uint64_t)v_lo + (uint64_t)blockIdx.x * kBlock + threadIdx.x; v < v_hi;
          v += stride) {
-        Rows r = row_of(row_ptr, (uint32_t)v, m);
+        Rows r = row_of(row_ptr, row_end, (uint32_t)v, m);
         const Span sp = span_of(fseg, nseg, n, v);
         for (int k = r0; k < r1; ++k) {
             uint64_t j = r.beg + (uint64_t)k;
@@ -190,6 +197,7 @@ __global__ void __launch_bounds__(kBlock) k_sample_min(const uint64_t *__restric
  * and keeps entry 1 in stash[v]; round 1 links v with stash[v] without
  * touching the row.  UINT32_MAX in the stash means no second entry. */
 __global__ void __launch_bounds__(kBlock) k_sample_stash(const uint64_t *__restrict__ row_ptr,
+                                                         const uint64_t *__restrict__ row_end,
                                                          const uint32_t *__restrict__ col,
                                                          uint32_t n, uint64_t m,
                                                          uint32_t *parent, uint32_t *stash,
@@ -199,7 +207,7 @@ __global__ void __launch_bounds__(kBlock) k_sample_stash(const uint64_t *__restr
     for (uint64_t v = (uint64_t)blockIdx.x * kBlock + threadIdx.x; v < n; v += stride) {
         uint32_t u;
         if (round == 0) {
-            Rows r = row_of(row_ptr, (uint32_t)v, m);
+            Rows r = row_of(row_ptr, row_end, (uint32_t)v, m);
             u = r.beg < r.end ? __ldg(col + r.beg) : 0xffffffffu;
             stash[v] = r.beg + 1 < r.end ? __ldg(col + r.beg + 1) : 0xffffffffu;
         } else {
@@ -249,6 +257,7 @@ __global__ void __launch_bounds__(kGiantSamples) k_giant(const uint32_t *parent,
 
 struct LinkParams {
     const uint64_t *row_ptr;
+    const uint64_t *row_end;   /* NULL, or the end of each row (row_of) */
     const uint32_t *col;
     uint32_t n;
     uint64_t m;
@@ -380,7 +389,7 @@ __global__ void __launch_bounds__(kBlock, 4) k_link_rows(LinkParams P)
                     if (P.giants && P.nseg > 1)
                         giant = P.giants[seg_of(P.seg, P.nseg, v64)];
                     if (giant == kNoGiant || cc_ldp(P.parent, v) != giant) {
-                        Rows r = row_of(P.row_ptr, v, P.m);
+                        Rows r = row_of(P.row_ptr, P.row_end, v, P.m);
                         beg[k] = r.beg + P.skip_from;
                         end[k] = r.end;
                         if (beg[k] > end[k])
@@ -480,7 +489,7 @@ __global__ void __launch_bounds__(kBlock) k_link_heavy(LinkParams P)
     if (cnt > P.heavy_cap)
         cnt = P.heavy_cap;
     const int lane = threadIdx.x & 31;
-    cc_for_heavy_pieces(P.heavy_list, cnt, P.row_ptr, P.m, P.skip_from, kHeavyPiece,
+    cc_for_heavy_pieces(P.heavy_list, cnt, P.row_ptr, P.row_end, P.m, P.skip_from, kHeavyPiece,
                         [&](uint32_t v, uint64_t jb, uint64_t je) {
                             const Span sp = span_of(P.fseg, P.nseg, P.n, v);
                             for (uint64_t j0 = jb; j0 < je; j0 += 32) {
@@ -526,7 +535,7 @@ __global__ void __launch_bounds__(kBlock) k_check_labels(const uint64_t *__restr
             else if (__ldg(L + lv) != lv)
                 local_bad++;
         }
-        Rows r = row_of(row_ptr, (uint32_t)v, m);
+        Rows r = row_of(row_ptr, nullptr, (uint32_t)v, m);
         for (uint64_t j = r.beg + lane; j < r.end; j += 32) {
             uint32_t u = __ldg(col + j);
             if (u < n && __ldg(L + u) != lv)
@@ -563,7 +572,7 @@ int launch_sample(ccgpu_ctx *ctx, const LocalCCArgs &a, uint32_t vlo, uint32_t v
 {
     const int first_done = (a.o.hook_mode & CCGPU_HOOK_FIRST) != 0;
     const uint64_t *fseg = a.seg_filter ? a.seg : nullptr;
-    CC_KLAUNCH(ctx, CCK_SAMPLE, k_sample<LAZY>, blocks, kBlock, 0, st, a.row_ptr, a.col, a.n,
+    CC_KLAUNCH(ctx, CCK_SAMPLE, k_sample<LAZY>, blocks, kBlock, 0, st, a.row_ptr, a.row_end, a.col, a.n,
                a.m, a.labels, vlo, vhi, r0, r1, first_done, fseg, a.nseg);
     return CCGPU_OK;
 }
@@ -575,7 +584,7 @@ int launch_sample_any(ccgpu_ctx *ctx, const LocalCCArgs &a, uint32_t vlo, uint32
 {
     if (a.o.hook_mode & CCGPU_HOOK_MINHOOK) {
         const uint64_t *fseg = a.seg_filter ? a.seg : nullptr;
-        CC_KLAUNCH(ctx, CCK_SAMPLE, k_sample_min, blocks, kBlock, 0, st, a.row_ptr, a.col, a.n,
+        CC_KLAUNCH(ctx, CCK_SAMPLE, k_sample_min, blocks, kBlock, 0, st, a.row_ptr, a.row_end, a.col, a.n,
                    a.m, a.labels, vlo, vhi, r0, r1, fseg, a.nseg);
         return CCGPU_OK;
     }
@@ -641,7 +650,7 @@ int cc_local_init(ccgpu_ctx *ctx, const LocalCCArgs &a, const LocalCCScratch &s,
     const unsigned sb = cc_blocks(a.n, kBlock, g.stream_blocks);
     const int first = (a.o.hook_mode & CCGPU_HOOK_FIRST) && a.o.sample_rounds > 0;
     CC_KLAUNCH(ctx, CCK_INIT, k_init, sb, kBlock, 0, st, a.labels, a.n, s.counters,
-               ((uintptr_t)a.labels & 15) == 0, a.row_ptr, a.col, a.m, first,
+               ((uintptr_t)a.labels & 15) == 0, a.row_ptr, a.row_end, a.col, a.m, first,
                a.seg_filter ? a.seg : (const uint64_t *)nullptr, a.nseg);
     return CCGPU_OK;
 }
@@ -687,7 +696,7 @@ int cc_local_run(ccgpu_ctx *ctx, const LocalCCArgs &a, const LocalCCScratch &s, 
                 for (int r = r_start; r < k; ++r) {
                     if (use_stash && r < 2)
                         CC_KLAUNCH(ctx, CCK_SAMPLE, k_sample_stash, sb, kBlock, 0, st, a.row_ptr,
-                                   a.col, a.n, a.m, a.labels, s.stash, r);
+                                   a.row_end, a.col, a.n, a.m, a.labels, s.stash, r);
                     else
                         CC_TRY(launch_sample_any(ctx, a, 0, a.n, r, r + 1, st, sb));
                     if (r + 1 < k)
@@ -706,6 +715,7 @@ int cc_local_run(ccgpu_ctx *ctx, const LocalCCArgs &a, const LocalCCScratch &s, 
     }
     LinkParams P;
     P.row_ptr = a.row_ptr;
+    P.row_end = a.row_end;
     P.col = a.col;
     P.n = a.n;
     P.m = a.m;

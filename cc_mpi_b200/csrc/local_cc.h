@@ -30,6 +30,11 @@ struct LocalCCArgs {
                                * neighbour, written by sampling round 0
                                * (same sector as the first) and read by
                                * round 1 instead of its row            */
+    const uint64_t *row_end;  /* [n] or NULL: row v is [row_ptr[v],
+                               * row_end[v]) instead of [row_ptr[v],
+                               * row_ptr[v+1]) - rows given as sub-ranges
+                               * of a larger column array (the local
+                               * entries of sorted partition rows)     */
 };
 
 /* Device counters a solve leaves behind (for stats). */

@@ -36,8 +36,9 @@ int cc_bufs_init(DevBufs *b, cudaStream_t st)
 
 int cc_bufs_get(DevBufs *b, void **p, size_t bytes)
 {
-    if (b->n >= 64)
-        return ccgpu_set_error(CCGPU_ERR_LIMIT, "internal: more than 64 temporary buffers");
+    if (b->n >= (int)(sizeof(b->ptrs) / sizeof(b->ptrs[0])))
+        return ccgpu_set_error(CCGPU_ERR_LIMIT, "internal: more than %d temporary buffers",
+                               (int)(sizeof(b->ptrs) / sizeof(b->ptrs[0])));
     if (bytes == 0)
         bytes = 16;
     cudaError_t e = cudaMallocAsync(p, bytes, b->st);

@@ -13,7 +13,7 @@
  * memory instead of returning it to the driver). */
 struct DevBufs {
     cudaStream_t st;
-    void *ptrs[64];
+    void *ptrs[128];
     int n;
 };
 int cc_bufs_init(DevBufs *b, cudaStream_t st);

@@ -188,7 +188,7 @@ static const char *const kKernelNames[CCK_NUM] = {
     "init", "sample", "compress", "giant", "link_rows", "link_heavy", "final_compress",
     "count_roots", "check_labels", "dist_split", "dist_fill", "dist_reps", "dist_pairs",
     "sort_hist", "sort_scan", "sort_scatter", "dist_dedup", "dist_ghosts", "dist_plan",
-    "merge_init", "merge_hook", "merge_upd", "merge_exch_pack", "merge_exch_scatter",
+    "merge_init", "merge_hook", "merge_upd", "merge_exchange", "merge_exch_push",
     "dist_labels", "dist_bounds", "scan", "batch", "misc", "dist_pairs_heavy",
     "dist_pairs_bitmap", "batch_init", "batch_sample", "batch_compress", "batch_giant",
     "batch_link", "batch_heavy", "batch_final", "dist_local_count", "dist_local_fill",

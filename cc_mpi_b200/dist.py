@@ -25,7 +25,7 @@ class DistStats(C.Structure):
                 ("ms_pairs", C.c_double), ("ms_sort", C.c_double), ("ms_ghosts", C.c_double),
                 ("ms_merge", C.c_double), ("ms_total", C.c_double),
                 ("sorted_keys", C.c_uint64), ("local_entries", C.c_uint64),
-                ("sorted_rows", C.c_int), ("pad2", C.c_int)]
+                ("sorted_rows", C.c_int), ("row_runs", C.c_int)]
 
 
 _bound = False

@@ -218,7 +218,10 @@ typedef struct {
     int sorted_rows;        /* 1: the boundary pairs came from the sorted-row
                              * passes (rows strictly ascending), 0: from the
                              * gather pass                                  */
-    int pad2;
+    int row_runs;           /* 1: the local subgraphs were read in place as
+                             * each row's run inside its own partition (rows
+                             * ascending, 2-8 partitions), 0: a local CSR
+                             * was built                                    */
 } ccgpu_dist_stats;
 
 void ccgpu_dist_opts_default(ccgpu_dist_opts *opts);

@@ -152,6 +152,32 @@ def test_sorted_row_mode_and_its_fallback(torch):
     assert st.sorted_rows == 0
 
 
+@pytest.mark.parametrize("parts", [2, 5, 6, 8])
+def test_partition_runs_every_width(torch, parts):
+    """Ascending rows with 2 to 8 partitions take the in-place partition
+    runs (no local CSR is built); counts and labels are the oracle's."""
+    for rp, col in (graphs.rmat_csr(13, 16, seed=101), graphs.grid_csr(120, 90, 0.2, seed=102)):
+        st = check_against_oracle(torch, rp, col, parts, 1, 2)
+        assert st.sorted_rows == 1
+
+
+def test_ids_beyond_n_are_ignored(torch):
+    """Column ids >= n (the reference skips them, src/cc_mpi.c:269,389) sit
+    at the end of ascending rows; the partition runs and the local CSR path
+    both leave them out of the local subgraph and of the raw cut count."""
+    rp, col = graphs.rmat_csr(12, 16, seed=103)
+    n = len(rp) - 1
+    rows = [list(col[int(rp[v]):int(rp[v + 1])]) for v in range(n)]
+    rng = np.random.default_rng(4)
+    for v in rng.choice(n, 300, replace=False):
+        rows[v] += sorted(int(x) for x in rng.choice(np.arange(n, n + 50), 2, replace=False))
+    rp2 = np.zeros(n + 1, np.uint64)
+    rp2[1:] = np.cumsum([len(r) for r in rows])
+    col2 = np.array([x for r in rows for x in r], np.uint32)
+    for parts in (4, 9):
+        check_against_oracle(torch, rp2, col2, parts, 1, 1)
+
+
 def test_bounds_match_reference_restatement(torch):
     rp, col = graphs.rmat_csr(12, 8, seed=6)
     d_rp, _ = dev(torch, rp, col)
