@@ -11,6 +11,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <strings.h>
 
 #include "cc_mpi.h"
 #include "ccgpu.h"
@@ -133,6 +134,56 @@ static int fill_dist(const CSRGraph *g, int use_edge, DistCSRGraph *out, cc_grou
     return 0;
 }
 
+/* A .mat graph for the partitioned path: the CSC arrays go to the device and
+ * are transposed there (ccgpu_graph_from_csc), the device CSR becomes the
+ * graph's mirror, and the host CSR the DistCSRGraph exposes is copied back
+ * from it.  Returns the loader's codes (src/graph.c:46,69,88), 100 on a
+ * device failure. */
+static int load_mat_on_device(const char *path, CSRGraph *full)
+{
+    mat_csc c;
+    int rc = load_csc_from_mat(path, &c);
+    if (rc != 0)
+        return rc;
+    ccgpu_graph *dev = NULL;
+    rc = ccgpu_graph_from_csc(c.jc, c.ir, c.nrows, c.ncols, c.nnz, &dev);
+    free_mat_csc(&c);
+    if (rc != CCGPU_OK) {
+        fprintf(stderr, "load_dist_csr: %s\n", ccgpu_last_error());
+        return 100;
+    }
+    const uint32_t n = ccgpu_graph_n(dev);
+    const uint64_t m = ccgpu_graph_m(dev);
+    full->n = n;
+    full->m = m;
+    full->row_ptr = (uint64_t *)malloc(((size_t)n + 1) * sizeof(uint64_t));
+    full->col_idx = (uint32_t *)malloc((size_t)(m ? m : 1) * sizeof(uint32_t));
+    if (!full->row_ptr || !full->col_idx) {
+        ccgpu_graph_free(dev);
+        return 3;
+    }
+    if (ccgpu_memcpy_d2h(full->row_ptr, ccgpu_graph_row_ptr(dev),
+                         ((size_t)n + 1) * sizeof(uint64_t)) != CCGPU_OK ||
+        ccgpu_memcpy_d2h(full->col_idx, ccgpu_graph_col_idx(dev),
+                         (size_t)m * sizeof(uint32_t)) != CCGPU_OK) {
+        fprintf(stderr, "load_dist_csr: %s\n", ccgpu_last_error());
+        ccgpu_graph_free(dev);
+        return 100;
+    }
+    mirror *mr = (mirror *)calloc(1, sizeof(mirror));
+    if (!mr) {
+        ccgpu_graph_free(dev);
+        return 3;
+    }
+    mr->host_row_ptr = full->row_ptr;
+    mr->dev = dev;
+    pthread_mutex_lock(&g_reg_mu);
+    mr->next = g_reg;
+    g_reg = mr;
+    pthread_mutex_unlock(&g_reg_mu);
+    return 0;
+}
+
 int load_dist_csr_from_file(const char *path, int symmetrize, int drop_self_loops, int use_edge,
                             DistCSRGraph *out, MPI_Comm comm)
 {
@@ -141,8 +192,15 @@ int load_dist_csr_from_file(const char *path, int symmetrize, int drop_self_loop
     memset(out, 0, sizeof(*out));
     CSRGraph full;
     memset(&full, 0, sizeof(full));
-    int rc = load_csr_from_file(path, symmetrize, drop_self_loops, &full);
+    const char *ext = strrchr(path ? path : "", '.');
+    int rc;
+    if (ext && strcasecmp(ext, ".mat") == 0)
+        rc = load_mat_on_device(path, &full);
+    else
+        rc = load_csr_from_file(path, symmetrize, drop_self_loops, &full);
     if (rc != 0) {
+        if (full.row_ptr)
+            reg_drop(full.row_ptr);
         free_csr(&full);
         return rc;
     }

@@ -17,6 +17,7 @@
 #include <zlib.h>
 
 #include "graph.h"
+#include "host_common.h"
 
 enum {
     miINT8 = 1, miUINT8 = 2, miINT16 = 3, miUINT16 = 4, miINT32 = 5, miUINT32 = 6,
@@ -276,7 +277,9 @@ static int parse_matrix_header(span s, mmatrix *M)
     return 0;
 }
 
-static int sparse_to_csr(const mmatrix *M, CSRGraph *out)
+/* The CSC arrays of a sparse matrix element. */
+static int sparse_arrays(const mmatrix *M, uint64_t **ir, uint64_t *nir, uint64_t **jc,
+                         uint64_t *njc)
 {
     span s = M->body;
     melem eir, ejc;
@@ -286,15 +289,61 @@ static int sparse_to_csr(const mmatrix *M, CSRGraph *out)
     s.len -= eir.consumed;
     if (next_elem(s, &ejc))
         return 4;
+    *ir = *jc = NULL;
+    int rc = int_array(&eir, ir, nir);
+    if (rc == 0)
+        rc = int_array(&ejc, jc, njc);
+    if (rc != 0) {
+        free(*ir);
+        free(*jc);
+        *ir = *jc = NULL;
+    }
+    return rc;
+}
+
+static int sparse_to_csr(const mmatrix *M, void *arg)
+{
     uint64_t *ir = NULL, *jc = NULL, nir = 0, njc = 0;
-    int rc = int_array(&eir, &ir, &nir);
+    int rc = sparse_arrays(M, &ir, &nir, &jc, &njc);
     if (rc == 0)
-        rc = int_array(&ejc, &jc, &njc);
-    if (rc == 0)
-        rc = csc_to_csr(M->dims[0], M->dims[1], ir, nir, jc, njc, out);
+        rc = csc_to_csr(M->dims[0], M->dims[1], ir, nir, jc, njc, (CSRGraph *)arg);
     free(ir);
     free(jc);
     return rc;
+}
+
+/* The CSC arrays as they are (row indices that are negative or do not fit
+ * 32 bits become UINT32_MAX, which every reader drops as out of range). */
+static int sparse_to_csc(const mmatrix *M, void *arg)
+{
+    mat_csc *out = (mat_csc *)arg;
+    uint64_t *ir = NULL, *jc = NULL, nir = 0, njc = 0;
+    int rc = sparse_arrays(M, &ir, &nir, &jc, &njc);
+    if (rc != 0)
+        return rc;
+    if (M->dims[0] > 0xfffffffeull || M->dims[1] > 0xfffffffeull || njc < M->dims[1] + 1) {
+        free(ir);
+        free(jc);
+        return 4;
+    }
+    uint64_t nz = jc[M->dims[1]];
+    if (nz > nir)
+        nz = nir;
+    uint32_t *ir32 = (uint32_t *)malloc((nz ? nz : 1) * sizeof(uint32_t));
+    if (!ir32) {
+        free(ir);
+        free(jc);
+        return 3;
+    }
+    for (uint64_t j = 0; j < nz; ++j)
+        ir32[j] = ir[j] > 0xffffffffull ? 0xffffffffu : (uint32_t)ir[j];
+    free(ir);
+    out->nrows = (uint32_t)M->dims[0];
+    out->ncols = (uint32_t)M->dims[1];
+    out->nnz = nz;
+    out->jc = jc;
+    out->ir = ir32;
+    return 0;
 }
 
 /* Finds field `want` of a 1x1 struct; returns its miMATRIX payload. */
@@ -327,9 +376,10 @@ static int struct_field(const mmatrix *M, const char *want, span *field)
     return 2;
 }
 
-int load_csr_from_mat(const char *path, CSRGraph *out)
+/* Walks the MAT file for struct Problem's field A, or else the first
+ * sparse variable (src/graph.c:49-63), and hands it to fn. */
+static int mat_find_sparse(const char *path, int (*fn)(const mmatrix *, void *), void *arg)
 {
-    memset(out, 0, sizeof(*out));
     unsigned char *buf = NULL;
     size_t len = 0;
     int rc = read_file(path, &buf, &len);
@@ -375,11 +425,11 @@ int load_csr_from_mat(const char *path, CSRGraph *out)
                     if (struct_field(&M, "A", &field) == 0) {
                         mmatrix A;
                         if (parse_matrix_header(field, &A) == 0 && A.cls == mxSPARSE_CLASS)
-                            rc = sparse_to_csr(&A, out);
+                            rc = fn(&A, arg);
                     }
                     done = 1;
                 } else if (M.cls == mxSPARSE_CLASS) {
-                    rc = sparse_to_csr(&M, out);
+                    rc = fn(&M, arg);
                     done = 1;
                 }
             }
@@ -394,6 +444,27 @@ int load_csr_from_mat(const char *path, CSRGraph *out)
     if (rc == 2)
         fprintf(stderr, "No sparse matrix found in .mat file %s\n", path);
     return rc;
+}
+
+int load_csr_from_mat(const char *path, CSRGraph *out)
+{
+    memset(out, 0, sizeof(*out));
+    return mat_find_sparse(path, sparse_to_csr, out);
+}
+
+int load_csc_from_mat(const char *path, mat_csc *out)
+{
+    memset(out, 0, sizeof(*out));
+    return mat_find_sparse(path, sparse_to_csc, out);
+}
+
+void free_mat_csc(mat_csc *c)
+{
+    if (!c)
+        return;
+    free(c->jc);
+    free(c->ir);
+    memset(c, 0, sizeof(*c));
 }
 
 /* ----------------------------------------------------------- MAT writer */

@@ -30,4 +30,16 @@ int cc_group_take(cc_group *view, int src,
                   void (*copy)(void *arg, const void *buf, int off, int cnt), void *arg);
 int cc_group_drain(cc_group *view);
 
+/* The CSC arrays of a .mat sparse matrix (struct Problem's field A, or the
+ * first sparse variable), as stored: column starts jc[ncols+1], row indices
+ * ir[nnz].  Return codes as load_csr_from_mat. */
+typedef struct {
+    uint32_t nrows, ncols;
+    uint64_t nnz;
+    uint64_t *jc;
+    uint32_t *ir;
+} mat_csc;
+int load_csc_from_mat(const char *path, mat_csc *out);
+void free_mat_csc(mat_csc *c);
+
 #endif

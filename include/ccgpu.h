@@ -90,6 +90,15 @@ typedef struct ccgpu_graph ccgpu_graph;
 int ccgpu_graph_upload(const uint64_t *h_row_ptr, const uint32_t *h_col_idx, uint32_t n,
                        uint64_t m, ccgpu_graph **out);
 void ccgpu_graph_free(ccgpu_graph *g);
+/* The CSC form of a .mat sparse matrix (column starts jc[ncols+1], row
+ * indices ir[nnz], host arrays) transposed into a device-resident CSR graph
+ * on the device: row r lists the columns c holding an entry (r, c) in
+ * ascending order, and entries whose row index is not below nrows are
+ * dropped - the count / prefix-sum / scatter of the reference's loader
+ * (src/graph.c:91-117), done here as a radix sort of (row, column) keys.
+ * Copy the result to the host with ccgpu_memcpy_d2h if needed. */
+int ccgpu_graph_from_csc(const uint64_t *h_jc, const uint32_t *h_ir, uint32_t nrows,
+                         uint32_t ncols, uint64_t nnz, ccgpu_graph **out);
 const uint64_t *ccgpu_graph_row_ptr(const ccgpu_graph *g);
 const uint32_t *ccgpu_graph_col_idx(const ccgpu_graph *g);
 uint32_t ccgpu_graph_n(const ccgpu_graph *g);

@@ -121,6 +121,50 @@ def test_load_dist_from_mat(L, tmp_path):
     L.cc_group_free(grp)
 
 
+def test_device_csc_to_csr_matches_host_loader(L, tmp_path):
+    """The partitioned loader transposes a .mat's CSC on the device
+    (ccgpu_graph_from_csc); the CSR it exposes equals the host loader's
+    (load_csr_from_mat, the reference's count / scan / scatter,
+    src/graph.c:91-117) entry for entry: rows in order, each row's
+    neighbours ascending.  Cases: a symmetric graph written by scipy, a
+    non-square matrix whose extra columns give ids >= n, empty rows and
+    columns."""
+    import scipy.io as sio
+    import scipy.sparse as sp
+    rp, col = graphs.rmat_csr(12, 8, seed=12)
+    n = len(rp) - 1
+    sym = sp.csc_matrix((np.ones(len(col), bool), col.astype(np.int64), rp.astype(np.int64)),
+                        shape=(n, n))
+    rect = sp.lil_matrix(sp.random(300, 420, density=0.02, random_state=14) != 0)
+    rect[:, 7] = 0
+    rect[11, :] = 0
+    rect = sp.csc_matrix(rect)
+    rect.eliminate_zeros()
+    L.load_csr_from_mat.argtypes = [C.c_char_p, C.POINTER(CSR)]
+    L.free_csr.argtypes = [C.POINTER(CSR)]
+    for name, A, packed in (("sym", sym, True), ("rect", rect, False)):
+        path = str(tmp_path / f"{name}.mat")
+        sio.savemat(path, {"Problem": {"A": A}}, do_compression=packed)
+        host = CSR()
+        assert L.load_csr_from_mat(path.encode(), C.byref(host)) == 0
+        grp = L.cc_group_create(2)
+        L.cc_group_set_verbose(grp, 0)
+        Gd = _lib.DistCSRGraph()
+        assert L.load_dist_csr_from_file(path.encode(), 1, 1, 1, C.byref(Gd), grp) == 0
+        assert Gd.n_global == host.n and Gd.m_global == host.m
+        hr = np.ctypeslib.as_array(host.row_ptr, (host.n + 1,))
+        hc = np.ctypeslib.as_array(host.col_idx, (max(host.m, 1),))[:host.m]
+        dr = np.ctypeslib.as_array(Gd.row_ptr, (Gd.n_global + 1,))
+        dc = np.ctypeslib.as_array(Gd.col_idx, (max(Gd.m_global, 1),))[:Gd.m_global]
+        assert (hr == dr).all() and (hc == dc).all(), name
+        want = sp.csr_matrix(A)
+        want.sort_indices()
+        assert (dr == want.indptr).all() and (dc == want.indices).all(), name
+        L.free_dist_csr(C.byref(Gd))
+        L.free_csr(C.byref(host))
+        L.cc_group_free(grp)
+
+
 def test_boundary_edges_host_api_golden(L):
     from conftest import GOLDEN
     d = np.load(os.path.join(GOLDEN, "boundary_sort.npz"))
