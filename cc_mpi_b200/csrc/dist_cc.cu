@@ -818,6 +818,18 @@ __device__ __forceinline__ bool ng_row(const EmitParams &E, const uint32_t *s_b,
         i <= E.parts ? s_b[i] : 0xffffffffu;                           \
     const uint64_t stride = (uint64_t)gridDim.x * kB
 
+/* With partition offsets (sorted rows), row v's cut entries are the runs
+ * before and after its own: [b, a1) and [c0, c1), c1 = the end of its
+ * valid ids. */
+__device__ __forceinline__ void cut_runs(const EmitParams &E, uint32_t v, int pv, uint64_t b,
+                                         uint64_t &a1, uint64_t &c0, uint64_t &c1)
+{
+    const uint32_t *r = E.roff + (uint64_t)v * E.parts;
+    a1 = b + (pv ? __ldg(r + pv - 1) : 0u);
+    c0 = b + __ldg(r + pv);
+    c1 = b + __ldg(r + E.parts - 1);
+}
+
 template <int PMAX>
 __global__ void __launch_bounds__(kB) k_ng_count(EmitParams E, uint32_t *cnt)
 {
@@ -826,11 +838,18 @@ __global__ void __launch_bounds__(kB) k_ng_count(EmitParams E, uint32_t *cnt)
         uint64_t b, e;
         int pv;
         uint32_t c = 0;
-        if (ng_row<PMAX>(E, s_b, sb, (uint32_t)v, b, e, pv))
-            for (uint64_t j = b; j < e; ++j) {
-                const uint32_t u = __ldg(E.col + j);
-                c += u < E.n && part_fast<PMAX>(s_b, sb, E.parts, u) != pv;
+        if (ng_row<PMAX>(E, s_b, sb, (uint32_t)v, b, e, pv)) {
+            if (E.roff) {
+                uint64_t a1, c0, c1;
+                cut_runs(E, (uint32_t)v, pv, b, a1, c0, c1);
+                c = (uint32_t)((a1 - b) + (c1 - c0));
+            } else {
+                for (uint64_t j = b; j < e; ++j) {
+                    const uint32_t u = __ldg(E.col + j);
+                    c += u < E.n && part_fast<PMAX>(s_b, sb, E.parts, u) != pv;
+                }
             }
+        }
         cnt[v] = c;
     }
 }
@@ -848,6 +867,20 @@ __global__ void __launch_bounds__(kB) k_ng_emit(EmitParams E, const uint64_t *of
         uint64_t o = off[v];
         const uint64_t o_end = off[v + 1];
         const uint32_t rep = __ldg(E.label + v) - s_b[pv];
+        if (E.roff) {
+            uint64_t a1, c0, c1;
+            cut_runs(E, (uint32_t)v, pv, b, a1, c0, c1);
+            for (int run = 0; run < 2; ++run) {
+                const uint64_t j0 = run ? c0 : b, j1 = run ? c1 : a1;
+                for (uint64_t j = j0; j < j1 && o < o_end; ++j) {
+                    const uint32_t u = __ldg(E.col + j);
+                    E.out[o] = make_key(E, pv, u, rep);
+                    work[o] = ((uint64_t)u << 32) | (uint32_t)v;
+                    ++o;
+                }
+            }
+            continue;
+        }
         for (uint64_t j = b; j < e && o < o_end; ++j) {
             const uint32_t u = __ldg(E.col + j);
             if (u >= E.n || part_fast<PMAX>(s_b, sb, E.parts, u) == pv)
@@ -1320,50 +1353,77 @@ __global__ void k_part_cols(const uint64_t *row_ptr, uint64_t m, const uint32_t 
 
 /* --------------------------------------------------------------- reps */
 
+/* Reps (src/cc_mpi.c:326-362): a vertex whose local label is itself.  Each
+ * rep's comp_label starts as its own id (cur and nxt, so reps no round
+ * updates keep it in both buffers) and its hook minimum as none.  The
+ * count is reduced per block, one atomic per block. */
 __global__ void __launch_bounds__(kB) k_reps(const uint32_t *__restrict__ label, uint32_t n,
-                                             uint32_t *rep_list, unsigned long long *rep_count,
-                                             uint32_t *cur, uint32_t *nxt, uint32_t *hook)
+                                             unsigned long long *rep_count, uint32_t *cur,
+                                             uint32_t *nxt, uint32_t *hook)
 {
-    const int lane = threadIdx.x & 31;
+    __shared__ unsigned long long s_w[kW];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint64_t stride = (uint64_t)gridDim.x * kB;
-    for (uint64_t base = (uint64_t)blockIdx.x * kB; base < n; base += stride) {
-        uint64_t v = base + threadIdx.x;
-        bool is_rep = v < n && __ldg(label + v) == (uint32_t)v;
-        unsigned mask = __ballot_sync(0xffffffffu, is_rep);
-        unsigned long long slot = 0;
-        if (lane == 0 && mask)
-            slot = atomicAdd(rep_count, (unsigned long long)__popc(mask));
-        slot = __shfl_sync(0xffffffffu, slot, 0);
-        if (is_rep) {
-            rep_list[slot + __popc(mask & ((1u << lane) - 1u))] = (uint32_t)v;
+    unsigned long long c = 0;
+    for (uint64_t v = (uint64_t)blockIdx.x * kB + threadIdx.x; v < n; v += stride) {
+        if (__ldg(label + v) == (uint32_t)v) {
             cur[v] = (uint32_t)v; /* comp_label[i] = v_start + i, src/cc_mpi.c:361-362 */
-            nxt[v] = (uint32_t)v; /* reps no round updates keep it in both buffers */
+            nxt[v] = (uint32_t)v;
             hook[v] = 0xffffffffu;
+            ++c;
         }
+    }
+    for (int o = 16; o > 0; o >>= 1)
+        c += __shfl_xor_sync(0xffffffffu, c, o);
+    if (lane == 0)
+        s_w[warp] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int w = 0; w < kW; ++w)
+            t += s_w[w];
+        if (t)
+            atomicAdd(rep_count, t);
     }
 }
 
 /* Reps that own at least one boundary pair (their hook minimum is set).  A
  * rep without one has no hook and its own label as its only jump target,
  * so a merge round never changes it (src/cc_mpi.c:575-622): the rounds
- * walk only the others. */
-__global__ void __launch_bounds__(kB) k_active_reps(const uint32_t *__restrict__ rep_list,
-                                                    uint64_t reps, const uint32_t *hook,
-                                                    uint32_t *act, unsigned long long *act_count)
+ * walk only the others.  kActiveV consecutive vertices per thread; the
+ * block scans its counts and reserves its slots with one atomic per
+ * step. */
+constexpr int kActiveV = 8;
+
+__global__ void __launch_bounds__(kB) k_active_reps(const uint32_t *__restrict__ label, uint32_t n,
+                                                    const uint32_t *hook, uint32_t *act,
+                                                    unsigned long long *act_count)
 {
-    const int lane = threadIdx.x & 31;
-    const uint64_t stride = (uint64_t)gridDim.x * kB;
-    for (uint64_t base = (uint64_t)blockIdx.x * kB; base < reps; base += stride) {
-        const uint64_t i = base + threadIdx.x;
-        const uint32_t r = i < reps ? __ldg(rep_list + i) : 0u;
-        const bool a = i < reps && hook[r] != 0xffffffffu;
-        const unsigned mask = __ballot_sync(0xffffffffu, a);
-        unsigned long long slot = 0;
-        if (lane == 0 && mask)
-            slot = atomicAdd(act_count, (unsigned long long)__popc(mask));
-        slot = __shfl_sync(0xffffffffu, slot, 0);
-        if (a)
-            act[slot + __popc(mask & ((1u << lane) - 1u))] = r;
+    __shared__ uint32_t s_warp[kW];
+    __shared__ unsigned long long s_base;
+    const uint64_t step = (uint64_t)kB * kActiveV;
+    for (uint64_t base = (uint64_t)blockIdx.x * step; base < n; base += (uint64_t)gridDim.x * step) {
+        const uint64_t v0 = base + (uint64_t)threadIdx.x * kActiveV;
+        uint32_t bits = 0;
+#pragma unroll
+        for (int k = 0; k < kActiveV; ++k) {
+            const uint64_t v = v0 + k;
+            if (v < n && __ldg(label + v) == (uint32_t)v && hook[v] != 0xffffffffu)
+                bits |= 1u << k;
+        }
+        const uint32_t mine = __popc(bits);
+        uint32_t total = 0;
+        const uint32_t incl = cc_block_incl_scan256<uint32_t>(mine, s_warp, &total);
+        if (threadIdx.x == 0)
+            s_base = total ? atomicAdd(act_count, (unsigned long long)total) : 0ull;
+        __syncthreads();
+        uint64_t o = s_base + incl - mine;
+        while (bits) {
+            const int k = __ffs(bits) - 1;
+            bits &= bits - 1;
+            act[o++] = (uint32_t)(v0 + k);
+        }
+        __syncthreads(); /* s_base is rewritten by the next step */
     }
 }
 
@@ -1947,9 +2007,8 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
     uint32_t *roff = nullptr;
     uint64_t *rlb = nullptr, *rle = nullptr;
     LocalCCScratch ls;
-    uint32_t *rep_list = nullptr, *cur = nullptr, *nxt = nullptr, *hook = nullptr;
+    uint32_t *cur = nullptr, *nxt = nullptr, *hook = nullptr;
     unsigned long long *counters = nullptr; /* [0] keys [1] reps [2] roots [3] sent [4] raw [5] active reps [6] bad */
-    CC_TRY(cc_bufs_get(&B, (void **)&rep_list, (size_t)n * sizeof(uint32_t)));
     CC_TRY(cc_bufs_get(&B, (void **)&cur, (size_t)n * sizeof(uint32_t)));
     CC_TRY(cc_bufs_get(&B, (void **)&nxt, (size_t)n * sizeof(uint32_t)));
     CC_TRY(cc_bufs_get(&B, (void **)&hook, (size_t)n * sizeof(uint32_t)));
@@ -2042,7 +2101,7 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
 
         /* 3. reps and boundary keys */
         CC_CUDA(cudaMemsetAsync(counters, 0, 8 * sizeof(unsigned long long), st));
-        CC_KLAUNCH(ctx, CCK_DIST_REPS, k_reps, sb, kB, 0, st, label, n, rep_list, counters + 1,
+        CC_KLAUNCH(ctx, CCK_DIST_REPS, k_reps, sb, kB, 0, st, label, n, counters + 1,
                    cur, nxt, hook);
         E.row_ptr = d_row_ptr;
         E.col = d_col;
@@ -2338,8 +2397,9 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
         uint32_t *act = nullptr;
         CC_TRY(cc_bufs_get(&B, (void **)&act, (size_t)S.rep_count * sizeof(uint32_t) + 4));
         CC_CUDA(cudaMemsetAsync(counters + 5, 0, sizeof(unsigned long long), st));
-        CC_KLAUNCH(ctx, CCK_MERGE_INIT, k_active_reps, cc_blocks(S.rep_count, kB, gbk), kB, 0,
-                   st, rep_list, S.rep_count, hook, act, counters + 5);
+        CC_KLAUNCH(ctx, CCK_MERGE_INIT, k_active_reps,
+                   cc_blocks((n + kActiveV - 1) / kActiveV, kB, gbk), kB, 0, st, label, n, hook,
+                   act, counters + 5);
         unsigned long long ac = 0;
         CC_CUDA(cudaMemcpyAsync(&ac, counters + 5, sizeof(ac), cudaMemcpyDeviceToHost, st));
         CC_CUDA(cudaStreamSynchronize(st));
