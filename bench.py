@@ -483,8 +483,9 @@ def dist_bytes(torch, ldeg, n, m, st, chunk):
     partitions' local subgraphs and are counted as in local_cc_bytes over
     the local row lengths; the rest as listed per kernel below.  Two layouts
     of the local subgraphs: read in place as each row's run inside its own
-    partition (row_runs: a row-start bitmap, a row-order check and per-row
-    partition offsets), or a local CSR built by a count and a fill pass."""
+    partition (row_runs: one streaming pass checks the row order and writes
+    per-row partition offsets), or a local CSR built by a count and a fill
+    pass."""
     from cc_mpi_b200 import _lib
     R, U, G, reps = int(st.sorted_keys), int(st.pair_count), int(st.ghost_count), \
         int(st.rep_count)
@@ -497,12 +498,9 @@ def dist_bytes(torch, ldeg, n, m, st, chunk):
     tiles, wtiles = (m + 4095) // 4096, (m + 511) // 512
     if runs:
         out.update({
-            # k_row_starts: row pointers in, one bit per entry out
-            "dist_tiles": [8 * (n + 1) + m // 8],
-            # k_rows_ascend: every column entry and its row-start bit
-            "dist_local_count": [4 * m + m // 8],
-            # k_row_ranges: row pointers in; P offsets and the own run out
-            "dist_local_fill": [8 * (n + 1) + 4 * P * n + 16 * n],
+            # k_row_scan: every column entry and row pointer in; P offsets
+            # and the own run (begin, end) of every row out
+            "dist_local_count": [4 * m + 8 * (n + 1) + 4 * P * n + 16 * n],
             # k_emit_ranges: row pointer and P offsets in, mask out (the
             # mirror-mark words it reads are not counted)
             "dist_pairs": [8 * n + 4 * P * n + 4 * n],

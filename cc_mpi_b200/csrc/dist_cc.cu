@@ -142,7 +142,7 @@ struct EmitParams {
     unsigned long long *bad; /* set when a row is not strictly ascending or a
                               * mirror entry is missing: sorted-row mode invalid */
     const uint32_t *roff;    /* [n*parts] partition offsets of sorted rows
-                              * (k_row_ranges), NULL = not computed      */
+                              * (k_row_scan), NULL = not computed        */
 };
 
 /* Plain keys are rare (most cut entries fall in a giant tree), so a block
@@ -425,106 +425,43 @@ __global__ void __launch_bounds__(kB) k_emit_sorted(EmitParams E, const uint32_t
  * When every row is strictly ascending - what the reference's loader always
  * builds (the CSC to CSR transposition of src/graph.c:91-117 emits each row
  * in column order) - a row's entries inside partition q are one contiguous
- * run, found by binary search on the partition bounds.  The local subgraph
- * of each partition (src/cc_mpi.c:252-297) is then the own run of every
- * row, read in place by the local CC (rows as [lb, le) sub-ranges), and the
- * boundary pairs of a row's run in partition q come from its mirror marks
- * alone.  The row order is checked first, in one streaming pass. */
+ * run.  The local subgraph of each partition (src/cc_mpi.c:252-297) is then
+ * the own run of every row, read in place by the local CC (rows as [lb, le)
+ * sub-ranges), and the boundary pairs of a row's run in partition q come
+ * from its mirror marks alone.  One streaming pass checks the row order and
+ * finds every run. */
 
-/* Bit rp[v] of starts for every non-empty row v (the bitmap is zeroed
- * first); lanes whose rows start in the same word combine their bits. */
-__global__ void __launch_bounds__(kB) k_row_starts(const uint64_t *__restrict__ row_ptr,
-                                                   uint32_t n, uint64_t m, uint32_t *starts)
-{
-    const int lane = threadIdx.x & 31;
-    const uint64_t stride = (uint64_t)gridDim.x * kB;
-    for (uint64_t base = (uint64_t)blockIdx.x * kB; base < n; base += stride) {
-        const uint64_t v = base + threadIdx.x;
-        uint64_t b = 0;
-        bool ok = false;
-        if (v < n) {
-            b = __ldg(row_ptr + v);
-            const uint64_t e = __ldg(row_ptr + v + 1);
-            ok = b < e && b < m;
-        }
-        const unsigned long long w = ok ? (unsigned long long)(b >> 5) : ~0ull;
-        const unsigned peers = __match_any_sync(0xffffffffu, w);
-        const uint32_t all = __reduce_or_sync(peers, ok ? 1u << (b & 31) : 0u);
-        if (ok && (__ffs(peers) - 1) == lane)
-            atomicOr(starts + w, all);
-    }
-}
+/* Row order check and partition offsets in one streaming pass over the
+ * column array, 16 entries per thread, kTile per block tile (16-byte loads
+ * when aligned).  The rows of a tile, [r_lo, r_hi] with r_lo holding its
+ * first entry, are staged in shared memory when at most kScanRows of them
+ * touch the tile (otherwise row pointers are read from global memory); a
+ * thread finds the row of its first entry by binary search and steps
+ * forward at each row start.  With ascending rows the count of a row's
+ * entries below bound b_q is the position of its first entry >= b_q, so
+ * every offset is written once: by the thread holding that entry, or by
+ * the thread holding the row's last entry when every entry is below b_q.
+ * Empty rows are written by the thread holding the next row start (or the
+ * array's last entry, for empty rows at the end).  roff[v*P + q-1] =
+ * entries of row v below bounds[q], q = 1..P (bounds[P] = n, so the last
+ * is the count of valid ids); lb/le: v's own run, its local entries.
+ * flags[0] is set when some row descends (its partition runs are not
+ * contiguous), flags[1] when some row repeats an entry (mirror marks need
+ * strictly ascending rows); local_total counts entries inside their row's
+ * own partition. */
+constexpr int kScanRows = 2048;
 
-/* Row order over the whole column array, 16 entries per lane (16-byte
- * loads when aligned): an entry that does not start a row is compared with
- * the one before it.  flags[0] is set when some row descends (its
- * partition runs are not contiguous), flags[1] when some row repeats an
- * entry (mirror marks need strictly ascending rows). */
-__global__ void __launch_bounds__(kB) k_rows_ascend(const uint32_t *__restrict__ col, uint64_t m,
-                                                    const uint32_t *__restrict__ starts, int vec,
-                                                    unsigned *flags)
-{
-    const int lane = threadIdx.x & 31;
-    const uint64_t groups = (m + kTileE - 1) / kTileE;
-    const uint64_t wstride = (uint64_t)gridDim.x * kB;
-    bool desc = false, dup = false;
-    for (uint64_t base = (uint64_t)blockIdx.x * kB + (threadIdx.x & ~31u); base < groups;
-         base += wstride) {
-        const uint64_t t = base + lane;
-        const uint64_t j0 = t * kTileE;
-        uint32_t c[kTileE];
-        if (vec && j0 + kTileE <= m) {
-            const uint4 *c4 = reinterpret_cast<const uint4 *>(col + j0);
-#pragma unroll
-            for (int q = 0; q < kTileE / 4; ++q) {
-                const uint4 x = __ldg(c4 + q);
-                c[4 * q] = x.x;
-                c[4 * q + 1] = x.y;
-                c[4 * q + 2] = x.z;
-                c[4 * q + 3] = x.w;
-            }
-        } else {
-#pragma unroll
-            for (int k = 0; k < kTileE; ++k)
-                c[k] = j0 + k < m ? __ldg(col + j0 + k) : 0u;
-        }
-        /* the entry before j0: the previous lane's last, or a load */
-        uint32_t prev = __shfl_up_sync(0xffffffffu, c[kTileE - 1], 1);
-        if (lane == 0)
-            prev = (j0 > 0 && j0 <= m) ? __ldg(col + j0 - 1) : 0u;
-        if (j0 < m) {
-            const uint32_t sb = __ldg(starts + (j0 >> 5)) >> (j0 & 31); /* j0 % 16 == 0 */
-            const int kv = m - j0 < (uint64_t)kTileE ? (int)(m - j0) : kTileE;
-#pragma unroll
-            for (int k = 0; k < kTileE; ++k) {
-                if (k < kv && !((sb >> k) & 1u)) {
-                    desc |= c[k] < prev;
-                    dup |= c[k] == prev;
-                }
-                prev = c[k];
-            }
-        }
-    }
-    if (__any_sync(0xffffffffu, desc) && lane == 0)
-        atomicOr(flags, 1u);
-    if (__any_sync(0xffffffffu, dup) && lane == 0)
-        atomicOr(flags + 1, 1u);
-}
-
-/* Partition offsets of every (ascending) row: roff[v*P + q-1] = entries of
- * row v below bounds[q], q = 1..P (bounds[P] = n, so the last is the count
- * of valid ids).  All P lower bounds of a row advance together (branchless
- * binary search, one power-of-two step per round), so their loads are
- * independent.  lb/le: v's own run (its local entries); local_total sums
- * them. */
 template <int PMAX>
-__global__ void __launch_bounds__(kB) k_row_ranges(const uint64_t *__restrict__ row_ptr,
-                                                   const uint32_t *__restrict__ col, uint32_t n,
-                                                   uint64_t m, const uint32_t *bounds, int parts,
-                                                   uint32_t *roff, uint64_t *lb, uint64_t *le,
-                                                   unsigned long long *local_total)
+__global__ void __launch_bounds__(kB) k_row_scan(const uint64_t *__restrict__ row_ptr,
+                                                 const uint32_t *__restrict__ col, uint32_t n,
+                                                 uint64_t m, const uint32_t *bounds, int parts,
+                                                 int vec, uint32_t *roff, uint64_t *lb,
+                                                 uint64_t *le, unsigned *flags,
+                                                 unsigned long long *local_total)
 {
+    __shared__ uint64_t s_rp[kScanRows + 1];
     __shared__ uint32_t s_b[PMAX + 1];
+    __shared__ uint32_t s_rlo, s_rhi;
     for (int i = threadIdx.x; i <= PMAX; i += kB)
         s_b[i] = i <= parts ? bounds[i] : 0xffffffffu;
     __syncthreads();
@@ -532,60 +469,156 @@ __global__ void __launch_bounds__(kB) k_row_ranges(const uint64_t *__restrict__ 
 #pragma unroll
     for (int i = 0; i <= PMAX; ++i)
         tb[i] = s_b[i];
-    const uint64_t stride = (uint64_t)gridDim.x * kB;
+    const int P = parts;
+    const uint64_t tiles = (m + kTile - 1) / kTile;
+    bool desc = false, dup = false;
     unsigned long long local = 0;
-    for (uint64_t v = (uint64_t)blockIdx.x * kB + threadIdx.x; v < n; v += stride) {
-        uint64_t b = __ldg(row_ptr + v), e = __ldg(row_ptr + v + 1);
-        e = e > m ? m : e;
-        b = b > e ? e : b;
-        const uint64_t len = e - b;
-        int p = 0;
-#pragma unroll
-        for (int i = 1; i < PMAX; ++i)
-            p += (int)((uint32_t)v >= tb[i]);
-        uint64_t pos[PMAX];
-#pragma unroll
-        for (int q = 0; q < PMAX; ++q)
-            pos[q] = 0;
-        if (len) {
-            const uint32_t first = __ldg(col + b), last = __ldg(col + e - 1);
-            bool open[PMAX], any = false;
-#pragma unroll
-            for (int q = 0; q < PMAX; ++q) {
-                const uint32_t t = tb[q + 1];
-                open[q] = q < parts && first < t && last >= t;
-                pos[q] = (q < parts && last < t) ? len : 0;
-                any |= open[q];
+    for (uint64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+        const uint64_t j0 = t * kTile, jend = j0 + kTile < m ? j0 + kTile : m;
+        if (threadIdx.x < 2) {
+            /* the row holding entry j0 (thread 0) or jend - 1 (thread 1):
+             * the last row whose start is <= that entry */
+            const uint64_t key = threadIdx.x ? jend - 1 : j0;
+            uint32_t lo = 0, hi = n; /* row_ptr[lo] <= key < row_ptr[hi] */
+            while (hi - lo > 1) {
+                const uint32_t mid = lo + (hi - lo) / 2;
+                if (__ldg(row_ptr + mid) <= key)
+                    lo = mid;
+                else
+                    hi = mid;
             }
-            uint64_t step = any ? 1ull << (63 - __clzll((long long)len)) : 0ull;
-            for (; step; step >>= 1) {
+            if (threadIdx.x)
+                s_rhi = lo;
+            else
+                s_rlo = lo;
+        }
+        __syncthreads();
+        const uint32_t r_lo = s_rlo, r_hi = s_rhi;
+        const bool staged = (uint64_t)r_hi - r_lo + 1 < (uint64_t)kScanRows;
+        if (staged)
+            for (uint32_t i = threadIdx.x; i <= r_hi - r_lo + 1; i += kB)
+                s_rp[i] = __ldg(row_ptr + r_lo + i);
+        __syncthreads();
+        auto rp_at = [&](uint64_t r) -> uint64_t {
+            return (staged && r >= r_lo && r <= (uint64_t)r_hi + 1) ? s_rp[r - r_lo]
+                                                                     : __ldg(row_ptr + r);
+        };
+        const uint64_t jt = j0 + (uint64_t)threadIdx.x * kTileE;
+        if (jt < jend) {
+            uint32_t c[kTileE];
+            if (vec && jt + kTileE <= m) {
+                const uint4 *c4 = reinterpret_cast<const uint4 *>(col + jt);
 #pragma unroll
-                for (int q = 0; q < PMAX; ++q)
-                    if (open[q] && pos[q] + step <= len &&
-                        __ldg(col + b + pos[q] + step - 1) < tb[q + 1])
-                        pos[q] += step;
+                for (int q = 0; q < kTileE / 4; ++q) {
+                    const uint4 x = __ldg(c4 + q);
+                    c[4 * q] = x.x;
+                    c[4 * q + 1] = x.y;
+                    c[4 * q + 2] = x.z;
+                    c[4 * q + 3] = x.w;
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < kTileE; ++k)
+                    c[k] = jt + k < m ? __ldg(col + jt + k) : 0u;
+            }
+            /* row of jt: last r in [r_lo, r_hi] with row_ptr[r] <= jt */
+            uint32_t lo = r_lo, hi = r_hi + 1;
+            while (hi - lo > 1) {
+                const uint32_t mid = lo + (hi - lo) / 2;
+                if (rp_at(mid) <= jt)
+                    lo = mid;
+                else
+                    hi = mid;
+            }
+            uint32_t r = lo;
+            uint64_t rbase = rp_at(r), rend = rp_at((uint64_t)r + 1);
+            int pr = 0;
+#pragma unroll
+            for (int i = 1; i < PMAX; ++i)
+                pr += (int)(r >= tb[i]);
+            int prevpart = -1;
+            uint32_t prev = 0;
+            if (jt > rbase) {
+                prev = __ldg(col + jt - 1);
+                int pp = 0;
+#pragma unroll
+                for (int i = 1; i <= PMAX; ++i)
+                    pp += (int)(i <= P && prev >= tb[i]);
+                prevpart = pp;
+            }
+            const int kv = jend - jt < (uint64_t)kTileE ? (int)(jend - jt) : kTileE;
+            auto event = [&](int q, uint64_t off) {
+                if (q >= 1)
+                    roff[(uint64_t)r * P + q - 1] = (uint32_t)off;
+                if (q == pr)
+                    lb[r] = rbase + off;
+                if (q == pr + 1)
+                    le[r] = rbase + off;
+            };
+#pragma unroll
+            for (int k = 0; k < kTileE; ++k) {
+                if (k >= kv)
+                    break;
+                const uint64_t j = jt + k;
+                if (j == rend) { /* a row start: the next non-empty row */
+                    while ((uint64_t)r + 1 < n && rp_at((uint64_t)r + 1) <= j)
+                        ++r;
+                    rbase = j;
+                    rend = rp_at((uint64_t)r + 1);
+                    pr = 0;
+#pragma unroll
+                    for (int i = 1; i < PMAX; ++i)
+                        pr += (int)(r >= tb[i]);
+                    prevpart = -1;
+                }
+                if (j == rbase) {
+                    /* empty rows just before this row start hold no entry:
+                     * their offsets and runs are all zero */
+                    for (uint64_t e = r; e > 0 && rp_at(e - 1) == j; --e) {
+                        const uint64_t er = e - 1;
+                        for (int q = 0; q < P; ++q)
+                            roff[er * P + q] = 0u;
+                        lb[er] = j;
+                        le[er] = j;
+                    }
+                } else {
+                    desc |= c[k] < prev;
+                    dup |= c[k] == prev;
+                }
+                int pv = 0;
+#pragma unroll
+                for (int i = 1; i <= PMAX; ++i)
+                    pv += (int)(i <= P && c[k] >= tb[i]);
+                local += (pv == pr);
+                for (int q = prevpart + 1; q <= pv; ++q)
+                    event(q, j - rbase);
+                if (pv > prevpart)
+                    prevpart = pv;
+                prev = c[k];
+                if (j + 1 == rend)
+                    for (int q = prevpart + 1; q <= P; ++q)
+                        event(q, rend - rbase);
+                if (j + 1 == m)
+                    /* empty rows after the last entry */
+                    for (uint64_t er = (uint64_t)r + 1; er < n; ++er) {
+                        for (int q = 0; q < P; ++q)
+                            roff[er * P + q] = 0u;
+                        lb[er] = m;
+                        le[er] = m;
+                    }
             }
         }
-#pragma unroll
-        for (int q = 0; q < PMAX; ++q)
-            if (q < parts)
-                roff[v * (uint64_t)parts + q] = (uint32_t)pos[q];
-        uint64_t lo = 0, hi = 0;
-#pragma unroll
-        for (int q = 0; q < PMAX; ++q) {
-            if (q + 1 == p)
-                lo = pos[q];
-            if (q == p)
-                hi = pos[q];
-        }
-        lb[v] = b + lo;
-        le[v] = b + hi;
-        local += hi - lo;
+        __syncthreads(); /* s_rp, s_rlo, s_rhi are rewritten by the next tile */
     }
+    const int lane = threadIdx.x & 31;
     for (int o = 16; o > 0; o >>= 1)
         local += __shfl_xor_sync(0xffffffffu, local, o);
-    if ((threadIdx.x & 31) == 0 && local)
+    if (lane == 0 && local)
         atomicAdd(local_total, local);
+    if (__any_sync(0xffffffffu, desc) && lane == 0)
+        atomicOr(flags, 1u);
+    if (__any_sync(0xffffffffu, dup) && lane == 0)
+        atomicOr(flags + 1, 1u);
 }
 
 /* True when some entry of [s, e) has no mirror mark. */
@@ -1639,6 +1672,9 @@ struct MergeParams {
     unsigned long long *sent;
     uint32_t *ghost_rep;          /* [ghosts] local rep of each ghost vertex */
     int ghost_rep_ready;          /* 0: k_exchange fills ghost_rep from label[] */
+    uint8_t *dirty;               /* [n] 1: the rep's label fell since the last
+                                   * exchange (set by k_upd, cleared after an
+                                   * exchange); read from the second exchange on */
 };
 
 /* An exchange lowers the hook minima by one pass over every pair (pull)
@@ -1709,8 +1745,10 @@ __global__ void __launch_bounds__(kB) k_upd(MergeParams M)
             x = y;
         }
         M.next[r] = x;
-        if (x < c)
+        if (x < c) {
             M.changed[p] = 1;
+            M.dirty[r] = 1;
+        }
     }
 }
 
@@ -1736,14 +1774,18 @@ __global__ void __launch_bounds__(kB) k_exchange(MergeParams M)
         bool send = false;
         if (g < M.ghosts) {
             uint32_t rep;
+            bool look = true;
             if (M.ghost_rep_ready) {
                 rep = __ldg(M.ghost_rep + g);
+                /* a rep whose label did not fall since the last exchange
+                 * still has the label last sent: nothing to send */
+                look = M.dirty[rep] != 0;
             } else {
                 rep = __ldg(M.label + __ldg(M.ghost_v + g)); /* fixed by the local solve */
                 M.ghost_rep[g] = rep;
             }
-            const uint32_t lbl = M.cur[rep];
-            if (lbl < M.prev_sent[g]) {
+            const uint32_t lbl = look ? M.cur[rep] : 0xffffffffu;
+            if (look && lbl < M.prev_sent[g]) {
                 M.prev_sent[g] = lbl;
                 M.ghost_labels[g] = lbl;
                 send = true;
@@ -2033,27 +2075,20 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
         CC_CUDA(cudaMemsetAsync(rflags, 0, 2 * sizeof(unsigned), st));
         if (ranges) {
             if (!roff) {
-                uint32_t *starts = nullptr;
-                const size_t words = (size_t)((m + 31) / 32);
-                CC_TRY(cc_bufs_get(&B, (void **)&starts, words * 4));
                 CC_TRY(cc_bufs_get(&B, (void **)&roff, (size_t)n * P * sizeof(uint32_t)));
                 CC_TRY(cc_bufs_get(&B, (void **)&rlb, (size_t)n * sizeof(uint64_t)));
                 CC_TRY(cc_bufs_get(&B, (void **)&rle, (size_t)n * sizeof(uint64_t)));
                 CC_TRY(cc_bufs_get(&B, (void **)&local_total, sizeof(unsigned long long)));
-                CC_CUDA(cudaMemsetAsync(starts, 0, words * 4, st));
                 CC_CUDA(cudaMemsetAsync(local_total, 0, sizeof(unsigned long long), st));
-                CC_KLAUNCH(ctx, CCK_DIST_TILES, k_row_starts, sb, kB, 0, st, d_row_ptr, n, m,
-                           starts);
-                const uint64_t groups = (m + kTileE - 1) / kTileE;
-                CC_KLAUNCH(ctx, CCK_DIST_LOCAL_COUNT, k_rows_ascend,
-                           cc_blocks(groups, kB, (unsigned)ctx->sm_count * 8), kB, 0, st, d_col, m,
-                           starts, Lp.vec, rflags);
+                const unsigned scan_b = cc_blocks(Lp.tiles, 1, (unsigned)ctx->sm_count * 8);
                 if (P <= 4)
-                    CC_KLAUNCH(ctx, CCK_DIST_LOCAL_FILL, k_row_ranges<4>, sb, kB, 0, st,
-                               d_row_ptr, d_col, n, m, bounds, P, roff, rlb, rle, local_total);
+                    CC_KLAUNCH(ctx, CCK_DIST_LOCAL_COUNT, k_row_scan<4>, scan_b, kB, 0, st,
+                               d_row_ptr, d_col, n, m, bounds, P, Lp.vec, roff, rlb, rle, rflags,
+                               local_total);
                 else
-                    CC_KLAUNCH(ctx, CCK_DIST_LOCAL_FILL, k_row_ranges<8>, sb, kB, 0, st,
-                               d_row_ptr, d_col, n, m, bounds, P, roff, rlb, rle, local_total);
+                    CC_KLAUNCH(ctx, CCK_DIST_LOCAL_COUNT, k_row_scan<8>, scan_b, kB, 0, st,
+                               d_row_ptr, d_col, n, m, bounds, P, Lp.vec, roff, rlb, rle, rflags,
+                               local_total);
             }
             l_rp = rlb;
             l_end = rle;
@@ -2386,6 +2421,8 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
     CC_TRY(cc_bufs_get(&B, (void **)&M.changed, P * sizeof(int)));
     CC_TRY(cc_bufs_get(&B, (void **)&M.ghost_rep, (size_t)(G ? G : 1) * sizeof(uint32_t)));
     M.ghost_rep_ready = 0;
+    CC_TRY(cc_bufs_get(&B, (void **)&M.dirty, (size_t)n));
+    CC_CUDA(cudaMemsetAsync(M.dirty, 0, (size_t)n, st));
     const unsigned gbk = (unsigned)ctx->sm_count * 8;
     uint64_t act_count = 0;
     if (U > 0) {
@@ -2451,6 +2488,7 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
                        st, M);
             CC_KLAUNCH(ctx, CCK_MERGE_EXCH_PULL, k_hook_pull, cc_blocks(U, kB, gbk), kB, 0, st,
                        M);
+            CC_CUDA(cudaMemsetAsync(M.dirty, 0, (size_t)n, st));
             S.exchanges++;
             for (int p = 0; p < P; ++p)
                 pending[p] = 0;
