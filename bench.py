@@ -501,9 +501,8 @@ def dist_bytes(torch, ldeg, n, m, st, chunk):
             # k_row_scan: every column entry and row pointer in; P offsets
             # and the own run (begin, end) of every row out
             "dist_local_count": [4 * m + 8 * (n + 1) + 4 * P * n + 16 * n],
-            # k_emit_ranges: row pointer and P offsets in, mask out (the
-            # mirror-mark words it reads are not counted)
-            "dist_pairs": [8 * n + 4 * P * n + 4 * n],
+            # k_emit_ranges: P offsets and P run counts in, mask out
+            "dist_pairs": [8 * P * n + 4 * n],
         })
     else:
         out.update({

@@ -143,6 +143,9 @@ struct EmitParams {
                               * mirror entry is missing: sorted-row mode invalid */
     const uint32_t *roff;    /* [n*parts] partition offsets of sorted rows
                               * (k_row_scan), NULL = not computed        */
+    uint32_t *qcnt;          /* [n*parts] with roff: entries of row u's run in
+                              * partition q whose vertex is outside q's giant
+                              * tree, counted from their local end         */
 };
 
 /* Plain keys are rare (most cut entries fall in a giant tree), so a block
@@ -446,10 +449,22 @@ __global__ void __launch_bounds__(kB) k_emit_sorted(EmitParams E, const uint32_t
  * entries of row v below bounds[q], q = 1..P (bounds[P] = n, so the last
  * is the count of valid ids); lb/le: v's own run, its local entries.
  * flags[0] is set when some row descends (its partition runs are not
- * contiguous), flags[1] when some row repeats an entry (mirror marks need
- * strictly ascending rows); local_total counts entries inside their row's
- * own partition. */
+ * contiguous), flags[1] when some row repeats an entry; local_total counts
+ * entries inside their row's own partition.  symsum checks symmetry: each
+ * entry (r, c) with c < n, c != r adds a 32-bit hash of the unordered pair
+ * {r, c}, positive when r < c and negative otherwise, so a symmetric graph
+ * sums to zero (an asymmetric one does except with probability about
+ * 2^-32). */
 constexpr int kScanRows = 2048;
+
+__device__ __forceinline__ uint32_t pair_hash(uint32_t a, uint32_t b)
+{
+    uint32_t x = a * 0x9E3779B1u ^ (b + 0x7F4A7C15u) * 0x85EBCA77u;
+    x ^= x >> 15;
+    x *= 0x2C1B3C6Du;
+    x ^= x >> 12;
+    return x;
+}
 
 template <int PMAX>
 __global__ void __launch_bounds__(kB) k_row_scan(const uint64_t *__restrict__ row_ptr,
@@ -457,7 +472,8 @@ __global__ void __launch_bounds__(kB) k_row_scan(const uint64_t *__restrict__ ro
                                                  uint64_t m, const uint32_t *bounds, int parts,
                                                  int vec, uint32_t *roff, uint64_t *lb,
                                                  uint64_t *le, unsigned *flags,
-                                                 unsigned long long *local_total)
+                                                 unsigned long long *local_total,
+                                                 unsigned long long *symsum)
 {
     __shared__ uint64_t s_rp[kScanRows + 1];
     __shared__ uint32_t s_b[PMAX + 1];
@@ -472,7 +488,7 @@ __global__ void __launch_bounds__(kB) k_row_scan(const uint64_t *__restrict__ ro
     const int P = parts;
     const uint64_t tiles = (m + kTile - 1) / kTile;
     bool desc = false, dup = false;
-    unsigned long long local = 0;
+    unsigned long long local = 0, sym = 0;
     for (uint64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
         const uint64_t j0 = t * kTile, jend = j0 + kTile < m ? j0 + kTile : m;
         if (threadIdx.x < 2) {
@@ -590,6 +606,10 @@ __global__ void __launch_bounds__(kB) k_row_scan(const uint64_t *__restrict__ ro
                 for (int i = 1; i <= PMAX; ++i)
                     pv += (int)(i <= P && c[k] >= tb[i]);
                 local += (pv == pr);
+                if (c[k] < n && c[k] != r) {
+                    const uint32_t h = c[k] < r ? pair_hash(c[k], r) : pair_hash(r, c[k]);
+                    sym += r < c[k] ? (unsigned long long)h : 0ull - (unsigned long long)h;
+                }
                 for (int q = prevpart + 1; q <= pv; ++q)
                     event(q, j - rbase);
                 if (pv > prevpart)
@@ -611,36 +631,25 @@ __global__ void __launch_bounds__(kB) k_row_scan(const uint64_t *__restrict__ ro
         __syncthreads(); /* s_rp, s_rlo, s_rhi are rewritten by the next tile */
     }
     const int lane = threadIdx.x & 31;
-    for (int o = 16; o > 0; o >>= 1)
+    for (int o = 16; o > 0; o >>= 1) {
         local += __shfl_xor_sync(0xffffffffu, local, o);
+        sym += __shfl_xor_sync(0xffffffffu, sym, o);
+    }
     if (lane == 0 && local)
         atomicAdd(local_total, local);
+    if (lane == 0 && sym)
+        atomicAdd(symsum, sym);
     if (__any_sync(0xffffffffu, desc) && lane == 0)
         atomicOr(flags, 1u);
     if (__any_sync(0xffffffffu, dup) && lane == 0)
         atomicOr(flags + 1, 1u);
 }
 
-/* True when some entry of [s, e) has no mirror mark. */
-__device__ __forceinline__ bool any_unmarked(const uint32_t *__restrict__ ngbits, uint64_t s,
-                                             uint64_t e)
-{
-    for (uint64_t w = s >> 5; w <= (e - 1) >> 5; ++w) {
-        uint32_t mask = 0xffffffffu;
-        if (w == s >> 5)
-            mask &= 0xffffffffu << (s & 31);
-        if (w == (e - 1) >> 5)
-            mask &= 0xffffffffu >> (31 - ((e - 1) & 31));
-        if (~__ldg(ngbits + w) & mask)
-            return true;
-    }
-    return false;
-}
-
 /* Sorted-row mode, remote end, from the partition offsets: row u's run in
- * partition q != u's own sets bit q of pmask[u] when it holds an unmarked
- * entry (a neighbour in q's giant tree; marked ones had their keys written
- * by the local end, k_ng_*).  The thread owning row u stores pmask[u]
+ * partition q != u's own sets bit q of pmask[u] when it holds a neighbour
+ * in q's giant tree, i.e. when the run is longer than the count of its
+ * entries outside that tree (qcnt, written by the local end, k_ng_emit,
+ * which also wrote their keys).  The thread owning row u stores pmask[u]
  * whole.  The raw cut count takes every valid entry outside u's own run. */
 template <int PMAX>
 __global__ void __launch_bounds__(kB) k_emit_ranges(EmitParams E)
@@ -653,7 +662,6 @@ __global__ void __launch_bounds__(kB) k_emit_ranges(EmitParams E)
     const uint64_t stride = (uint64_t)gridDim.x * kB;
     unsigned long long raw = 0;
     for (uint64_t u = (uint64_t)blockIdx.x * kB + threadIdx.x; u < E.n; u += stride) {
-        const uint64_t b = __ldg(E.row_ptr + u);
         int p = 0;
 #pragma unroll
         for (int i = 1; i < PMAX; ++i)
@@ -672,7 +680,7 @@ __global__ void __launch_bounds__(kB) k_emit_ranges(EmitParams E)
                 own = o[q + 1] - o[q];
                 continue;
             }
-            if (any_unmarked(E.ngbits, b + o[q], b + o[q + 1]))
+            if (o[q + 1] - o[q] > __ldg(E.qcnt + u * (uint64_t)P + q))
                 bits |= 1u << q;
         }
         raw += (uint64_t)(o[P < PMAX ? P : PMAX] - own);
@@ -908,7 +916,9 @@ __global__ void __launch_bounds__(kB) k_ng_emit(EmitParams E, const uint64_t *of
                 for (uint64_t j = j0; j < j1 && o < o_end; ++j) {
                     const uint32_t u = __ldg(E.col + j);
                     E.out[o] = make_key(E, pv, u, rep);
-                    work[o] = ((uint64_t)u << 32) | (uint32_t)v;
+                    /* the graph is symmetric: v is an entry of row u's run
+                     * in pv, and not one of pv's giant tree */
+                    atomicAdd(E.qcnt + (uint64_t)u * E.parts + pv, 1u);
                     ++o;
                 }
             }
@@ -971,15 +981,10 @@ __device__ __forceinline__ uint64_t find_sorted(const uint32_t *col, uint64_t lo
 }
 
 /* Marks the mirror entry v of row u for every plain key (u, v) of the
- * local end.  With partition offsets the search covers only row u's run in
- * v's partition. */
+ * local end (the sorted-row mode over a built local CSR). */
 __global__ void __launch_bounds__(kB) k_ng_mark(EmitParams E, const uint64_t *work,
                                                 const uint64_t *total)
 {
-    __shared__ uint32_t s_b[CCGPU_MAX_PARTS + 1];
-    for (int i = threadIdx.x; i <= E.parts; i += kB)
-        s_b[i] = E.bounds[i];
-    __syncthreads();
     const uint64_t items = *total;
     const uint64_t stride = (uint64_t)gridDim.x * kB;
     bool missing = false;
@@ -989,12 +994,6 @@ __global__ void __launch_bounds__(kB) k_ng_mark(EmitParams E, const uint64_t *wo
         uint64_t lo = __ldg(E.row_ptr + u), hi = __ldg(E.row_ptr + u + 1);
         hi = hi > E.m ? E.m : hi;
         lo = lo > hi ? hi : lo;
-        if (E.roff) {
-            const int pv = part_of(s_b, E.parts, v);
-            const uint64_t base = lo;
-            hi = base + __ldg(E.roff + (uint64_t)u * E.parts + pv);
-            lo = base + (pv ? __ldg(E.roff + (uint64_t)u * E.parts + pv - 1) : 0u);
-        }
         const uint64_t pos = find_sorted(E.col, lo, hi, v);
         if (pos != ~0ull)
             atomicOr(E.ngbits + (pos >> 5), 1u << (pos & 31));
@@ -1109,6 +1108,7 @@ __global__ void __launch_bounds__(kB) k_merge(const uint64_t *__restrict__ a, ui
                                               uint64_t *__restrict__ out)
 {
     __shared__ uint64_t s_k[kMergeTile];
+    __shared__ uint64_t s_o[kMergeTile];
     __shared__ uint64_t s_ia[2];
     const uint64_t total = na + nb;
     for (uint64_t d0 = (uint64_t)blockIdx.x * kMergeTile; d0 < total;
@@ -1138,9 +1138,13 @@ __global__ void __launch_bounds__(kB) k_merge(const uint64_t *__restrict__ a, ui
             const uint32_t end = dt + kMergeItems < la + lb ? dt + kMergeItems : la + lb;
             for (uint32_t o = dt; o < end; ++o) {
                 const bool take_a = ib >= lb || (ia < la && s_k[ia] <= s_k[la + ib]);
-                out[d0 + o] = take_a ? s_k[ia++] : s_k[la + ib++];
+                s_o[o] = take_a ? s_k[ia++] : s_k[la + ib++];
             }
         }
+        __syncthreads();
+        /* the tile's outputs leave in order, coalesced */
+        for (uint32_t i = threadIdx.x; i < la + lb; i += kB)
+            out[d0 + i] = s_o[i];
         __syncthreads();
     }
 }
@@ -2078,17 +2082,18 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
                 CC_TRY(cc_bufs_get(&B, (void **)&roff, (size_t)n * P * sizeof(uint32_t)));
                 CC_TRY(cc_bufs_get(&B, (void **)&rlb, (size_t)n * sizeof(uint64_t)));
                 CC_TRY(cc_bufs_get(&B, (void **)&rle, (size_t)n * sizeof(uint64_t)));
-                CC_TRY(cc_bufs_get(&B, (void **)&local_total, sizeof(unsigned long long)));
-                CC_CUDA(cudaMemsetAsync(local_total, 0, sizeof(unsigned long long), st));
+                /* [0] local entries, [1] symmetry sum */
+                CC_TRY(cc_bufs_get(&B, (void **)&local_total, 2 * sizeof(unsigned long long)));
+                CC_CUDA(cudaMemsetAsync(local_total, 0, 2 * sizeof(unsigned long long), st));
                 const unsigned scan_b = cc_blocks(Lp.tiles, 1, (unsigned)ctx->sm_count * 8);
                 if (P <= 4)
                     CC_KLAUNCH(ctx, CCK_DIST_LOCAL_COUNT, k_row_scan<4>, scan_b, kB, 0, st,
                                d_row_ptr, d_col, n, m, bounds, P, Lp.vec, roff, rlb, rle, rflags,
-                               local_total);
+                               local_total, local_total + 1);
                 else
                     CC_KLAUNCH(ctx, CCK_DIST_LOCAL_COUNT, k_row_scan<8>, scan_b, kB, 0, st,
                                d_row_ptr, d_col, n, m, bounds, P, Lp.vec, roff, rlb, rle, rflags,
-                               local_total);
+                               local_total, local_total + 1);
             }
             l_rp = rlb;
             l_end = rle;
@@ -2178,7 +2183,7 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
         sorted_mode = use_mask && P > 1 && P < 32 && (ranges || col_tiles > 0);
         auto emit = [&]() -> int {
             const unsigned lb = cc_blocks(n, kB, (unsigned)ctx->sm_count * 8);
-            if (E.ngbits) {
+            if (E.roff || E.ngbits) {
                 uint32_t *cnt = nullptr;
                 uint64_t *off = nullptr, *work = nullptr;
                 CC_TRY(cc_bufs_get(&B, (void **)&cnt, (size_t)n * sizeof(uint32_t)));
@@ -2192,9 +2197,11 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
                                st, E, cnt);
                 CC_TRY(cc_scan_u32(ctx, cnt, off, n, &B, st));
                 unsigned long long items = 0;
-                CC_CUDA(cudaMemcpyAsync(&items, off + n, sizeof(items), cudaMemcpyDeviceToHost,
-                                        st));
-                CC_CUDA(cudaStreamSynchronize(st));
+                if (!E.roff) {
+                    CC_CUDA(cudaMemcpyAsync(&items, off + n, sizeof(items),
+                                            cudaMemcpyDeviceToHost, st));
+                    CC_CUDA(cudaStreamSynchronize(st));
+                }
                 CC_TRY(cc_bufs_get(&B, (void **)&work,
                                    (size_t)(items ? items : 1) * sizeof(uint64_t)));
                 if (P <= 4)
@@ -2206,7 +2213,6 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
                 else
                     CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_emit<CCGPU_MAX_PARTS>, lb, kB, 0,
                                st, E, off, work);
-                CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_mark, lb, kB, 0, st, E, work, off + n);
                 CC_CUDA(cudaMemcpyAsync(E.count, off + n, sizeof(unsigned long long),
                                         cudaMemcpyDeviceToDevice, st));
                 if (E.roff) {
@@ -2215,6 +2221,8 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
                     else
                         CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit_ranges<8>, lb, kB, 0, st, E);
                 } else {
+                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_mark, lb, kB, 0, st, E, work,
+                               off + n);
                     const unsigned wb = cc_blocks(wtiles, kW, (unsigned)ctx->sm_count * 8);
                     if (P <= 4)
                         CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit_sorted<4>, wb, kB, 0, st, E,
@@ -2240,7 +2248,11 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
             }
             return CCGPU_OK;
         };
-        if (sorted_mode) {
+        E.qcnt = nullptr;
+        if (sorted_mode && ranges) {
+            CC_TRY(cc_bufs_get(&B, (void **)&E.qcnt, (size_t)n * P * sizeof(uint32_t)));
+            CC_CUDA(cudaMemsetAsync(E.qcnt, 0, (size_t)n * P * sizeof(uint32_t), st));
+        } else if (sorted_mode) {
             const size_t words = (size_t)((m + 31) / 32);
             CC_TRY(cc_bufs_get(&B, (void **)&E.ngbits, words * 4));
             CC_CUDA(cudaMemsetAsync(E.ngbits, 0, words * 4, st));
@@ -2248,20 +2260,27 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
         if (P > 1 && m > 0)
             CC_TRY(emit());
         unsigned hf[2] = {0, 0};
+        unsigned long long hl[2] = {m, 0};
         CC_CUDA(cudaMemcpyAsync(hc, counters, 7 * sizeof(unsigned long long),
                                 cudaMemcpyDeviceToHost, st));
         CC_CUDA(cudaMemcpyAsync(hf, rflags, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, st));
         if (ranges)
-            CC_CUDA(cudaMemcpyAsync(&l_m, local_total, sizeof(l_m), cudaMemcpyDeviceToHost, st));
+            CC_CUDA(cudaMemcpyAsync(hl, local_total, sizeof(hl), cudaMemcpyDeviceToHost, st));
         CC_CUDA(cudaStreamSynchronize(st));
+        if (ranges)
+            l_m = hl[0];
         if (ranges && hf[0]) {
             /* some row descends: its partition runs are not contiguous */
             ranges = false;
             continue;
         }
-        if (sorted_mode && (hc[6] || hf[1])) {
+        /* the run counts need a symmetric graph, the mirror marks strictly
+         * ascending rows with every mirror present */
+        const bool redo = ranges ? hl[1] != 0 : (hc[6] || hf[1]);
+        if (sorted_mode && redo) {
             E.ngbits = nullptr;
             E.roff = nullptr;
+            E.qcnt = nullptr;
             CC_CUDA(cudaMemsetAsync(counters, 0, sizeof(unsigned long long), st));
             CC_CUDA(cudaMemsetAsync(counters + 4, 0, sizeof(unsigned long long), st));
             CC_CUDA(cudaMemsetAsync(counters + 6, 0, sizeof(unsigned long long), st));

@@ -121,19 +121,21 @@ def test_unaligned_columns(torch):
 
 
 def test_sorted_row_mode_and_its_fallback(torch):
-    """Strictly ascending rows take the sorted-row boundary passes; the same
-    graph with its rows shuffled, or with a duplicated (mirrored) entry,
-    falls back to the gather pass.  Every variant matches the oracle."""
+    """Ascending rows take the partition runs and the sorted-row boundary
+    passes; the same graph with its rows shuffled falls back to the local
+    CSR build and the gather pass.  A duplicated (mirrored) entry keeps the
+    runs: the run counts of the local end see both copies.  Every variant
+    matches the oracle."""
     rp, col = graphs.rmat_csr(12, 16, seed=91)
     st = check_against_oracle(torch, rp, col, 4, 1, 1)
-    assert st.sorted_rows == 1
+    assert st.sorted_rows == 1 and st.row_runs == 1
     rng = np.random.default_rng(3)
     shuffled = col.copy()
     for v in range(len(rp) - 1):
         a, b = int(rp[v]), int(rp[v + 1])
         shuffled[a:b] = rng.permutation(shuffled[a:b])
     st = check_against_oracle(torch, rp, shuffled, 4, 1, 1)
-    assert st.sorted_rows == 0
+    assert st.sorted_rows == 0 and st.row_runs == 0
     # duplicate the first cut edge found (both directions): rows stay
     # ascending but not strictly
     n = len(rp) - 1
@@ -149,7 +151,26 @@ def test_sorted_row_mode_and_its_fallback(torch):
     rp2[1:] = np.cumsum([len(r) for r in rows])
     col2 = np.array([x for r in rows for x in r], np.uint32)
     st = check_against_oracle(torch, rp2, col2, 4, 1, 1)
-    assert st.sorted_rows == 0
+    assert st.sorted_rows == 1 and st.row_runs == 1
+
+
+def test_asymmetric_input_takes_the_gather_pass(torch):
+    """The run counts assume a symmetric graph (the reference's input); the
+    row scan's symmetry sum catches a cut edge stored in one direction only
+    and the pairs are made by the gather pass instead."""
+    rp, col = graphs.rmat_csr(12, 16, seed=92)
+    n = len(rp) - 1
+    bounds = np.array(oracle.weighted_bounds(rp, 4), dtype=np.int64)
+    part = np.searchsorted(bounds, np.arange(n), side="right") - 1
+    src = np.repeat(np.arange(n), np.diff(rp.astype(np.int64)))
+    cut = np.nonzero(part[src] != part[col])[0][:3]
+    keep = np.ones(len(col), bool)
+    keep[cut] = False
+    col2 = col[keep]
+    rp2 = np.zeros(n + 1, np.uint64)
+    rp2[1:] = np.cumsum(np.bincount(src[keep], minlength=n))
+    _, st, _ = run(torch, rp2, col2, 4, 1, 1)
+    assert st.sorted_rows == 0 and st.row_runs == 1
 
 
 @pytest.mark.parametrize("parts", [2, 5, 6, 8])
