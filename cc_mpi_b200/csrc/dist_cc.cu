@@ -900,6 +900,52 @@ __global__ void __launch_bounds__(kB) k_ng_emit(EmitParams E, const uint64_t *of
                                                 uint64_t *work)
 {
     NG_PROLOGUE;
+    const int lane = threadIdx.x & 31;
+    if (E.roff) {
+        /* partition runs: a row's cut entries are its runs before and after
+         * its own; rows with at least 32 of them are walked by the whole
+         * warp, the others by their thread */
+        for (uint64_t base = (uint64_t)blockIdx.x * kB; base < E.n; base += stride) {
+            const uint64_t v = base + threadIdx.x;
+            uint64_t b = 0, e = 0, a1 = 0, c0 = 0, c1 = 0, o = 0;
+            int pv = 0;
+            uint32_t rep = 0;
+            bool on = v < E.n && ng_row<PMAX>(E, s_b, sb, (uint32_t)v, b, e, pv);
+            if (on) {
+                cut_runs(E, (uint32_t)v, pv, b, a1, c0, c1);
+                o = off[v];
+                rep = __ldg(E.label + v) - s_b[pv];
+            }
+            const uint64_t na = a1 - b, cnt = on ? na + (c1 - c0) : 0;
+            unsigned big = __ballot_sync(0xffffffffu, cnt >= 32);
+            if (cnt && cnt < 32) {
+                for (uint64_t i = 0; i < cnt; ++i) {
+                    const uint32_t u = __ldg(E.col + (i < na ? b + i : c0 + (i - na)));
+                    E.out[o + i] = make_key(E, pv, u, rep);
+                    /* the graph is symmetric: v is an entry of row u's run
+                     * in pv, and not one of pv's giant tree */
+                    atomicAdd(E.qcnt + (uint64_t)u * E.parts + pv, 1u);
+                }
+            }
+            while (big) {
+                const int src = __ffs(big) - 1;
+                big &= big - 1;
+                const uint64_t wb = __shfl_sync(0xffffffffu, b, src);
+                const uint64_t wna = __shfl_sync(0xffffffffu, na, src);
+                const uint64_t wc0 = __shfl_sync(0xffffffffu, c0, src);
+                const uint64_t wcnt = __shfl_sync(0xffffffffu, cnt, src);
+                const uint64_t wo = __shfl_sync(0xffffffffu, o, src);
+                const int wpv = __shfl_sync(0xffffffffu, pv, src);
+                const uint32_t wrep = __shfl_sync(0xffffffffu, rep, src);
+                for (uint64_t i = lane; i < wcnt; i += 32) {
+                    const uint32_t u = __ldg(E.col + (i < wna ? wb + i : wc0 + (i - wna)));
+                    E.out[wo + i] = make_key(E, wpv, u, wrep);
+                    atomicAdd(E.qcnt + (uint64_t)u * E.parts + wpv, 1u);
+                }
+            }
+        }
+        return;
+    }
     for (uint64_t v = (uint64_t)blockIdx.x * kB + threadIdx.x; v < E.n; v += stride) {
         uint64_t b, e;
         int pv;
@@ -908,22 +954,6 @@ __global__ void __launch_bounds__(kB) k_ng_emit(EmitParams E, const uint64_t *of
         uint64_t o = off[v];
         const uint64_t o_end = off[v + 1];
         const uint32_t rep = __ldg(E.label + v) - s_b[pv];
-        if (E.roff) {
-            uint64_t a1, c0, c1;
-            cut_runs(E, (uint32_t)v, pv, b, a1, c0, c1);
-            for (int run = 0; run < 2; ++run) {
-                const uint64_t j0 = run ? c0 : b, j1 = run ? c1 : a1;
-                for (uint64_t j = j0; j < j1 && o < o_end; ++j) {
-                    const uint32_t u = __ldg(E.col + j);
-                    E.out[o] = make_key(E, pv, u, rep);
-                    /* the graph is symmetric: v is an entry of row u's run
-                     * in pv, and not one of pv's giant tree */
-                    atomicAdd(E.qcnt + (uint64_t)u * E.parts + pv, 1u);
-                    ++o;
-                }
-            }
-            continue;
-        }
         for (uint64_t j = b; j < e && o < o_end; ++j) {
             const uint32_t u = __ldg(E.col + j);
             if (u >= E.n || part_fast<PMAX>(s_b, sb, E.parts, u) == pv)
@@ -1650,6 +1680,31 @@ __global__ void k_plan(const uint32_t *__restrict__ ghost_v, const uint64_t *__r
     seg[t] = lo;
 }
 
+/* Id buckets of every partition's ghost list: gbucket[p*(nb+1) + b] = the
+ * first of p's ghosts with id >= b << shift (p's ghosts ascend), for
+ * b = 0..nb; one binary search per bucket. */
+__global__ void __launch_bounds__(kB) k_ghost_buckets(const uint32_t *__restrict__ ghost_v,
+                                                      const uint64_t *__restrict__ gh_off,
+                                                      int parts, uint32_t nb, int shift,
+                                                      uint32_t *gbucket)
+{
+    const uint64_t total = (uint64_t)parts * (nb + 1);
+    const uint64_t stride = (uint64_t)gridDim.x * kB;
+    for (uint64_t i = (uint64_t)blockIdx.x * kB + threadIdx.x; i < total; i += stride) {
+        const int p = (int)(i / (nb + 1));
+        const uint64_t key = (uint64_t)(i % (nb + 1)) << shift;
+        uint64_t lo = gh_off[p], hi = gh_off[p + 1];
+        while (lo < hi) {
+            const uint64_t mid = lo + (hi - lo) / 2;
+            if (__ldg(ghost_v + mid) < key)
+                lo = mid + 1;
+            else
+                hi = mid;
+        }
+        gbucket[i] = (uint32_t)lo;
+    }
+}
+
 /* ------------------------------------------------------------- merge */
 
 struct MergeParams {
@@ -1676,6 +1731,9 @@ struct MergeParams {
     unsigned long long *sent;
     uint32_t *ghost_rep;          /* [ghosts] local rep of each ghost vertex */
     int ghost_rep_ready;          /* 0: k_exchange fills ghost_rep from label[] */
+    const uint32_t *gbucket;      /* [parts*(gnb+1)] first ghost of each id bucket */
+    uint32_t gnb;                 /* id buckets per partition                      */
+    int gshift;                   /* bucket = id >> gshift                         */
     uint8_t *dirty;               /* [n] 1: the rep's label fell since the last
                                    * exchange (set by k_upd, cleared after an
                                    * exchange); read from the second exchange on */
@@ -1713,7 +1771,9 @@ __device__ __forceinline__ bool label_of(const MergeParams &M, const uint32_t *s
         y = M.cur[__ldg(M.label + x)];
         return true;
     }
-    uint64_t lo = M.gh_off[p], hi = M.gh_off[p + 1];
+    /* p's ghosts are ascending; the bucket of x narrows the search */
+    const uint32_t *bk = M.gbucket + (uint64_t)p * (M.gnb + 1) + (x >> M.gshift);
+    uint64_t lo = __ldg(bk), hi = __ldg(bk + 1);
     while (lo < hi) {
         uint64_t mid = lo + (hi - lo) / 2;
         if (__ldg(M.ghost_v + mid) < x)
@@ -2406,6 +2466,17 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
         CC_KLAUNCH(ctx, CCK_DIST_PLAN, k_plan, (tot + kB - 1) / kB, kB, 0, st, D.ghost_v, gh_off,
                    bounds, P, segs);
     }
+    /* id buckets of the ghost lists for the merge's lookups: about 16 ids
+     * per bucket, at most ~64 MB in all */
+    int gshift = 4;
+    while (gshift < 31 && (uint64_t)P * ((n >> gshift) + 2) * 4 > (64ull << 20))
+        ++gshift;
+    const uint32_t gnb = (uint32_t)((n >> gshift) + 1);
+    uint32_t *gbucket = nullptr;
+    CC_TRY(cc_bufs_get(&B, (void **)&gbucket, (size_t)P * (gnb + 1) * sizeof(uint32_t)));
+    CC_KLAUNCH(ctx, CCK_DIST_PLAN, k_ghost_buckets,
+               cc_blocks((uint64_t)P * (gnb + 1), kB, (unsigned)ctx->sm_count * 8), kB, 0, st,
+               D.ghost_v, gh_off, P, gnb, gshift, gbucket);
     CC_TRY(clock_mark(clk, st)); /* 5 */
     if (o.verbose >= 2) {
         for (int p = 0; p < P; ++p)
@@ -2433,6 +2504,9 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
     M.prev_sent = D.prev_sent;
     M.ghosts = G;
     M.gh_off = gh_off;
+    M.gbucket = gbucket;
+    M.gnb = gnb;
+    M.gshift = gshift;
     M.seg = segs;
     M.sent = counters + 3;
     CC_TRY(cc_bufs_get(&B, (void **)&M.delta, (size_t)(G ? G : 1) * sizeof(uint32_t)));
