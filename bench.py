@@ -61,6 +61,7 @@ WORKLOADS = {
                          big_frac=0.0, seconds=6.0, served=True),
 }
 L2_BYTES = 126 * 1024 * 1024
+ORACLE_MAX_N = 1_000_000  # batched workloads: graphs up to this size are checked by the oracle
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -541,7 +542,12 @@ def dist_bytes(torch, ldeg, n, m, st, chunk):
 # unit of work, so that a capture on a smaller graph scales to the bench's
 # graph: "entry" = CSR entries, "vertex" = vertices.  Each figure comes from
 # the capture summarised in the named profiles/ file.
-NCU_TRAFFIC = {}
+NCU_TRAFFIC = {
+    # k_sample_stash, rounds 0 and 1 averaged (173.8 MB and 34.2 MB) on R-MAT
+    # scale 22 (4,194,304 vertices)
+    "sample": {"per": "vertex", "bytes_per_unit": 103_996_544 / 4_194_304,
+               "source": "profiles/local_cc_sample_stash_rmat22_ncu.md"},
+}
 
 
 def ncu_traffic(kernel, n, m):
@@ -882,21 +888,45 @@ def run_batch(args, torch, dist_mod, rank, world, dev):
     torch.cuda.synchronize()
     comps, done = plan.results(stream=sptr)
     verified = bool(torch.equal(d_lab, want)) and bool((done == 1).all())
+    # the same plan as one persistent launch (kb_persist): labels checked too
+    ptune = batch.Tuning()
+    C.memmove(C.byref(ptune), C.byref(tuning), C.sizeof(batch.Tuning))
+    ptune.persistent = 1
+    pplan = batch.BatchPlan(vo, eo, d_rp, d_col, d_lab, tuning=ptune)
+    d_lab.fill_(-1)
+    pplan.launch(stream=sptr)
+    torch.cuda.synchronize()
+    pcomps, pdone = pplan.results(stream=sptr)
+    p_verified = bool(torch.equal(d_lab, want)) and bool((pdone == 1).all()) and \
+        bool((pcomps == comps).all())
+    verified = verified and p_verified
     oracle_checked = []
     if rank == 0 and not args.no_verify:
+        # every graph of at most ORACLE_MAX_N vertices against the oracle's
+        # union-find labels, on the host's cores (the C oracle releases the
+        # interpreter lock)
         import oracle
+        from concurrent.futures import ThreadPoolExecutor
         lab = d_lab.cpu().numpy().view(np.uint32)
-        order = np.argsort([n for _, n, _ in spec])
-        for g in sorted({int(order[0]), int(order[G // 2]), int(order[-1])} |
-                        {int(x) for x in range(0, G, max(1, G // 16))}):
+        rp_all = d_rp.cpu().numpy().view(np.uint64)
+        small = [g for g in range(G) if int(vo[g + 1] - vo[g]) <= ORACLE_MAX_N]
+
+        def check(g):
             a, n = int(vo[g]), int(vo[g + 1] - vo[g])
-            rp = d_rp[a + g:a + g + n + 1].cpu().numpy().view(np.uint64)
+            rp = rp_all[a + g:a + g + n + 1]
             col = d_col[int(eo[g]):int(eo[g + 1])].cpu().numpy().view(np.uint32)
             ref = oracle.uf_labels(rp, col)
-            ok = bool((batch.labels_of(lab, vo, g) == ref).all()) and \
+            return bool((batch.labels_of(lab, vo, g) == ref).all()) and \
                 int(comps[g]) == oracle.count_components(ref)
-            verified = verified and ok
-            oracle_checked.append(g)
+
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(max(1, os.cpu_count() or 1)) as ex:
+            oks = list(ex.map(check, small))
+        log(f"batch: {len(small)} graphs checked against the oracle in "
+            f"{time.perf_counter() - t0:.1f} s")
+        verified = verified and all(oks)
+        oracle_checked = small
+        del rp_all, lab
     for _ in range(args.warmup):
         flush.fill_(1)
         plan.launch(stream=sptr)
@@ -921,9 +951,17 @@ def run_batch(args, torch, dist_mod, rank, world, dev):
             t = float(tt.item())
         return t
 
+    for _ in range(args.warmup):
+        flush.fill_(1)
+        pplan.launch(stream=sptr)
+    torch.cuda.synchronize()
     with ClockSampler(dev.index or 0) as clk:
-        t_ms = timed(lambda: plan.launch(stream=sptr), args.steps)
-    launches = plan.kernels() * args.steps
+        t_graph_ms = timed(lambda: plan.launch(stream=sptr), args.steps)
+        t_pers_ms = timed(lambda: pplan.launch(stream=sptr), args.steps)
+    persistent = t_pers_ms <= t_graph_ms if args.batch_launch == "best" else \
+        args.batch_launch == "persistent"
+    t_ms = t_pers_ms if persistent else t_graph_ms
+    launches = (pplan if persistent else plan).kernels() * args.steps
     plain_steps = max(1, min(args.steps, 3))
     t_plain_ms = timed(lambda: plain_loop(want), plain_steps)
 
@@ -970,7 +1008,8 @@ def run_batch(args, torch, dist_mod, rank, world, dev):
             t0 = time.perf_counter()
             d_rp.copy_(rp_h, non_blocking=True)
             d_col[:max(M, 1)].copy_(col_h, non_blocking=True)
-            _lib.check(Lb.ccgpu_batch_cc(None, C.byref(b), C.byref(tuning), None, sptr))
+            _lib.check(Lb.ccgpu_batch_cc(None, C.byref(b), C.byref(ptune if persistent else tuning),
+                                         None, sptr))
             lab_h.copy_(d_lab, non_blocking=True)
             torch.cuda.synchronize()
             t_e2e.append(time.perf_counter() - t0)
@@ -1018,10 +1057,13 @@ def run_batch(args, torch, dist_mod, rank, world, dev):
                "mix": "log-uniform vertex counts; ER mean degree 8 / R-MAT ef 16 / grid 10% "
                       "deleted, one third each",
                "graphs_per_class": [int(x) for x in classes], "tuning": tuning.as_dict(),
+               "launch": "one persistent launch (kb_persist)" if persistent else
+                         "CUDA graph replay of the per-phase kernels",
                "autotune_s": tune_s, "build_s": gen_s,
                "l2": "2x L2 buffer written between timed steps; packed batch > L2",
                "parallelism": f"replicas{world}" if world > 1 else "single",
-               "verified_vs_plain_kernel": verified, "oracle_checked_graphs": len(oracle_checked)}
+               "verified_vs_plain_kernel": verified, "oracle_checked_graphs": len(oracle_checked),
+               "oracle_checked": f"every graph of at most {ORACLE_MAX_N} vertices"}
         line = {
             "metric": "batched CC graphs/s", "value": G * world / (t_ms / 1e3),
             "unit": "graphs/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -1041,13 +1083,21 @@ def run_batch(args, torch, dist_mod, rank, world, dev):
                              "gbs": round(bytes_per.get(kk, 0) / (v[0] / 1e3) / 1e9, 1)}
                         for kk, v in per.items()},
             "ms_per_step_kernel_by_kernel": t_prof_ms,
-            "timing": "value: K replays of the batch's CUDA graph; kernels: the same K solves "
-                      "launched kernel by kernel with events around every launch",
+            "launch_modes": {
+                "graph_replay": {"ms_per_step": t_graph_ms, "graphs_per_s": G / (t_graph_ms / 1e3),
+                                 "kernels_per_step": plan.kernels()},
+                "persistent": {"ms_per_step": t_pers_ms, "graphs_per_s": G / (t_pers_ms / 1e3),
+                               "kernels_per_step": pplan.kernels(),
+                               "whole_solve_frac": step_bytes / (t_pers_ms / 1e3) / 1e9 / peak}},
+            "timing": "value: K solves in the faster launch mode (launch_modes: K replays of "
+                      "the CUDA graph of per-phase kernels, K persistent launches); kernels: the "
+                      "per-phase kernels launched one by one with events around every launch",
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
     plan.close()
+    pplan.close()
     return 0
 
 
@@ -1225,6 +1275,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-verify", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-launch", choices=["best", "graph", "persistent"], default="best",
+                    help="batched workloads: launch mode of the headline value")
     ap.add_argument("--hook-mode", type=int, default=-1, help="ccgpu_cc_opts.hook_mode")
     ap.add_argument("--sample-rounds", type=int, default=-1)
     ap.add_argument("--parts", type=int, default=0, help="partitions (partitioned workloads)")

@@ -35,11 +35,13 @@ class ClassOpts(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("class_bounds", C.c_float * (CLASSES - 1)), ("heavy_degree", C.c_int),
-                ("cls", ClassOpts * CLASSES)]
+                ("cls", ClassOpts * CLASSES), ("persistent", C.c_int), ("wait_ms", C.c_int),
+                ("stall_graph", C.c_int)]
 
     def as_dict(self):
         return {"class_bounds": list(self.class_bounds), "heavy_degree": self.heavy_degree,
-                "classes": [self.cls[c].as_dict() for c in range(CLASSES)]}
+                "classes": [self.cls[c].as_dict() for c in range(CLASSES)],
+                "persistent": self.persistent, "wait_ms": self.wait_ms}
 
 
 _bound = False

@@ -108,51 +108,60 @@ __device__ __forceinline__ void row_bounds(const Tile &T, uint32_t v, uint64_t &
         b = e;
 }
 
-__global__ void __launch_bounds__(kB) kb_init(BatchK K)
+__device__ __forceinline__ void tile_init(const Tile &T)
 {
-    for (uint32_t t = blockIdx.x; t < K.tiles; t += gridDim.x) {
-        const Tile T = tile_of(K, t);
-        for (uint32_t v = T.v0 + threadIdx.x; v < T.v1; v += kB)
-            T.parent[v] = v;
+    for (uint32_t v = T.v0 + threadIdx.x; v < T.v1; v += kB)
+        T.parent[v] = v;
+}
+
+/* Links row entry r of every vertex of the tile (MINHOOK sampling). */
+__device__ __forceinline__ void tile_sample(const BatchK &K, const Tile &T, int r)
+{
+    uint32_t *stash = K.stash ? K.stash + (T.parent - K.labels) : nullptr;
+    for (uint32_t v = T.v0 + threadIdx.x; v < T.v1; v += kB) {
+        uint32_t u;
+        if (stash && r == 1) {
+            u = stash[v]; /* written by round 0 */
+        } else {
+            uint64_t b, e;
+            row_bounds(T, v, b, e);
+            u = b + (uint64_t)r < e ? __ldg(T.col + b + r) : 0xffffffffu;
+            if (stash && r == 0)
+                stash[v] = b + 1 < e ? __ldg(T.col + b + 1) : 0xffffffffu;
+        }
+        if (u >= T.n)
+            continue;
+        const uint32_t rv = cc_find(T.parent, v), ru = cc_find(T.parent, u);
+        if (rv != ru)
+            atomicMin(T.parent + (rv > ru ? rv : ru), rv < ru ? rv : ru);
     }
 }
 
-/* Links row entry r of every vertex (MINHOOK sampling). */
+__device__ __forceinline__ void tile_compress(const Tile &T)
+{
+    for (uint32_t v = T.v0 + threadIdx.x; v < T.v1; v += kB) {
+        const uint32_t r = cc_find(T.parent, v);
+        if (r != v)
+            T.parent[v] = r;
+    }
+}
+
+__global__ void __launch_bounds__(kB) kb_init(BatchK K)
+{
+    for (uint32_t t = blockIdx.x; t < K.tiles; t += gridDim.x)
+        tile_init(tile_of(K, t));
+}
+
 __global__ void __launch_bounds__(kB) kb_sample(BatchK K, int r)
 {
-    for (uint32_t t = blockIdx.x; t < K.tiles; t += gridDim.x) {
-        const Tile T = tile_of(K, t);
-        uint32_t *stash = K.stash ? K.stash + (T.parent - K.labels) : nullptr;
-        for (uint32_t v = T.v0 + threadIdx.x; v < T.v1; v += kB) {
-            uint32_t u;
-            if (stash && r == 1) {
-                u = stash[v]; /* written by round 0 */
-            } else {
-                uint64_t b, e;
-                row_bounds(T, v, b, e);
-                u = b + (uint64_t)r < e ? __ldg(T.col + b + r) : 0xffffffffu;
-                if (stash && r == 0)
-                    stash[v] = b + 1 < e ? __ldg(T.col + b + 1) : 0xffffffffu;
-            }
-            if (u >= T.n)
-                continue;
-            const uint32_t rv = cc_find(T.parent, v), ru = cc_find(T.parent, u);
-            if (rv != ru)
-                atomicMin(T.parent + (rv > ru ? rv : ru), rv < ru ? rv : ru);
-        }
-    }
+    for (uint32_t t = blockIdx.x; t < K.tiles; t += gridDim.x)
+        tile_sample(K, tile_of(K, t), r);
 }
 
 __global__ void __launch_bounds__(kB) kb_compress(BatchK K)
 {
-    for (uint32_t t = blockIdx.x; t < K.tiles; t += gridDim.x) {
-        const Tile T = tile_of(K, t);
-        for (uint32_t v = T.v0 + threadIdx.x; v < T.v1; v += kB) {
-            const uint32_t r = cc_find(T.parent, v);
-            if (r != v)
-                T.parent[v] = r;
-        }
-    }
+    for (uint32_t t = blockIdx.x; t < K.tiles; t += gridDim.x)
+        tile_compress(tile_of(K, t));
 }
 
 /* One CTA per graph of the class: most frequent root of 1024 samples. */
@@ -220,21 +229,136 @@ __device__ __forceinline__ void warp_row(const Tile &T, uint32_t v, uint64_t b, 
     }
 }
 
-/* Finish pass: tiles grabbed with an atomic counter; rows of vertices in
- * the graph's giant tree are skipped (valid for symmetric graphs: every
- * edge leaving the tree is seen from its other end). */
 /* Vertices a thread takes per step of the finish pass (consecutive), so
  * the step's barriers are paid once per kVPT vertices per thread. */
 constexpr int kVPT = 4;
 constexpr int kStep = kB * kVPT;
 
+/* Shared memory of one tile of the finish pass. */
+struct LinkSmem {
+    uint32_t off[kStep + 1];
+    uint64_t beg[kStep];
+    uint32_t wsum[kWarpsB];
+    uint32_t heavy_n;
+    uint32_t heavy_v[kStep];
+    uint64_t heavy_b[kStep], heavy_e[kStep];
+};
+
+/* Finish pass over one tile: rows of vertices outside the graph's giant tree
+ * (valid for symmetric graphs: every edge leaving the tree is seen from its
+ * other end).  Short rows are gathered per CTA and walked edge-parallel,
+ * rows of at least warp_deg entries by a warp; rows above heavy_deg go to
+ * the class's heavy queue, or, with inline_heavy, are walked by the whole
+ * CTA once the tile's other rows are done. */
+__device__ __forceinline__ void tile_link(const BatchK &K, const Tile &T, LinkSmem &S,
+                                          bool inline_heavy)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t giant = K.skip ? __ldg(K.giants + T.g) : kNone;
+    if (threadIdx.x == 0)
+        S.heavy_n = 0;
+    __syncthreads();
+    for (uint32_t t0 = T.v0; t0 < T.v1; t0 += kStep) {
+        uint64_t beg[kVPT], end[kVPT];
+        uint32_t small[kVPT], mine = 0;
+#pragma unroll
+        for (int k = 0; k < kVPT; ++k) {
+            const uint32_t v = t0 + threadIdx.x * kVPT + k;
+            beg[k] = end[k] = 0;
+            if (v < T.v1 && (giant == kNone || cc_ldp(T.parent, v) != giant))
+                row_bounds(T, v, beg[k], end[k]);
+            uint64_t deg = end[k] - beg[k];
+            if (deg > K.heavy_deg) {
+                if (inline_heavy) {
+                    const uint32_t slot = atomicAdd(&S.heavy_n, 1u);
+                    S.heavy_v[slot] = v;
+                    S.heavy_b[slot] = beg[k];
+                    S.heavy_e[slot] = end[k];
+                    deg = 0;
+                    end[k] = beg[k];
+                } else {
+                    const uint32_t slot = atomicAdd(K.heavy_count, 1u);
+                    if (slot < K.heavy_cap) {
+                        K.heavy_list[slot] = ((uint64_t)T.g << 32) | v;
+                        deg = 0;
+                        end[k] = beg[k];
+                    }
+                }
+            }
+            unsigned big = __ballot_sync(0xffffffffu, deg >= K.warp_deg);
+            while (big) {
+                const int src = __ffs(big) - 1;
+                big &= big - 1;
+                const uint32_t vv = __shfl_sync(0xffffffffu, v, src);
+                const uint64_t bb = __shfl_sync(0xffffffffu, beg[k], src);
+                const uint64_t ee = __shfl_sync(0xffffffffu, end[k], src);
+                warp_row(T, vv, bb, ee, lane);
+            }
+            small[k] = deg < K.warp_deg ? (uint32_t)deg : 0u;
+            mine += small[k];
+            S.beg[threadIdx.x * kVPT + k] = beg[k];
+        }
+        uint32_t incl = mine;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o)
+                incl += y;
+        }
+        if (lane == 31)
+            S.wsum[warp] = incl;
+        __syncthreads();
+        uint32_t wpre = 0, total = 0;
+#pragma unroll
+        for (int w = 0; w < kWarpsB; ++w) {
+            const uint32_t x = S.wsum[w];
+            wpre += (w < warp) ? x : 0u;
+            total += x;
+        }
+        uint32_t run = wpre + incl - mine;
+#pragma unroll
+        for (int k = 0; k < kVPT; ++k) {
+            S.off[threadIdx.x * kVPT + k] = run;
+            run += small[k];
+        }
+        if (threadIdx.x == 0)
+            S.off[kStep] = total;
+        __syncthreads();
+        for (uint32_t e = threadIdx.x; e < total; e += kB) {
+            int lo = 0, hi = kStep;
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (S.off[mid] <= e)
+                    lo = mid;
+                else
+                    hi = mid;
+            }
+            const uint32_t u = __ldg(T.col + S.beg[lo] + (e - S.off[lo]));
+            if (u < T.n)
+                cc_link(T.parent, t0 + (uint32_t)lo, u);
+        }
+        if (inline_heavy) { /* this step's heavy rows (at most kStep) */
+            const uint32_t nh = S.heavy_n;
+            for (uint32_t h = 0; h < nh; ++h) {
+                const uint32_t v = S.heavy_v[h];
+                for (uint64_t j = S.heavy_b[h] + threadIdx.x; j < S.heavy_e[h]; j += kB) {
+                    const uint32_t u = __ldg(T.col + j);
+                    if (u < T.n)
+                        cc_link(T.parent, v, u);
+                }
+            }
+        }
+        __syncthreads();
+        if (inline_heavy && threadIdx.x == 0)
+            S.heavy_n = 0;
+        __syncthreads();
+    }
+}
+
+/* Finish pass: tiles grabbed with an atomic counter. */
 __global__ void __launch_bounds__(kB, 4) kb_link(BatchK K)
 {
-    __shared__ uint32_t s_off[kStep + 1];
-    __shared__ uint64_t s_beg[kStep];
-    __shared__ uint32_t s_wsum[kWarpsB];
+    __shared__ LinkSmem S;
     __shared__ unsigned long long s_t;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (;;) {
         if (threadIdx.x == 0)
             s_t = atomicAdd(K.grab, 1ull);
@@ -243,79 +367,7 @@ __global__ void __launch_bounds__(kB, 4) kb_link(BatchK K)
         __syncthreads();
         if (t >= K.tiles)
             break;
-        const Tile T = tile_of(K, (uint32_t)t);
-        const uint32_t giant = K.skip ? __ldg(K.giants + T.g) : kNone;
-        for (uint32_t t0 = T.v0; t0 < T.v1; t0 += kStep) {
-            uint64_t beg[kVPT], end[kVPT];
-            uint32_t small[kVPT], mine = 0;
-#pragma unroll
-            for (int k = 0; k < kVPT; ++k) {
-                const uint32_t v = t0 + threadIdx.x * kVPT + k;
-                beg[k] = end[k] = 0;
-                if (v < T.v1 && (giant == kNone || cc_ldp(T.parent, v) != giant))
-                    row_bounds(T, v, beg[k], end[k]);
-                uint64_t deg = end[k] - beg[k];
-                if (deg > K.heavy_deg) {
-                    const uint32_t slot = atomicAdd(K.heavy_count, 1u);
-                    if (slot < K.heavy_cap) {
-                        K.heavy_list[slot] = ((uint64_t)T.g << 32) | v;
-                        deg = 0;
-                        end[k] = beg[k];
-                    }
-                }
-                unsigned big = __ballot_sync(0xffffffffu, deg >= K.warp_deg);
-                while (big) {
-                    const int src = __ffs(big) - 1;
-                    big &= big - 1;
-                    const uint32_t vv = __shfl_sync(0xffffffffu, v, src);
-                    const uint64_t bb = __shfl_sync(0xffffffffu, beg[k], src);
-                    const uint64_t ee = __shfl_sync(0xffffffffu, end[k], src);
-                    warp_row(T, vv, bb, ee, lane);
-                }
-                small[k] = deg < K.warp_deg ? (uint32_t)deg : 0u;
-                mine += small[k];
-                s_beg[threadIdx.x * kVPT + k] = beg[k];
-            }
-            uint32_t incl = mine;
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o)
-                    incl += y;
-            }
-            if (lane == 31)
-                s_wsum[warp] = incl;
-            __syncthreads();
-            uint32_t wpre = 0, total = 0;
-#pragma unroll
-            for (int w = 0; w < kWarpsB; ++w) {
-                const uint32_t x = s_wsum[w];
-                wpre += (w < warp) ? x : 0u;
-                total += x;
-            }
-            uint32_t run = wpre + incl - mine;
-#pragma unroll
-            for (int k = 0; k < kVPT; ++k) {
-                s_off[threadIdx.x * kVPT + k] = run;
-                run += small[k];
-            }
-            if (threadIdx.x == 0)
-                s_off[kStep] = total;
-            __syncthreads();
-            for (uint32_t e = threadIdx.x; e < total; e += kB) {
-                int lo = 0, hi = kStep;
-                while (hi - lo > 1) {
-                    const int mid = (lo + hi) >> 1;
-                    if (s_off[mid] <= e)
-                        lo = mid;
-                    else
-                        hi = mid;
-                }
-                const uint32_t u = __ldg(T.col + s_beg[lo] + (e - s_off[lo]));
-                if (u < T.n)
-                    cc_link(T.parent, t0 + (uint32_t)lo, u);
-            }
-            __syncthreads();
-        }
+        tile_link(K, tile_of(K, (uint32_t)t), S, false);
     }
 }
 
@@ -358,34 +410,249 @@ __global__ void __launch_bounds__(kB) kb_heavy(BatchK K)
         });
 }
 
+/* Root of x read through L2 (ld.global.cg): in a persistent launch a
+ * block's L1 may hold parent values written before other blocks' links,
+ * and a stale "root" must not become a final label. */
+__device__ __forceinline__ uint32_t find_coherent(uint32_t *parent, uint32_t x)
+{
+    uint32_t p;
+    asm volatile("ld.global.cg.u32 %0, [%1];" : "=r"(p) : "l"(parent + x));
+    while (p != x) {
+        uint32_t gp;
+        asm volatile("ld.global.cg.u32 %0, [%1];" : "=r"(gp) : "l"(parent + p));
+        if (gp == p)
+            return p;
+        atomicMin(parent + x, gp);
+        x = gp;
+        asm volatile("ld.global.cg.u32 %0, [%1];" : "=r"(p) : "l"(parent + x));
+    }
+    return x;
+}
+
+/* labels[v] = root(v) over the tile; the graph's component count, and its
+ * done flag set by its last tile. */
+__device__ __forceinline__ void tile_final(const BatchK &K, const Tile &T, uint32_t *s_c,
+                                           bool coherent)
+{
+    uint32_t c = 0;
+    for (uint32_t v = T.v0 + threadIdx.x; v < T.v1; v += kB) {
+        const uint32_t r = coherent ? find_coherent(T.parent, v) : cc_find(T.parent, v);
+        if (r != v)
+            T.parent[v] = r;
+        c += r == v;
+    }
+    c = __reduce_add_sync(0xffffffffu, c);
+    if ((threadIdx.x & 31) == 0)
+        s_c[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t sum = 0;
+        for (int w = 0; w < kWarpsB; ++w)
+            sum += s_c[w];
+        if (sum)
+            atomicAdd(K.comps + T.g, sum);
+        const uint32_t ntiles = (T.n + K.tile - 1) / K.tile;
+        __threadfence();
+        if (atomicAdd(K.tiles_done + T.g, 1u) + 1 == ntiles)
+            atomicExch(K.done + T.g, 1u);
+    }
+    __syncthreads();
+}
+
 __global__ void __launch_bounds__(kB) kb_final(BatchK K)
 {
     __shared__ uint32_t s_c[kWarpsB];
-    for (uint32_t t = blockIdx.x; t < K.tiles; t += gridDim.x) {
-        const Tile T = tile_of(K, t);
-        uint32_t c = 0;
-        for (uint32_t v = T.v0 + threadIdx.x; v < T.v1; v += kB) {
-            const uint32_t r = cc_find(T.parent, v);
-            if (r != v)
-                T.parent[v] = r;
-            c += r == v;
+    for (uint32_t t = blockIdx.x; t < K.tiles; t += gridDim.x)
+        tile_final(K, tile_of(K, t), s_c, false);
+}
+
+/* ------------------------------------------------- persistent launch */
+
+/* One launch moves every graph of every degree class through the solve's
+ * phases.  Each class's solve is a program of phases (init, sample rounds
+ * and compressions, giant, link, final); a phase's work items are its
+ * class's tiles - or graphs, for the giant phase.  The launch's items are
+ * the segments (class, phase) in phase-major order across the classes, so
+ * the classes advance together; blocks take items from one counter in that
+ * order.  An item of phase k of a class waits until its graph's counter of
+ * phase k-1 shows all of that phase's items done.  Items are taken in
+ * order and every item depends only on items before it, so the oldest
+ * unfinished item never waits and the launch always progresses; each wait
+ * is still bounded (wait_ns of the global timer), and one that runs out
+ * sets *err, after which every block stops taking items. */
+constexpr int kMaxPhases = 12;
+constexpr int kMaxSegs = CCGPU_BATCH_CLASSES * kMaxPhases;
+enum { PH_INIT = 0, PH_SAMPLE = 1, PH_COMPRESS = 2, PH_GIANT = 3, PH_LINK = 4, PH_FINAL = 5 };
+
+struct PersistK {
+    BatchK K[CCGPU_BATCH_CLASSES];
+    int nseg;
+    int cls[kMaxSegs];             /* class of the segment                  */
+    int kind[kMaxSegs];
+    int round[kMaxSegs];           /* sample round                          */
+    int phase[kMaxSegs];           /* phase index within its class          */
+    int prev_kind[kMaxSegs];       /* kind of the class's previous phase    */
+    uint64_t off[kMaxSegs + 1];    /* first item of each segment            */
+    uint32_t *pcnt;                /* [G * kMaxPhases] items done per graph */
+    unsigned long long *grab;
+    int *err;
+    unsigned long long wait_ns;
+    uint32_t stall_graph;          /* kNone = off                           */
+};
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t *p)
+{
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+/* The giant phase of one graph with 256 threads: the same 1024 seeded
+ * samples as kb_giant, sorted bitonically 4 per thread, and the most
+ * frequent root (ties to the smaller). */
+__device__ __forceinline__ void graph_giant(const BatchK &K, uint32_t g, uint32_t seed,
+                                            uint32_t *s, unsigned long long *s_best)
+{
+    const uint32_t n = __ldg(&K.gr[g].n);
+    const uint32_t *parent = K.labels + __ldg(&K.gr[g].lab);
+    if (n == 0) {
+        if (threadIdx.x == 0)
+            K.giants[g] = kNone;
+        return;
+    }
+    for (uint32_t i = threadIdx.x; i < 1024; i += kB) {
+        const uint32_t h = cc_mix32(i * 0x9e3779b9u + seed + g);
+        const uint32_t v = (uint32_t)(((uint64_t)h * n) >> 32);
+        s[i] = cc_find_ro(parent, v);
+    }
+    __syncthreads();
+    for (uint32_t k = 2; k <= 1024; k <<= 1) {
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+            for (uint32_t i = threadIdx.x; i < 1024; i += kB) {
+                const uint32_t ij = i ^ j;
+                if (ij > i) {
+                    const uint32_t a = s[i], b = s[ij];
+                    const bool up = (i & k) == 0;
+                    if ((a > b) == up) {
+                        s[i] = b;
+                        s[ij] = a;
+                    }
+                }
+            }
+            __syncthreads();
         }
-        c = __reduce_add_sync(0xffffffffu, c);
-        if ((threadIdx.x & 31) == 0)
-            s_c[threadIdx.x >> 5] = c;
+    }
+    unsigned long long key = 0;
+    for (uint32_t i = threadIdx.x; i < 1024; i += kB) {
+        const uint32_t val = s[i];
+        if (i == 0 || s[i - 1] != val) {
+            uint32_t a = i, b = 1024;
+            while (a < b) {
+                const uint32_t mid = (a + b) >> 1;
+                if (s[mid] <= val)
+                    a = mid + 1;
+                else
+                    b = mid;
+            }
+            const unsigned long long kk = ((unsigned long long)(a - i) << 32) | (uint32_t)~val;
+            key = kk > key ? kk : key;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
+        key = other > key ? other : key;
+    }
+    if ((threadIdx.x & 31) == 0)
+        s_best[threadIdx.x >> 5] = key;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long best = 0;
+        for (int w = 0; w < kWarpsB; ++w)
+            best = s_best[w] > best ? s_best[w] : best;
+        K.giants[g] = ~(uint32_t)best;
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kB) kb_persist(const __grid_constant__ PersistK Q)
+{
+    __shared__ LinkSmem S;
+    __shared__ uint32_t s_g[1024];
+    __shared__ unsigned long long s_best[kWarpsB];
+    __shared__ uint32_t s_c[kWarpsB];
+    __shared__ unsigned long long s_item;
+    __shared__ int s_seg, s_stop;
+    const uint64_t total = Q.off[Q.nseg];
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const unsigned long long item =
+                *(volatile int *)Q.err ? ~0ull : atomicAdd(Q.grab, 1ull);
+            int sg = 0;
+            while (sg + 1 < Q.nseg && Q.off[sg + 1] <= item)
+                ++sg;
+            s_item = item;
+            s_seg = sg;
+            s_stop = 0;
+        }
+        __syncthreads();
+        const unsigned long long item = s_item;
+        if (item >= total)
+            break;
+        const int sg = s_seg;
+        const BatchK &K = Q.K[Q.cls[sg]];
+        const uint64_t idx = item - Q.off[sg];
+        const int kind = Q.kind[sg], ph = Q.phase[sg];
+        Tile T;
+        uint32_t g;
+        if (kind == PH_GIANT) {
+            g = __ldg(K.graphs + idx);
+        } else {
+            T = tile_of(K, (uint32_t)idx);
+            g = T.g;
+        }
+        if (ph > 0 && threadIdx.x == 0) {
+            /* items of the class's previous phase for this graph: one giant
+             * item, or one per tile */
+            const uint32_t n = __ldg(&K.gr[g].n);
+            uint32_t need = Q.prev_kind[sg] == PH_GIANT ? 1u : (n + K.tile - 1) / K.tile;
+            if (g == Q.stall_graph && ph == 1)
+                need += 1; /* never met: exercises the bounded wait */
+            const uint32_t *c = Q.pcnt + (uint64_t)g * kMaxPhases + (ph - 1);
+            if (ld_acquire(c) < need) {
+                const unsigned long long t0 = global_ns();
+                while (ld_acquire(c) < need) {
+                    if (*(volatile int *)Q.err || global_ns() - t0 > Q.wait_ns) {
+                        atomicExch(Q.err, 1);
+                        s_stop = 1;
+                        break;
+                    }
+                    __nanosleep(256);
+                }
+            }
+        }
+        __syncthreads();
+        if (s_stop)
+            break;
+        switch (kind) {
+        case PH_INIT: tile_init(T); break;
+        case PH_SAMPLE: tile_sample(K, T, Q.round[sg]); break;
+        case PH_COMPRESS: tile_compress(T); break;
+        case PH_GIANT: graph_giant(K, g, 0x5eed1234u, s_g, s_best); break;
+        case PH_LINK: tile_link(K, T, S, true); break;
+        default: tile_final(K, T, s_c, true); break;
+        }
         __syncthreads();
         if (threadIdx.x == 0) {
-            uint32_t sum = 0;
-            for (int w = 0; w < kWarpsB; ++w)
-                sum += s_c[w];
-            if (sum)
-                atomicAdd(K.comps + T.g, sum);
-            const uint32_t ntiles = (T.n + K.tile - 1) / K.tile;
             __threadfence();
-            if (atomicAdd(K.tiles_done + T.g, 1u) + 1 == ntiles)
-                atomicExch(K.done + T.g, 1u);
+            atomicAdd(Q.pcnt + (uint64_t)g * kMaxPhases + ph, 1u);
         }
-        __syncthreads();
     }
 }
 
@@ -494,6 +761,8 @@ int batch_check_tuning(ccgpu_batch_tuning *t)
 {
     if (t->heavy_degree < 32)
         t->heavy_degree = 32;
+    if (t->wait_ms < 0)
+        return ccgpu_set_error(CCGPU_ERR_INVALID, "batch: wait_ms %d is negative", t->wait_ms);
     for (int c = 0; c < CCGPU_BATCH_CLASSES; ++c) {
         const ccgpu_batch_class_opts &o = t->cls[c];
         if (o.sample_rounds < 0 || o.sample_rounds > 4)
@@ -519,6 +788,9 @@ int batch_core_init(BatchCore *c, ccgpu_ctx *ctx, const ccgpu_batch_tuning *tuni
         ccgpu_batch_tuning_default(&c->tune);
     CC_TRY(batch_check_tuning(&c->tune));
     CC_CUDA(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming));
+    CC_CUDA(cudaMalloc((void **)&c->d_err, sizeof(int)));
+    CC_CUDA(cudaMemset(c->d_err, 0, sizeof(int)));
+    CC_CUDA(cudaMalloc((void **)&c->d_grab, sizeof(unsigned long long)));
     for (int k = 0; k < CCGPU_BATCH_CLASSES; ++k) {
         c->cls[k].o = c->tune.cls[k];
         CC_CUDA(cudaStreamCreateWithFlags(&c->cls[k].st, cudaStreamNonBlocking));
@@ -550,6 +822,9 @@ void batch_core_free(BatchCore *c)
     cudaFree(c->d_comps);
     cudaFree(c->d_tiles_done);
     cudaFree(c->d_done);
+    cudaFree(c->d_pcnt);
+    cudaFree(c->d_err);
+    cudaFree(c->d_grab);
     if (c->h_stage)
         cudaFreeHost(c->h_stage);
     cudaFree(c->stash);
@@ -569,14 +844,16 @@ int batch_core_reserve(BatchCore *c, size_t graphs, size_t tiles, size_t heavy)
         cudaFree(c->d_comps);
         cudaFree(c->d_tiles_done);
         cudaFree(c->d_done);
+        cudaFree(c->d_pcnt);
         c->d_gr = nullptr;
-        c->d_giants = c->d_comps = c->d_tiles_done = c->d_done = nullptr;
+        c->d_giants = c->d_comps = c->d_tiles_done = c->d_done = c->d_pcnt = nullptr;
         c->g_cap = 0;
         CC_CUDA(cudaMalloc((void **)&c->d_gr, graphs * sizeof(BGraph)));
         CC_CUDA(cudaMalloc((void **)&c->d_giants, graphs * sizeof(uint32_t)));
         CC_CUDA(cudaMalloc((void **)&c->d_comps, graphs * sizeof(uint32_t)));
         CC_CUDA(cudaMalloc((void **)&c->d_tiles_done, graphs * sizeof(uint32_t)));
         CC_CUDA(cudaMalloc((void **)&c->d_done, graphs * sizeof(uint32_t)));
+        CC_CUDA(cudaMalloc((void **)&c->d_pcnt, graphs * kMaxPhases * sizeof(uint32_t)));
         c->g_cap = graphs;
     }
     for (int k = 0; k < CCGPU_BATCH_CLASSES; ++k) {
@@ -613,8 +890,9 @@ int batch_core_set(BatchCore *c, const uint64_t *row_ptr, const uint32_t *col, u
         cudaFree(c->d_comps);
         cudaFree(c->d_tiles_done);
         cudaFree(c->d_done);
+        cudaFree(c->d_pcnt);
         c->d_gr = nullptr;
-        c->d_giants = c->d_comps = c->d_tiles_done = c->d_done = nullptr;
+        c->d_giants = c->d_comps = c->d_tiles_done = c->d_done = c->d_pcnt = nullptr;
         c->g_cap = 0;
         const size_t want = (size_t)G + G / 2 + 64;
         CC_CUDA(cudaMalloc((void **)&c->d_gr, want * sizeof(BGraph)));
@@ -622,6 +900,7 @@ int batch_core_set(BatchCore *c, const uint64_t *row_ptr, const uint32_t *col, u
         CC_CUDA(cudaMalloc((void **)&c->d_comps, want * sizeof(uint32_t)));
         CC_CUDA(cudaMalloc((void **)&c->d_tiles_done, want * sizeof(uint32_t)));
         CC_CUDA(cudaMalloc((void **)&c->d_done, want * sizeof(uint32_t)));
+        CC_CUDA(cudaMalloc((void **)&c->d_pcnt, want * kMaxPhases * sizeof(uint32_t)));
         c->g_cap = want;
     }
     /* staging: descriptors, then per class graph list and tile list */
@@ -724,12 +1003,90 @@ int batch_core_enqueue_class(BatchCore *c, int k, cudaStream_t st, int *kernels)
     return CCGPU_OK;
 }
 
+/* The whole batch as one persistent launch (kb_persist). */
+int batch_core_enqueue_persistent(BatchCore *c, cudaStream_t st, int *kernels)
+{
+    PersistK Q;
+    memset(&Q, 0, sizeof(Q));
+    struct Prog {
+        int n = 0;
+        int kind[kMaxPhases], round[kMaxPhases];
+        uint64_t items[kMaxPhases];
+    } prog[CCGPU_BATCH_CLASSES];
+    int longest = 0;
+    for (int k = 0; k < CCGPU_BATCH_CLASSES; ++k) {
+        BatchClass &C = c->cls[k];
+        if (C.graphs.empty() || C.tiles == 0)
+            continue;
+        Q.K[k] = kargs(c, k);
+        Prog &P = prog[k];
+        auto add = [&](int kind, int round, uint64_t items) {
+            P.kind[P.n] = kind;
+            P.round[P.n] = round;
+            P.items[P.n] = items;
+            P.n++;
+        };
+        const int rounds = C.o.sample_rounds;
+        add(PH_INIT, 0, C.tiles);
+        for (int r = 0; r < rounds; ++r) {
+            add(PH_SAMPLE, r, C.tiles);
+            if (C.o.cadence || r + 1 == rounds)
+                add(PH_COMPRESS, 0, C.tiles);
+        }
+        if (rounds > 0)
+            add(PH_GIANT, 0, C.graphs.size());
+        add(PH_LINK, 0, C.tiles);
+        add(PH_FINAL, 0, C.tiles);
+        longest = P.n > longest ? P.n : longest;
+    }
+    for (int ph = 0; ph < longest; ++ph)
+        for (int k = 0; k < CCGPU_BATCH_CLASSES; ++k) {
+            const Prog &P = prog[k];
+            if (ph >= P.n)
+                continue;
+            const int sg = Q.nseg++;
+            Q.cls[sg] = k;
+            Q.kind[sg] = P.kind[ph];
+            Q.round[sg] = P.round[ph];
+            Q.phase[sg] = ph;
+            Q.prev_kind[sg] = ph ? P.kind[ph - 1] : -1;
+            Q.off[sg + 1] = Q.off[sg] + P.items[ph];
+        }
+    if (Q.nseg == 0)
+        return CCGPU_OK;
+    Q.pcnt = c->d_pcnt;
+    Q.grab = c->d_grab;
+    Q.err = c->d_err;
+    Q.wait_ns = (unsigned long long)(c->tune.wait_ms ? c->tune.wait_ms : 2000) * 1000000ull;
+    Q.stall_graph = c->tune.stall_graph >= 0 ? (uint32_t)c->tune.stall_graph : kNone;
+    if (!c->persist_blocks) {
+        CC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c->persist_blocks, kb_persist, kB,
+                                                              0));
+        if (c->persist_blocks < 1)
+            c->persist_blocks = 1;
+    }
+    CC_CUDA(cudaMemsetAsync(c->d_grab, 0, sizeof(unsigned long long), st));
+    const uint64_t items = Q.off[Q.nseg];
+    uint64_t grid = (uint64_t)c->sms * (uint64_t)c->persist_blocks;
+    if (grid > items)
+        grid = items;
+    CC_KLAUNCH(c->ctx, CCK_BATCH, kb_persist, (unsigned)(grid ? grid : 1), kB, 0, st, Q);
+    if (kernels)
+        *kernels += 1;
+    return CCGPU_OK;
+}
+
 int batch_core_enqueue(BatchCore *c, cudaStream_t st, int *kernels)
 {
     const size_t gbytes = (c->gr.empty() ? 1 : c->gr.size()) * sizeof(uint32_t);
     CC_CUDA(cudaMemsetAsync(c->d_comps, 0, gbytes, st));
     CC_CUDA(cudaMemsetAsync(c->d_tiles_done, 0, gbytes, st));
     CC_CUDA(cudaMemsetAsync(c->d_done, 0, gbytes, st));
+    if (c->tune.persistent) {
+        CC_CUDA(cudaMemsetAsync(c->d_pcnt, 0, gbytes * kMaxPhases, st));
+        CC_CUDA(cudaMemsetAsync(c->d_err, 0, sizeof(int), st));
+        return batch_core_enqueue_persistent(c, st, kernels);
+    }
     CC_CUDA(cudaEventRecord(c->fork, st));
     for (int k = 0; k < CCGPU_BATCH_CLASSES; ++k) {
         BatchClass &C = c->cls[k];
@@ -840,6 +1197,9 @@ extern "C" void ccgpu_batch_tuning_default(ccgpu_batch_tuning *t)
     t->class_bounds[0] = 6.0f;
     t->class_bounds[1] = 16.0f;
     t->heavy_degree = 8192;
+    t->persistent = 0;
+    t->wait_ms = 0;
+    t->stall_graph = -1;
     for (int c = 0; c < CCGPU_BATCH_CLASSES; ++c) {
         t->cls[c].sample_rounds = 2;
         t->cls[c].cadence = 1;
@@ -1035,11 +1395,19 @@ extern "C" int ccgpu_batch_plan_results(ccgpu_batch_plan *p, uint32_t *h_compone
         CC_CUDA(cudaMemcpyAsync(h_components, p->core.d_comps, gb, cudaMemcpyDeviceToHost, st));
     if (h_done)
         CC_CUDA(cudaMemcpyAsync(h_done, p->core.d_done, gb, cudaMemcpyDeviceToHost, st));
+    int err = 0;
+    if (p->core.tune.persistent)
+        CC_CUDA(cudaMemcpyAsync(&err, p->core.d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     CC_CUDA(cudaStreamSynchronize(st));
     /* a graph without vertices has no tile: it is solved, with 0 components */
     for (uint32_t g = 0; h_done && g < p->G; ++g)
         if (p->vtx_off[g + 1] == p->vtx_off[g])
             h_done[g] = 1;
+    if (err)
+        return ccgpu_set_error(CCGPU_ERR_TIMEOUT,
+                               "batch: a persistent launch gave up waiting for a graph's "
+                               "previous phase (wait_ms %d)",
+                               p->core.tune.wait_ms ? p->core.tune.wait_ms : 2000);
     return CCGPU_OK;
 }
 

@@ -51,6 +51,10 @@ struct BatchCore {
     std::vector<BGraph> gr;
     BGraph *d_gr = nullptr;
     uint32_t *d_giants = nullptr, *d_comps = nullptr, *d_tiles_done = nullptr, *d_done = nullptr;
+    uint32_t *d_pcnt = nullptr; /* persistent launches: [g_cap * 12] phase counters */
+    int *d_err = nullptr;       /* persistent launches: 1 once a wait ran out      */
+    unsigned long long *d_grab = nullptr; /* persistent launches: item counter */
+    int persist_blocks = 0;     /* resident blocks of the persistent kernel per SM */
     size_t g_cap = 0;
     BatchClass cls[CCGPU_BATCH_CLASSES];
     cudaEvent_t fork = nullptr;

@@ -435,214 +435,291 @@ __global__ void __launch_bounds__(kB) k_emit_sorted(EmitParams E, const uint32_t
  * finds every run. */
 
 /* Row order check and partition offsets in one streaming pass over the
- * column array, 16 entries per thread, kTile per block tile (16-byte loads
- * when aligned).  The rows of a tile, [r_lo, r_hi] with r_lo holding its
- * first entry, are staged in shared memory when at most kScanRows of them
- * touch the tile (otherwise row pointers are read from global memory); a
- * thread finds the row of its first entry by binary search and steps
- * forward at each row start.  With ascending rows the count of a row's
- * entries below bound b_q is the position of its first entry >= b_q, so
- * every offset is written once: by the thread holding that entry, or by
- * the thread holding the row's last entry when every entry is below b_q.
- * Empty rows are written by the thread holding the next row start (or the
- * array's last entry, for empty rows at the end).  roff[v*P + q-1] =
- * entries of row v below bounds[q], q = 1..P (bounds[P] = n, so the last
- * is the count of valid ids); lb/le: v's own run, its local entries.
- * flags[0] is set when some row descends (its partition runs are not
- * contiguous), flags[1] when some row repeats an entry; local_total counts
- * entries inside their row's own partition.  symsum checks symmetry: each
- * entry (r, c) with c < n, c != r adds a 32-bit hash of the unordered pair
- * {r, c}, positive when r < c and negative otherwise, so a symmetric graph
- * sums to zero (an asymmetric one does except with probability about
- * 2^-32). */
-constexpr int kScanRows = 2048;
+ * column array, kTile entries per block tile, kTileE consecutive entries
+ * per thread (16-byte loads when aligned).
+ *
+ * With ascending rows the count of a row's entries below bound b_q is the
+ * position of its first entry >= b_q, so a row's offsets change only at a
+ * few entries: its first entry (S), the entries where the partition of the
+ * column rises (C) and its last entry (E).  The per-entry path is the same
+ * for every lane - the entry's partition, the order test, the symmetry
+ * hash and one event bit - and the events are resolved afterwards, the
+ * warp's lanes spread evenly over the warp's events, each re-reading its
+ * entry and the one before it (still in L1).
+ *
+ * Per tile a bitmap marks where non-empty rows start (positions 0..kTile,
+ * the last one meaning that the tile's last row ends with the tile; the
+ * array's end is marked too) and s_rowat[pos] names the row starting at
+ * pos.  The row holding a position is the row of the last start at or
+ * before it - found from the bitmap and a block-wide max-scan of each
+ * thread's last start - or, before the tile's first start, the row holding
+ * the tile's first entry (tile_first, k_scan_prep).  Empty rows hold no
+ * entry; k_scan_prep writes their offsets.
+ *
+ * roff[v*P + q-1] = entries of row v below bounds[q], q = 1..P (bounds[P] =
+ * n, so the last is the count of valid ids); lb/le: v's own run, its local
+ * entries.  flags[0] is set when some row descends (its partition runs are
+ * not contiguous); repeated entries are allowed.  local_total counts the
+ * entries inside their row's own partition, from the events: each own-run
+ * segment adds its end and subtracts its start.  symsum checks symmetry:
+ * each entry (r, c) with c < n adds r*B(c) - B(r)*c (mod 2^32) for a mix B,
+ * antisymmetric in (r, c), so a symmetric graph sums to zero; an entry
+ * without its mirror leaves a term that cancels only by chance (self loops
+ * add zero). */
+constexpr int kScanWords = kTile / 32 + 2; /* start bits 0..kTile, one spare word */
 
-__device__ __forceinline__ uint32_t pair_hash(uint32_t a, uint32_t b)
+__device__ __forceinline__ uint32_t sym_mix(uint32_t x)
 {
-    uint32_t x = a * 0x9E3779B1u ^ (b + 0x7F4A7C15u) * 0x85EBCA77u;
-    x ^= x >> 15;
-    x *= 0x2C1B3C6Du;
-    x ^= x >> 12;
-    return x;
+    x = (x ^ 0x9E3779B9u) * 0x85EBCA6Bu;
+    return x ^ (x >> 16);
+}
+
+/* Offsets and empty runs of every empty row, and the row holding each
+ * tile's first entry (as k_tile_first, width kTile). */
+__global__ void __launch_bounds__(kB) k_scan_prep(const uint64_t *__restrict__ row_ptr, uint32_t n,
+                                                  uint64_t m, uint64_t tiles, uint32_t *first,
+                                                  int P, uint32_t *roff, uint64_t *lb,
+                                                  uint64_t *le)
+{
+    const uint64_t stride = (uint64_t)gridDim.x * kB;
+    for (uint64_t v = (uint64_t)blockIdx.x * kB + threadIdx.x; v <= n; v += stride) {
+        if (v == 0) {
+            first[tiles] = n + 1;
+            uint64_t r0 = __ldg(row_ptr), rn = __ldg(row_ptr + n);
+            r0 = r0 > m ? m : r0;
+            rn = rn > m ? m : rn;
+            for (uint64_t t = 0; t * kTile < r0; ++t)
+                first[t] = 0;
+            for (uint64_t t = (rn + kTile - 1) / kTile; t < tiles; ++t)
+                first[t] = n + 1;
+            continue;
+        }
+        uint64_t a = __ldg(row_ptr + v - 1), b = __ldg(row_ptr + v);
+        if (b > m)
+            b = m;
+        if (a > b)
+            a = b;
+        for (uint64_t t = (a + kTile - 1) / kTile; t * kTile < b; ++t)
+            first[t] = (uint32_t)v;
+        if (a == b) {
+            for (int q = 0; q < P; ++q)
+                roff[(v - 1) * P + q] = 0u;
+            lb[v - 1] = a;
+            le[v - 1] = a;
+        }
+    }
 }
 
 template <int PMAX>
 __global__ void __launch_bounds__(kB) k_row_scan(const uint64_t *__restrict__ row_ptr,
                                                  const uint32_t *__restrict__ col, uint32_t n,
                                                  uint64_t m, const uint32_t *bounds, int parts,
-                                                 int vec, uint32_t *roff, uint64_t *lb,
-                                                 uint64_t *le, unsigned *flags,
-                                                 unsigned long long *local_total,
+                                                 int vec, const uint32_t *__restrict__ tile_first,
+                                                 uint32_t *roff, uint64_t *lb, uint64_t *le,
+                                                 unsigned *flags, unsigned long long *local_total,
                                                  unsigned long long *symsum)
 {
-    __shared__ uint64_t s_rp[kScanRows + 1];
-    __shared__ uint32_t s_b[PMAX + 1];
-    __shared__ uint32_t s_rlo, s_rhi;
-    for (int i = threadIdx.x; i <= PMAX; i += kB)
-        s_b[i] = i <= parts ? bounds[i] : 0xffffffffu;
-    __syncthreads();
-    uint32_t tb[PMAX + 1];
-#pragma unroll
-    for (int i = 0; i <= PMAX; ++i)
-        tb[i] = s_b[i];
+    __shared__ uint32_t s_bits[kScanWords];
+    __shared__ uint32_t s_rowat[kTile + 1];
+    __shared__ int s_wlast[kB / 32];
+    __shared__ uint64_t s_lo_base;
     const int P = parts;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    /* cut[i] = bounds[i] below P, n at P, above every id past P: the
+     * partition of id x is the number of cuts <= x, capped at P */
+    uint32_t cut[PMAX + 1];
+#pragma unroll
+    for (int i = 1; i <= PMAX; ++i)
+        cut[i] = i < P ? __ldg(bounds + i) : i == P ? n : 0xffffffffu;
+    auto part = [&](uint32_t x) {
+        int p = 0;
+#pragma unroll
+        for (int i = 1; i <= PMAX; ++i)
+            p += (int)(x >= cut[i]);
+        return p < P ? p : P;
+    };
     const uint64_t tiles = (m + kTile - 1) / kTile;
-    bool desc = false, dup = false;
-    unsigned long long local = 0, sym = 0;
+    bool desc = false;
+    unsigned long long local = 0;
+    uint32_t sym = 0;
     for (uint64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
         const uint64_t j0 = t * kTile, jend = j0 + kTile < m ? j0 + kTile : m;
-        if (threadIdx.x < 2) {
-            /* the row holding entry j0 (thread 0) or jend - 1 (thread 1):
-             * the last row whose start is <= that entry */
-            const uint64_t key = threadIdx.x ? jend - 1 : j0;
-            uint32_t lo = 0, hi = n; /* row_ptr[lo] <= key < row_ptr[hi] */
-            while (hi - lo > 1) {
-                const uint32_t mid = lo + (hi - lo) / 2;
-                if (__ldg(row_ptr + mid) <= key)
-                    lo = mid;
-                else
-                    hi = mid;
+        const uint32_t tb = threadIdx.x * kTileE; /* first position of this thread */
+        const uint64_t jt = j0 + tb;
+        const int kv = jt >= jend ? 0 : jend - jt < (uint64_t)kTileE ? (int)(jend - jt) : kTileE;
+        uint32_t c[kTileE];
+        if (vec && jt + kTileE <= m) {
+            const uint4 *c4 = reinterpret_cast<const uint4 *>(col + jt);
+#pragma unroll
+            for (int q = 0; q < kTileE / 4; ++q) {
+                const uint4 x = __ldg(c4 + q);
+                c[4 * q] = x.x;
+                c[4 * q + 1] = x.y;
+                c[4 * q + 2] = x.z;
+                c[4 * q + 3] = x.w;
             }
-            if (threadIdx.x)
-                s_rhi = lo;
-            else
-                s_rlo = lo;
+        } else {
+#pragma unroll
+            for (int k = 0; k < kTileE; ++k)
+                c[k] = k < kv ? __ldg(col + jt + k) : 0u;
+        }
+        const uint32_t f0 = __ldg(tile_first + t), f1 = __ldg(tile_first + t + 1);
+        const uint32_t r_lo = f0 ? f0 - 1 : 0u;
+        const uint32_t r_hi = f1 < n ? f1 : n; /* row_ptr[r_hi] > jend - 1 */
+        for (int i = threadIdx.x; i < kScanWords; i += kB)
+            s_bits[i] = 0u;
+        if (threadIdx.x == 0)
+            s_lo_base = __ldg(row_ptr + r_lo);
+        __syncthreads();
+        /* starts of the non-empty rows in [j0, jend]; the array's end */
+        for (uint32_t r = r_lo + threadIdx.x; r < r_hi; r += kB) {
+            const uint64_t a = __ldg(row_ptr + r), b = __ldg(row_ptr + r + 1);
+            if (a < b && a >= j0 && a <= jend) {
+                const uint32_t o = (uint32_t)(a - j0);
+                atomicOr(&s_bits[o >> 5], 1u << (o & 31));
+                s_rowat[o] = r;
+            }
+        }
+        if (threadIdx.x == 0 && jend == m) {
+            const uint32_t o = (uint32_t)(jend - j0);
+            atomicOr(&s_bits[o >> 5], 1u << (o & 31));
         }
         __syncthreads();
-        const uint32_t r_lo = s_rlo, r_hi = s_rhi;
-        const bool staged = (uint64_t)r_hi - r_lo + 1 < (uint64_t)kScanRows;
-        if (staged)
-            for (uint32_t i = threadIdx.x; i <= r_hi - r_lo + 1; i += kB)
-                s_rp[i] = __ldg(row_ptr + r_lo + i);
+        /* this thread's start bits (and the one after them), and the last
+         * start before its first entry: a block-wide max-scan */
+        const uint32_t w0 = threadIdx.x >> 1;
+        const uint64_t ww = (uint64_t)s_bits[w0] | ((uint64_t)s_bits[w0 + 1] << 32);
+        const uint32_t sb = kv ? (uint32_t)(ww >> (16 * (threadIdx.x & 1))) & 0x1FFFFu : 0u;
+        const uint32_t own = sb & 0xFFFFu;
+        const int mylast = own ? (int)(tb + 31 - __clz(own)) : -1;
+        int incl = mylast;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o)
+                incl = y > incl ? y : incl;
+        }
+        if (lane == 31)
+            s_wlast[warp] = incl;
+        int excl = __shfl_up_sync(0xffffffffu, incl, 1);
+        if (lane == 0)
+            excl = -1;
         __syncthreads();
-        auto rp_at = [&](uint64_t r) -> uint64_t {
-            return (staged && r >= r_lo && r <= (uint64_t)r_hi + 1) ? s_rp[r - r_lo]
-                                                                     : __ldg(row_ptr + r);
-        };
-        const uint64_t jt = j0 + (uint64_t)threadIdx.x * kTileE;
-        if (jt < jend) {
-            uint32_t c[kTileE];
-            if (vec && jt + kTileE <= m) {
-                const uint4 *c4 = reinterpret_cast<const uint4 *>(col + jt);
 #pragma unroll
-                for (int q = 0; q < kTileE / 4; ++q) {
-                    const uint4 x = __ldg(c4 + q);
-                    c[4 * q] = x.x;
-                    c[4 * q + 1] = x.y;
-                    c[4 * q + 2] = x.z;
-                    c[4 * q + 3] = x.w;
-                }
-            } else {
-#pragma unroll
-                for (int k = 0; k < kTileE; ++k)
-                    c[k] = jt + k < m ? __ldg(col + jt + k) : 0u;
-            }
-            /* row of jt: last r in [r_lo, r_hi] with row_ptr[r] <= jt */
-            uint32_t lo = r_lo, hi = r_hi + 1;
-            while (hi - lo > 1) {
-                const uint32_t mid = lo + (hi - lo) / 2;
-                if (rp_at(mid) <= jt)
-                    lo = mid;
-                else
-                    hi = mid;
-            }
-            uint32_t r = lo;
-            uint64_t rbase = rp_at(r), rend = rp_at((uint64_t)r + 1);
-            int pr = 0;
-#pragma unroll
-            for (int i = 1; i < PMAX; ++i)
-                pr += (int)(r >= tb[i]);
-            int prevpart = -1;
-            uint32_t prev = 0;
-            if (jt > rbase) {
-                prev = __ldg(col + jt - 1);
-                int pp = 0;
-#pragma unroll
-                for (int i = 1; i <= PMAX; ++i)
-                    pp += (int)(i <= P && prev >= tb[i]);
-                prevpart = pp;
-            }
-            const int kv = jend - jt < (uint64_t)kTileE ? (int)(jend - jt) : kTileE;
-            auto event = [&](int q, uint64_t off) {
-                if (q >= 1)
-                    roff[(uint64_t)r * P + q - 1] = (uint32_t)off;
-                if (q == pr)
-                    lb[r] = rbase + off;
-                if (q == pr + 1)
-                    le[r] = rbase + off;
-            };
+        for (int w = 0; w < kB / 32; ++w)
+            if (w < warp)
+                excl = s_wlast[w] > excl ? s_wlast[w] : excl;
+        uint32_t evmask = 0;
+        const uint32_t up = __shfl_up_sync(0xffffffffu, c[kTileE - 1], 1);
+        if (kv > 0) {
+            uint32_t r = excl >= 0 ? s_rowat[excl] : r_lo;
+            uint32_t br = sym_mix(r);
+            /* the entry before jt: the previous lane's last, or a load (not
+             * needed at a row start) */
+            uint32_t prev = lane ? up : (!(own & 1u) && jt > 0 ? __ldg(col + jt - 1) : 0u);
+            int pp = part(prev);
 #pragma unroll
             for (int k = 0; k < kTileE; ++k) {
-                if (k >= kv)
-                    break;
-                const uint64_t j = jt + k;
-                if (j == rend) { /* a row start: the next non-empty row */
-                    while ((uint64_t)r + 1 < n && rp_at((uint64_t)r + 1) <= j)
-                        ++r;
-                    rbase = j;
-                    rend = rp_at((uint64_t)r + 1);
-                    pr = 0;
-#pragma unroll
-                    for (int i = 1; i < PMAX; ++i)
-                        pr += (int)(r >= tb[i]);
-                    prevpart = -1;
-                }
-                if (j == rbase) {
-                    /* empty rows just before this row start hold no entry:
-                     * their offsets and runs are all zero */
-                    for (uint64_t e = r; e > 0 && rp_at(e - 1) == j; --e) {
-                        const uint64_t er = e - 1;
-                        for (int q = 0; q < P; ++q)
-                            roff[er * P + q] = 0u;
-                        lb[er] = j;
-                        le[er] = j;
+                if (k < kv) {
+                    const uint32_t x = c[k];
+                    const bool st = (sb >> k) & 1u;
+                    const int p = part(x);
+                    if (st) {
+                        r = s_rowat[tb + k];
+                        br = sym_mix(r);
                     }
-                } else {
-                    desc |= c[k] < prev;
-                    dup |= c[k] == prev;
+                    desc |= !st && x < prev;
+                    const bool ev = st || p > pp || ((sb >> (k + 1)) & 1u);
+                    evmask |= (uint32_t)ev << k;
+                    if (p < P)
+                        sym += r * sym_mix(x) - br * x;
+                    prev = x;
+                    pp = p;
                 }
-                int pv = 0;
-#pragma unroll
-                for (int i = 1; i <= PMAX; ++i)
-                    pv += (int)(i <= P && c[k] >= tb[i]);
-                local += (pv == pr);
-                if (c[k] < n && c[k] != r) {
-                    const uint32_t h = c[k] < r ? pair_hash(c[k], r) : pair_hash(r, c[k]);
-                    sym += r < c[k] ? (unsigned long long)h : 0ull - (unsigned long long)h;
-                }
-                for (int q = prevpart + 1; q <= pv; ++q)
-                    event(q, j - rbase);
-                if (pv > prevpart)
-                    prevpart = pv;
-                prev = c[k];
-                if (j + 1 == rend)
-                    for (int q = prevpart + 1; q <= P; ++q)
-                        event(q, rend - rbase);
-                if (j + 1 == m)
-                    /* empty rows after the last entry */
-                    for (uint64_t er = (uint64_t)r + 1; er < n; ++er) {
-                        for (int q = 0; q < P; ++q)
-                            roff[er * P + q] = 0u;
-                        lb[er] = m;
-                        le[er] = m;
-                    }
             }
         }
-        __syncthreads(); /* s_rp, s_rlo, s_rhi are rewritten by the next tile */
+        /* the warp's events, spread over its lanes: event i of the warp is
+         * the (i - before)-th set bit of the lane that holds it */
+        const uint32_t cnt = __popc(evmask);
+        uint32_t ci = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, ci, o);
+            if (lane >= o)
+                ci += y;
+        }
+        const uint32_t total = __shfl_sync(0xffffffffu, ci, 31);
+        for (uint32_t i0 = 0; i0 < total; i0 += 32) {
+            const uint32_t i = i0 + lane;
+            /* owner: the first lane whose inclusive count exceeds i */
+            int ow = 0;
+#pragma unroll
+            for (int s = 16; s > 0; s >>= 1) {
+                const uint32_t y = __shfl_sync(0xffffffffu, ci, ow + s - 1);
+                if (y <= i)
+                    ow += s;
+            }
+            const uint32_t om = __shfl_sync(0xffffffffu, evmask, ow);
+            const uint32_t ob = __shfl_sync(0xffffffffu, ci - cnt, ow);
+            const uint32_t osb = __shfl_sync(0xffffffffu, sb, ow);
+            const int oex = __shfl_sync(0xffffffffu, excl, ow);
+            if (i >= total)
+                continue;
+            uint32_t mm = om; /* drop the lower set bits, then the lowest left */
+            for (uint32_t d = i - ob; d > 0; --d)
+                mm &= mm - 1u;
+            const int k = __ffs(mm) - 1;
+            const uint32_t o = (uint32_t)(warp * 32 + ow) * kTileE + k;
+            const uint64_t j = j0 + o;
+            /* the row of j: the last start at or before it */
+            const uint32_t below = osb & ((2u << k) - 1u) & 0xFFFFu;
+            const int ls = below ? (int)(o - k + 31 - __clz(below)) : oex;
+            const uint32_t r = ls >= 0 ? s_rowat[ls] : r_lo;
+            const uint64_t rbase = ls >= 0 ? j0 + ls : s_lo_base;
+            const int pr = part(r);
+            const bool st = (osb >> k) & 1u, en = (osb >> (k + 1)) & 1u;
+            const int pj = part(__ldg(col + j));
+            const int pp = st || j == 0 ? -1 : part(__ldg(col + j - 1));
+            uint32_t *ro = roff + (uint64_t)r * P;
+            if (st || pj > pp) {
+                for (int q = pp + 1; q <= pj; ++q) {
+                    if (q >= 1)
+                        ro[q - 1] = (uint32_t)(j - rbase);
+                    if (q == pr)
+                        lb[r] = j;
+                    if (q == pr + 1)
+                        le[r] = j;
+                }
+                if (pj == pr)
+                    local -= j;
+                if (pp == pr)
+                    local += j;
+            }
+            if (en) {
+                for (int q = pj + 1; q <= P; ++q) {
+                    ro[q - 1] = (uint32_t)(j + 1 - rbase);
+                    if (q == pr)
+                        lb[r] = j + 1;
+                    if (q == pr + 1)
+                        le[r] = j + 1;
+                }
+                if (pj == pr)
+                    local += j + 1;
+            }
+        }
+        __syncthreads(); /* s_bits, s_rowat are rewritten by the next tile */
     }
-    const int lane = threadIdx.x & 31;
     for (int o = 16; o > 0; o >>= 1) {
         local += __shfl_xor_sync(0xffffffffu, local, o);
         sym += __shfl_xor_sync(0xffffffffu, sym, o);
     }
+    const bool any_desc = __any_sync(0xffffffffu, desc);
     if (lane == 0 && local)
         atomicAdd(local_total, local);
     if (lane == 0 && sym)
-        atomicAdd(symsum, sym);
-    if (__any_sync(0xffffffffu, desc) && lane == 0)
+        atomicAdd(symsum, (unsigned long long)sym);
+    if (lane == 0 && any_desc)
         atomicOr(flags, 1u);
-    if (__any_sync(0xffffffffu, dup) && lane == 0)
-        atomicOr(flags + 1, 1u);
 }
 
 /* Sorted-row mode, remote end, from the partition offsets: row u's run in
@@ -2145,14 +2222,20 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
                 /* [0] local entries, [1] symmetry sum */
                 CC_TRY(cc_bufs_get(&B, (void **)&local_total, 2 * sizeof(unsigned long long)));
                 CC_CUDA(cudaMemsetAsync(local_total, 0, 2 * sizeof(unsigned long long), st));
+                /* tile starts (the same array tiles_of() builds) and the
+                 * empty rows' offsets */
+                CC_TRY(cc_bufs_get(&B, (void **)&tile_first, (Lp.tiles + 1) * sizeof(uint32_t)));
+                col_tiles = Lp.tiles;
+                CC_KLAUNCH(ctx, CCK_DIST_TILES, k_scan_prep, vb, kB, 0, st, d_row_ptr, n, m,
+                           Lp.tiles, tile_first, P, roff, rlb, rle);
                 const unsigned scan_b = cc_blocks(Lp.tiles, 1, (unsigned)ctx->sm_count * 8);
                 if (P <= 4)
                     CC_KLAUNCH(ctx, CCK_DIST_LOCAL_COUNT, k_row_scan<4>, scan_b, kB, 0, st,
-                               d_row_ptr, d_col, n, m, bounds, P, Lp.vec, roff, rlb, rle, rflags,
+                               d_row_ptr, d_col, n, m, bounds, P, Lp.vec, tile_first, roff, rlb, rle, rflags,
                                local_total, local_total + 1);
                 else
                     CC_KLAUNCH(ctx, CCK_DIST_LOCAL_COUNT, k_row_scan<8>, scan_b, kB, 0, st,
-                               d_row_ptr, d_col, n, m, bounds, P, Lp.vec, roff, rlb, rle, rflags,
+                               d_row_ptr, d_col, n, m, bounds, P, Lp.vec, tile_first, roff, rlb, rle, rflags,
                                local_total, local_total + 1);
             }
             l_rp = rlb;
@@ -2336,7 +2419,7 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
         }
         /* the run counts need a symmetric graph, the mirror marks strictly
          * ascending rows with every mirror present */
-        const bool redo = ranges ? hl[1] != 0 : (hc[6] || hf[1]);
+        const bool redo = ranges ? (uint32_t)hl[1] != 0u : (hc[6] || hf[1]);
         if (sorted_mode && redo) {
             E.ngbits = nullptr;
             E.roff = nullptr;

@@ -61,14 +61,20 @@ extern "C" int ccgpu_graph_upload(const uint64_t *h_row_ptr, const uint32_t *h_c
     cudaGetDevice(&g->device);
     g->n = n;
     g->m = m;
-    cudaError_t e = cudaMalloc(&g->row_ptr, ((size_t)n + 1) * sizeof(uint64_t));
+    /* stream-ordered pool memory: a graph uploaded again after one was
+     * freed reuses the pool's pages instead of mapping new ones */
+    CC_TRY(cc_pool_tune());
+    cudaError_t e = cudaMallocAsync((void **)&g->row_ptr, ((size_t)n + 1) * sizeof(uint64_t), 0);
     if (e == cudaSuccess)
-        e = cudaMalloc(&g->col, (size_t)(m ? m : 1) * sizeof(uint32_t));
+        e = cudaMallocAsync((void **)&g->col, (size_t)(m ? m : 1) * sizeof(uint32_t), 0);
     if (e == cudaSuccess)
-        e = cudaMemcpy(g->row_ptr, h_row_ptr, ((size_t)n + 1) * sizeof(uint64_t),
-                       cudaMemcpyHostToDevice);
+        e = cudaMemcpyAsync(g->row_ptr, h_row_ptr, ((size_t)n + 1) * sizeof(uint64_t),
+                            cudaMemcpyHostToDevice, 0);
     if (e == cudaSuccess && m)
-        e = cudaMemcpy(g->col, h_col_idx, (size_t)m * sizeof(uint32_t), cudaMemcpyHostToDevice);
+        e = cudaMemcpyAsync(g->col, h_col_idx, (size_t)m * sizeof(uint32_t),
+                            cudaMemcpyHostToDevice, 0);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(0);
     if (e != cudaSuccess) {
         int rc = ccgpu_cuda_fail(e, "ccgpu_graph_upload", __FILE__, __LINE__);
         ccgpu_graph_free(g);
@@ -82,8 +88,20 @@ extern "C" void ccgpu_graph_free(ccgpu_graph *g)
 {
     if (!g)
         return;
-    cudaFree(g->row_ptr);
-    cudaFree(g->col);
+    /* like cudaFree, wait for work that may still read the arrays; the
+     * pool memory goes back on the graph's own device */
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (cur != g->device)
+        cudaSetDevice(g->device);
+    cudaDeviceSynchronize();
+    if (g->row_ptr)
+        cudaFreeAsync(g->row_ptr, 0);
+    if (g->col)
+        cudaFreeAsync(g->col, 0);
+    cudaStreamSynchronize(0);
+    if (cur >= 0 && cur != g->device)
+        cudaSetDevice(cur);
     free(g);
 }
 
@@ -188,7 +206,11 @@ extern "C" int ccgpu_graph_from_csc(const uint64_t *h_jc, const uint32_t *h_ir, 
     if (rc == CCGPU_OK) {
         cudaGetDevice(&g->device);
         g->n = nrows;
-        cuda(cudaMalloc(&g->row_ptr, ((size_t)nrows + 1) * sizeof(uint64_t)), __LINE__);
+        rc = cc_pool_tune();
+    }
+    if (rc == CCGPU_OK) {
+        cuda(cudaMallocAsync((void **)&g->row_ptr, ((size_t)nrows + 1) * sizeof(uint64_t), st),
+             __LINE__);
     }
     if (rc == CCGPU_OK)
         rc = cc_bufs_get(&B, (void **)&d_jc, ((size_t)ncols + 1) * sizeof(uint64_t));
@@ -222,7 +244,8 @@ extern "C" int ccgpu_graph_from_csc(const uint64_t *h_jc, const uint32_t *h_ir, 
     }
     if (rc == CCGPU_OK) {
         g->m = m;
-        cuda(cudaMalloc(&g->col, (size_t)(m ? m : 1) * sizeof(uint32_t)), __LINE__);
+        cuda(cudaMallocAsync((void **)&g->col, (size_t)(m ? m : 1) * sizeof(uint32_t), st),
+             __LINE__);
     }
     if (rc == CCGPU_OK && m) {
         CC_KLAUNCH(ctx, CCK_MISC, k_csc_cols, cc_blocks(m, kCsc, grid), kCsc, 0, st, sorted, m,

@@ -17,7 +17,7 @@
 
 /* ------------------------------------------------------------- buffers */
 
-int cc_bufs_init(DevBufs *b, cudaStream_t st)
+int cc_pool_tune(void)
 {
     static thread_local int pool_tuned = -1;
     int dev = 0;
@@ -29,6 +29,12 @@ int cc_bufs_init(DevBufs *b, cudaStream_t st)
         CC_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thresh));
         pool_tuned = dev;
     }
+    return CCGPU_OK;
+}
+
+int cc_bufs_init(DevBufs *b, cudaStream_t st)
+{
+    CC_TRY(cc_pool_tune());
     b->st = st;
     b->n = 0;
     return CCGPU_OK;

@@ -17,6 +17,9 @@ struct DevBufs {
     int n;
 };
 int cc_bufs_init(DevBufs *b, cudaStream_t st);
+/* Raises the release threshold of the current device's default pool (once
+ * per thread and device). */
+int cc_pool_tune(void);
 int cc_bufs_get(DevBufs *b, void **p, size_t bytes);
 void cc_bufs_release(DevBufs *b);
 

@@ -343,6 +343,15 @@ typedef struct {
     float class_bounds[CCGPU_BATCH_CLASSES - 1]; /* mean-row-length cut points (6, 16) */
     int heavy_degree;                            /* rows above it are queued (8192)    */
     ccgpu_batch_class_opts cls[CCGPU_BATCH_CLASSES];
+    int persistent;   /* 1: each class is one persistent launch that moves every
+                       * graph through init, sampling, shortcuts, giant, finish and
+                       * final by per-graph phase counters (0: one launch per
+                       * phase)                                                  */
+    int wait_ms;      /* persistent: limit of one wait on a graph's previous phase
+                       * (0 = 2000); a wait that runs out ends the launch and the
+                       * results call returns CCGPU_ERR_TIMEOUT                   */
+    int stall_graph;  /* test aid, -1 = off: graph whose first wait can never be
+                       * met, to exercise the bounded wait                        */
 } ccgpu_batch_tuning;
 
 void ccgpu_batch_tuning_default(ccgpu_batch_tuning *t);
@@ -366,7 +375,9 @@ int ccgpu_batch_plan_tuning(const ccgpu_batch_plan *p, ccgpu_batch_tuning *out);
 /* Graphs per class (array of CCGPU_BATCH_CLASSES). */
 int ccgpu_batch_plan_class_graphs(const ccgpu_batch_plan *p, uint32_t *counts);
 /* Per-graph component counts and done flags of the last solve (host arrays
- * of G entries, either may be NULL).  Synchronous on `stream`. */
+ * of G entries, either may be NULL).  Synchronous on `stream`.
+ * CCGPU_ERR_TIMEOUT when a persistent launch gave up a wait (graphs whose
+ * done flag is 0 were not solved). */
 int ccgpu_batch_plan_results(ccgpu_batch_plan *p, uint32_t *h_components, uint32_t *h_done,
                              void *stream);
 void ccgpu_batch_plan_destroy(ccgpu_batch_plan *p);

@@ -184,3 +184,81 @@ def test_mixed_batch_matches_plain_kernel_and_autotune(torch):
         assert (batch.labels_of(lab, vo, g) == ref).all(), g
         assert comps[g] == oracle.count_components(ref)
     plan.close()
+
+
+def persistent(t=None, **kw):
+    t = t or batch.default_tuning()
+    t.persistent = 1
+    for k, v in kw.items():
+        setattr(t, k, v)
+    return t
+
+
+@pytest.mark.parametrize("sched", SCHEDULES[:6], ids=[str(s) for s in SCHEDULES[:6]])
+def test_persistent_launch_matches_oracle(torch, sched):
+    """One persistent launch per class (work items in phase order, per-graph
+    phase counters) gives every graph the oracle's labels, replay after
+    replay, under the schedules the autotuner can pick."""
+    gs = small_batch(seed=29, count=50)
+    vo, eo, d_rp, d_col, d_lab = to_device(torch, gs)
+    plan = batch.BatchPlan(vo, eo, d_rp, d_col, d_lab,
+                           tuning=persistent(tuning_with(**sched)))
+    for _ in range(2):
+        d_lab.fill_(-3)
+        plan.launch()
+        comps, done = plan.results()
+        check_oracle(torch, gs, vo, d_lab, comps, done)
+    assert plan.kernels() <= batch.CLASSES
+    plan.close()
+
+
+def test_persistent_mixed_batch_matches_phase_launches(torch):
+    spec = batch.mix_spec(graphs=120, n_min=1000, n_max=200_000, seed=5)
+    vo, eo, d_rp, d_col, kinds = batch.build_batch_torch(torch, spec)
+    d_a = torch.full((int(vo[-1]),), -1, dtype=torch.int32, device="cuda")
+    d_b = torch.full_like(d_a, -2)
+    plan_a = batch.BatchPlan(vo, eo, d_rp, d_col, d_a)
+    plan_b = batch.BatchPlan(vo, eo, d_rp, d_col, d_b, tuning=persistent(heavy_degree=256))
+    plan_a.launch()
+    plan_b.launch()
+    torch.cuda.synchronize()
+    assert torch.equal(d_a, d_b)
+    comps_a, _ = plan_a.results()
+    comps_b, done_b = plan_b.results()
+    assert (comps_a == comps_b).all() and (done_b == 1).all()
+    lab = d_b.cpu().numpy().view(np.uint32)
+    for g in range(0, len(spec), 17):
+        a, n = int(vo[g]), int(vo[g + 1] - vo[g])
+        rp = d_rp[a + g:a + g + n + 1].cpu().numpy().view(np.uint64)
+        col = d_col[int(eo[g]):int(eo[g + 1])].cpu().numpy().view(np.uint32)
+        assert (batch.labels_of(lab, vo, g) == oracle.uf_labels(rp, col)).all(), g
+    plan_a.close()
+    plan_b.close()
+
+
+def test_persistent_wait_runs_out_and_reports(torch):
+    """A graph whose first wait can never be met (the stall_graph test aid):
+    the bounded wait runs out after wait_ms, the launch ends, the results
+    call returns CCGPU_ERR_TIMEOUT, and the same plan solves the batch
+    afterwards once the aid is off."""
+    import ctypes as C
+    gs = small_batch(seed=31, count=30)
+    vo, eo, d_rp, d_col, d_lab = to_device(torch, gs)
+    stalled = next(g for g in range(len(gs)) if vo[g + 1] > vo[g])
+    L = batch._bind()
+    plan = batch.BatchPlan(vo, eo, d_rp, d_col, d_lab,
+                           tuning=persistent(wait_ms=50, stall_graph=stalled))
+    plan.launch()
+    torch.cuda.synchronize()
+    comps = np.zeros(len(gs), np.uint32)
+    done = np.zeros(len(gs), np.uint32)
+    rc = L.ccgpu_batch_plan_results(plan.p, comps.ctypes.data, done.ctypes.data,
+                                    torch.cuda.current_stream().cuda_stream)
+    assert rc == 4  # CCGPU_ERR_TIMEOUT
+    assert done[stalled] == 0
+    plan.close()
+    plan = batch.BatchPlan(vo, eo, d_rp, d_col, d_lab, tuning=persistent(wait_ms=50))
+    plan.launch()
+    comps2, done2 = plan.results()
+    check_oracle(torch, gs, vo, d_lab, comps2, done2)
+    plan.close()
