@@ -435,8 +435,9 @@ __global__ void __launch_bounds__(kB) k_emit_sorted(EmitParams E, const uint32_t
  * finds every run. */
 
 /* Row order check and partition offsets in one streaming pass over the
- * column array, kTile entries per block tile, kTileE consecutive entries
- * per thread (16-byte loads when aligned).
+ * column array.  Each warp takes chunks of kChunk consecutive entries,
+ * kTileE per lane (16-byte loads when aligned), and works on them alone:
+ * no block barrier, so a warp with many events never holds up the others.
  *
  * With ascending rows the count of a row's entries below bound b_q is the
  * position of its first entry >= b_q, so a row's offsets change only at a
@@ -444,16 +445,16 @@ __global__ void __launch_bounds__(kB) k_emit_sorted(EmitParams E, const uint32_t
  * column rises (C) and its last entry (E).  The per-entry path is the same
  * for every lane - the entry's partition, the order test, the symmetry
  * hash and one event bit - and the events are resolved afterwards, the
- * warp's lanes spread evenly over the warp's events, each re-reading its
- * entry and the one before it (still in L1).
+ * warp's lanes spread evenly over the chunk's events, each re-reading its
+ * entry and the one before it (in L1).
  *
- * Per tile a bitmap marks where non-empty rows start (positions 0..kTile,
- * the last one meaning that the tile's last row ends with the tile; the
- * array's end is marked too) and s_rowat[pos] names the row starting at
- * pos.  The row holding a position is the row of the last start at or
- * before it - found from the bitmap and a block-wide max-scan of each
- * thread's last start - or, before the tile's first start, the row holding
- * the tile's first entry (tile_first, k_scan_prep).  Empty rows hold no
+ * Per chunk a bitmap marks where non-empty rows start (positions
+ * 0..kChunk, the last one meaning that the chunk's last row ends with the
+ * chunk; the array's end is marked too) and rowat[pos] names the row
+ * starting at pos.  The row holding a position is the row of the last
+ * start at or before it - found from the bitmap and a warp max-scan of each
+ * lane's last start - or, before the chunk's first start, the row holding
+ * the chunk's first entry (chunk_first, k_scan_prep).  Empty rows hold no
  * entry; k_scan_prep writes their offsets.
  *
  * roff[v*P + q-1] = entries of row v below bounds[q], q = 1..P (bounds[P] =
@@ -462,11 +463,12 @@ __global__ void __launch_bounds__(kB) k_emit_sorted(EmitParams E, const uint32_t
  * not contiguous); repeated entries are allowed.  local_total counts the
  * entries inside their row's own partition, from the events: each own-run
  * segment adds its end and subtracts its start.  symsum checks symmetry:
- * each entry (r, c) with c < n adds r*B(c) - B(r)*c (mod 2^32) for a mix B,
- * antisymmetric in (r, c), so a symmetric graph sums to zero; an entry
- * without its mirror leaves a term that cancels only by chance (self loops
- * add zero). */
-constexpr int kScanWords = kTile / 32 + 2; /* start bits 0..kTile, one spare word */
+ * each entry (r, c) with c < n adds r*B(c) - B(r)*c (mod 2^32) for a
+ * multiply-xorshift mix B, antisymmetric in (r, c), so a symmetric graph
+ * sums to zero; an entry without its mirror leaves a term that cancels only
+ * by chance (self loops add zero). */
+constexpr int kChunk = 32 * kTileE;           /* entries per warp chunk          */
+constexpr int kChunkWords = kChunk / 32 + 2;  /* start bits 0..kChunk, one spare */
 
 __device__ __forceinline__ uint32_t sym_mix(uint32_t x)
 {
@@ -475,22 +477,22 @@ __device__ __forceinline__ uint32_t sym_mix(uint32_t x)
 }
 
 /* Offsets and empty runs of every empty row, and the row holding each
- * tile's first entry (as k_tile_first, width kTile). */
+ * chunk's first entry (as k_tile_first, width kChunk). */
 __global__ void __launch_bounds__(kB) k_scan_prep(const uint64_t *__restrict__ row_ptr, uint32_t n,
-                                                  uint64_t m, uint64_t tiles, uint32_t *first,
+                                                  uint64_t m, uint64_t chunks, uint32_t *first,
                                                   int P, uint32_t *roff, uint64_t *lb,
                                                   uint64_t *le)
 {
     const uint64_t stride = (uint64_t)gridDim.x * kB;
     for (uint64_t v = (uint64_t)blockIdx.x * kB + threadIdx.x; v <= n; v += stride) {
         if (v == 0) {
-            first[tiles] = n + 1;
+            first[chunks] = n + 1;
             uint64_t r0 = __ldg(row_ptr), rn = __ldg(row_ptr + n);
             r0 = r0 > m ? m : r0;
             rn = rn > m ? m : rn;
-            for (uint64_t t = 0; t * kTile < r0; ++t)
+            for (uint64_t t = 0; t * kChunk < r0; ++t)
                 first[t] = 0;
-            for (uint64_t t = (rn + kTile - 1) / kTile; t < tiles; ++t)
+            for (uint64_t t = (rn + kChunk - 1) / kChunk; t < chunks; ++t)
                 first[t] = n + 1;
             continue;
         }
@@ -499,7 +501,7 @@ __global__ void __launch_bounds__(kB) k_scan_prep(const uint64_t *__restrict__ r
             b = m;
         if (a > b)
             a = b;
-        for (uint64_t t = (a + kTile - 1) / kTile; t * kTile < b; ++t)
+        for (uint64_t t = (a + kChunk - 1) / kChunk; t * kChunk < b; ++t)
             first[t] = (uint32_t)v;
         if (a == b) {
             for (int q = 0; q < P; ++q)
@@ -510,41 +512,40 @@ __global__ void __launch_bounds__(kB) k_scan_prep(const uint64_t *__restrict__ r
     }
 }
 
-template <int PMAX>
-__global__ void __launch_bounds__(kB) k_row_scan(const uint64_t *__restrict__ row_ptr,
+template <int P>
+__global__ void __launch_bounds__(kB, 4) k_row_scan(const uint64_t *__restrict__ row_ptr,
                                                  const uint32_t *__restrict__ col, uint32_t n,
-                                                 uint64_t m, const uint32_t *bounds, int parts,
-                                                 int vec, const uint32_t *__restrict__ tile_first,
+                                                 uint64_t m, const uint32_t *bounds, int vec,
+                                                 const uint32_t *__restrict__ chunk_first,
                                                  uint32_t *roff, uint64_t *lb, uint64_t *le,
                                                  unsigned *flags, unsigned long long *local_total,
                                                  unsigned long long *symsum)
 {
-    __shared__ uint32_t s_bits[kScanWords];
-    __shared__ uint32_t s_rowat[kTile + 1];
-    __shared__ int s_wlast[kB / 32];
-    __shared__ uint64_t s_lo_base;
-    const int P = parts;
+    __shared__ uint32_t s_bits[kW][kChunkWords];
+    __shared__ uint32_t s_rowat[kW][kChunk + 1];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    /* cut[i] = bounds[i] below P, n at P, above every id past P: the
-     * partition of id x is the number of cuts <= x, capped at P */
-    uint32_t cut[PMAX + 1];
+    uint32_t *bits = s_bits[warp], *rowat = s_rowat[warp];
+    /* cut[i] = bounds[i] below P, n at P: the partition of id x is the
+     * number of cuts <= x (P for ids >= n) */
+    uint32_t cut[P + 1];
 #pragma unroll
-    for (int i = 1; i <= PMAX; ++i)
-        cut[i] = i < P ? __ldg(bounds + i) : i == P ? n : 0xffffffffu;
+    for (int i = 1; i < P; ++i)
+        cut[i] = __ldg(bounds + i);
+    cut[P] = n;
     auto part = [&](uint32_t x) {
         int p = 0;
 #pragma unroll
-        for (int i = 1; i <= PMAX; ++i)
+        for (int i = 1; i <= P; ++i)
             p += (int)(x >= cut[i]);
-        return p < P ? p : P;
+        return p;
     };
-    const uint64_t tiles = (m + kTile - 1) / kTile;
+    const uint64_t chunks = (m + kChunk - 1) / kChunk;
     bool desc = false;
     unsigned long long local = 0;
     uint32_t sym = 0;
-    for (uint64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
-        const uint64_t j0 = t * kTile, jend = j0 + kTile < m ? j0 + kTile : m;
-        const uint32_t tb = threadIdx.x * kTileE; /* first position of this thread */
+    for (uint64_t t = (uint64_t)blockIdx.x * kW + warp; t < chunks; t += (uint64_t)gridDim.x * kW) {
+        const uint64_t j0 = t * kChunk, jend = j0 + kChunk < m ? j0 + kChunk : m;
+        const uint32_t tb = lane * kTileE; /* first position of this lane */
         const uint64_t jt = j0 + tb;
         const int kv = jt >= jend ? 0 : jend - jt < (uint64_t)kTileE ? (int)(jend - jt) : kTileE;
         uint32_t c[kTileE];
@@ -563,33 +564,31 @@ __global__ void __launch_bounds__(kB) k_row_scan(const uint64_t *__restrict__ ro
             for (int k = 0; k < kTileE; ++k)
                 c[k] = k < kv ? __ldg(col + jt + k) : 0u;
         }
-        const uint32_t f0 = __ldg(tile_first + t), f1 = __ldg(tile_first + t + 1);
+        const uint32_t f0 = __ldg(chunk_first + t), f1 = __ldg(chunk_first + t + 1);
         const uint32_t r_lo = f0 ? f0 - 1 : 0u;
         const uint32_t r_hi = f1 < n ? f1 : n; /* row_ptr[r_hi] > jend - 1 */
-        for (int i = threadIdx.x; i < kScanWords; i += kB)
-            s_bits[i] = 0u;
-        if (threadIdx.x == 0)
-            s_lo_base = __ldg(row_ptr + r_lo);
-        __syncthreads();
+        if (lane < kChunkWords)
+            bits[lane] = 0u;
+        __syncwarp();
         /* starts of the non-empty rows in [j0, jend]; the array's end */
-        for (uint32_t r = r_lo + threadIdx.x; r < r_hi; r += kB) {
+        for (uint32_t r = r_lo + lane; r < r_hi; r += 32) {
             const uint64_t a = __ldg(row_ptr + r), b = __ldg(row_ptr + r + 1);
             if (a < b && a >= j0 && a <= jend) {
                 const uint32_t o = (uint32_t)(a - j0);
-                atomicOr(&s_bits[o >> 5], 1u << (o & 31));
-                s_rowat[o] = r;
+                atomicOr(&bits[o >> 5], 1u << (o & 31));
+                rowat[o] = r;
             }
         }
-        if (threadIdx.x == 0 && jend == m) {
+        if (lane == 0 && jend == m) {
             const uint32_t o = (uint32_t)(jend - j0);
-            atomicOr(&s_bits[o >> 5], 1u << (o & 31));
+            atomicOr(&bits[o >> 5], 1u << (o & 31));
         }
-        __syncthreads();
-        /* this thread's start bits (and the one after them), and the last
-         * start before its first entry: a block-wide max-scan */
-        const uint32_t w0 = threadIdx.x >> 1;
-        const uint64_t ww = (uint64_t)s_bits[w0] | ((uint64_t)s_bits[w0 + 1] << 32);
-        const uint32_t sb = kv ? (uint32_t)(ww >> (16 * (threadIdx.x & 1))) & 0x1FFFFu : 0u;
+        __syncwarp();
+        /* this lane's start bits (and the one after them), and the last
+         * start before its first entry: a warp max-scan */
+        const uint32_t w0 = lane >> 1;
+        const uint64_t ww = (uint64_t)bits[w0] | ((uint64_t)bits[w0 + 1] << 32);
+        const uint32_t sb = kv ? (uint32_t)(ww >> (16 * (lane & 1))) & 0x1FFFFu : 0u;
         const uint32_t own = sb & 0xFFFFu;
         const int mylast = own ? (int)(tb + 31 - __clz(own)) : -1;
         int incl = mylast;
@@ -599,47 +598,47 @@ __global__ void __launch_bounds__(kB) k_row_scan(const uint64_t *__restrict__ ro
             if (lane >= o)
                 incl = y > incl ? y : incl;
         }
-        if (lane == 31)
-            s_wlast[warp] = incl;
         int excl = __shfl_up_sync(0xffffffffu, incl, 1);
         if (lane == 0)
             excl = -1;
-        __syncthreads();
-#pragma unroll
-        for (int w = 0; w < kB / 32; ++w)
-            if (w < warp)
-                excl = s_wlast[w] > excl ? s_wlast[w] : excl;
         uint32_t evmask = 0;
         const uint32_t up = __shfl_up_sync(0xffffffffu, c[kTileE - 1], 1);
         if (kv > 0) {
-            uint32_t r = excl >= 0 ? s_rowat[excl] : r_lo;
+            uint32_t r = excl >= 0 ? rowat[excl] : r_lo;
             uint32_t br = sym_mix(r);
             /* the entry before jt: the previous lane's last, or a load (not
              * needed at a row start) */
             uint32_t prev = lane ? up : (!(own & 1u) && jt > 0 ? __ldg(col + jt - 1) : 0u);
             int pp = part(prev);
-#pragma unroll
-            for (int k = 0; k < kTileE; ++k) {
-                if (k < kv) {
-                    const uint32_t x = c[k];
-                    const bool st = (sb >> k) & 1u;
-                    const int p = part(x);
-                    if (st) {
-                        r = s_rowat[tb + k];
-                        br = sym_mix(r);
-                    }
-                    desc |= !st && x < prev;
-                    const bool ev = st || p > pp || ((sb >> (k + 1)) & 1u);
-                    evmask |= (uint32_t)ev << k;
-                    if (p < P)
-                        sym += r * sym_mix(x) - br * x;
-                    prev = x;
-                    pp = p;
+            auto entry = [&](int k) {
+                const uint32_t x = c[k];
+                const bool st = (sb >> k) & 1u;
+                const int p = part(x);
+                if (st) {
+                    r = rowat[tb + k];
+                    br = sym_mix(r);
                 }
+                desc |= !st && x < prev;
+                const bool ev = st || p > pp || ((sb >> (k + 1)) & 1u);
+                evmask |= (uint32_t)ev << k;
+                if (p < P)
+                    sym += r * sym_mix(x) - br * x;
+                prev = x;
+                pp = p;
+            };
+            if (kv == kTileE) {
+#pragma unroll
+                for (int k = 0; k < kTileE; ++k)
+                    entry(k);
+            } else {
+#pragma unroll
+                for (int k = 0; k < kTileE; ++k)
+                    if (k < kv)
+                        entry(k);
             }
         }
-        /* the warp's events, spread over its lanes: event i of the warp is
-         * the (i - before)-th set bit of the lane that holds it */
+        /* the chunk's events, spread over the lanes: event i is the
+         * (i - before)-th set bit of the lane that holds it */
         const uint32_t cnt = __popc(evmask);
         uint32_t ci = cnt;
 #pragma unroll
@@ -669,13 +668,13 @@ __global__ void __launch_bounds__(kB) k_row_scan(const uint64_t *__restrict__ ro
             for (uint32_t d = i - ob; d > 0; --d)
                 mm &= mm - 1u;
             const int k = __ffs(mm) - 1;
-            const uint32_t o = (uint32_t)(warp * 32 + ow) * kTileE + k;
+            const uint32_t o = (uint32_t)ow * kTileE + k;
             const uint64_t j = j0 + o;
             /* the row of j: the last start at or before it */
             const uint32_t below = osb & ((2u << k) - 1u) & 0xFFFFu;
             const int ls = below ? (int)(o - k + 31 - __clz(below)) : oex;
-            const uint32_t r = ls >= 0 ? s_rowat[ls] : r_lo;
-            const uint64_t rbase = ls >= 0 ? j0 + ls : s_lo_base;
+            const uint32_t r = ls >= 0 ? rowat[ls] : r_lo;
+            const uint64_t rbase = ls >= 0 ? j0 + ls : __ldg(row_ptr + r_lo);
             const int pr = part(r);
             const bool st = (osb >> k) & 1u, en = (osb >> (k + 1)) & 1u;
             const int pj = part(__ldg(col + j));
@@ -707,7 +706,7 @@ __global__ void __launch_bounds__(kB) k_row_scan(const uint64_t *__restrict__ ro
                     local += j + 1;
             }
         }
-        __syncthreads(); /* s_bits, s_rowat are rewritten by the next tile */
+        __syncwarp(); /* bits, rowat are rewritten by the next chunk */
     }
     for (int o = 16; o > 0; o >>= 1) {
         local += __shfl_xor_sync(0xffffffffu, local, o);
@@ -1114,85 +1113,123 @@ __global__ void __launch_bounds__(kB) k_ng_mark(EmitParams E, const uint64_t *wo
 /* The mask keys in sorted order: key (p, u, giant rep of p) for every bit
  * p of pmask[u], partition-major and ascending in u - already the sort
  * order, so they skip the radix sort and are merged with the sorted plain
- * keys.  Pass 1 counts the bits of each partition per block of kMaskBlock
- * vertices (counts stored partition-major); after a scan, pass 2 writes
- * each block's keys at its offsets in vertex order. */
-constexpr int kMaskBlock = kB * 8;
+ * keys.  A block step covers kMaskBlock vertices, kMaskV consecutive ones
+ * per thread (two 16-byte loads).  Pass 1 counts the bits of each
+ * partition per block step (counts stored partition-major); after a scan,
+ * pass 2 places each thread's keys of partition p after those of the lower
+ * threads (one block scan for all partitions) and writes them in vertex
+ * order. */
+constexpr int kMaskV = 8;
+constexpr int kMaskBlock = kB * kMaskV;
 
+/* pmask of the thread's kMaskV vertices starting at u0 (0 past n). */
+__device__ __forceinline__ void mask_load(const EmitParams &E, uint64_t u0, uint32_t (&bits)[kMaskV])
+{
+    if (u0 + kMaskV <= E.n) {
+        const uint4 *p4 = reinterpret_cast<const uint4 *>(E.pmask + u0);
+        const uint4 x = __ldg(p4), y = __ldg(p4 + 1);
+        bits[0] = x.x; bits[1] = x.y; bits[2] = x.z; bits[3] = x.w;
+        bits[4] = y.x; bits[5] = y.y; bits[6] = y.z; bits[7] = y.w;
+    } else {
+#pragma unroll
+        for (int k = 0; k < kMaskV; ++k)
+            bits[k] = u0 + k < E.n ? __ldg(E.pmask + u0 + k) : 0u;
+    }
+}
+
+template <int PMAX>
 __global__ void __launch_bounds__(kB) k_mask_count(EmitParams E, uint32_t nblk, uint32_t *cnt)
 {
-    __shared__ uint32_t s_c[32];
+    __shared__ uint32_t s_c[kW][PMAX];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (uint32_t blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
-        if (threadIdx.x < 32)
-            s_c[threadIdx.x] = 0;
-        __syncthreads();
-        const uint64_t v0 = (uint64_t)blk * kMaskBlock;
-        uint32_t mine[32];
+        uint32_t bits[kMaskV];
+        mask_load(E, (uint64_t)blk * kMaskBlock + (uint64_t)threadIdx.x * kMaskV, bits);
 #pragma unroll
-        for (int p = 0; p < 32; ++p)
-            mine[p] = 0;
-        for (int k = 0; k < 8; ++k) {
-            const uint64_t u = v0 + (uint64_t)k * kB + threadIdx.x;
-            const uint32_t bits = u < E.n ? E.pmask[u] : 0u;
+        for (int p = 0; p < PMAX; ++p) {
+            if (p < E.parts) {
+                uint32_t c = 0;
 #pragma unroll
-            for (int p = 0; p < 32; ++p)
-                mine[p] += (bits >> p) & 1u;
-        }
-        for (int p = 0; p < E.parts; ++p) {
-            const uint32_t c = __reduce_add_sync(0xffffffffu, mine[p]);
-            if ((threadIdx.x & 31) == 0 && c)
-                atomicAdd(&s_c[p], c);
+                for (int k = 0; k < kMaskV; ++k)
+                    c += (bits[k] >> p) & 1u;
+                c = __reduce_add_sync(0xffffffffu, c);
+                if (lane == 0)
+                    s_c[warp][p] = c;
+            }
         }
         __syncthreads();
-        if (threadIdx.x < (unsigned)E.parts)
-            cnt[(uint64_t)threadIdx.x * nblk + blk] = s_c[threadIdx.x];
+        if (threadIdx.x < (unsigned)E.parts) {
+            uint32_t t = 0;
+#pragma unroll
+            for (int w = 0; w < kW; ++w)
+                t += s_c[w][threadIdx.x];
+            cnt[(uint64_t)threadIdx.x * nblk + blk] = t;
+        }
         __syncthreads();
     }
 }
 
+template <int PMAX>
 __global__ void __launch_bounds__(kB) k_mask_write(EmitParams E, uint32_t nblk,
                                                    const uint64_t *off, uint64_t *out)
 {
     __shared__ uint32_t s_b[CCGPU_MAX_PARTS + 1];
     __shared__ uint32_t s_gl[CCGPU_MAX_PARTS];
-    __shared__ uint32_t s_w[kW];
+    __shared__ uint32_t s_w[kW][PMAX];
     for (int i = threadIdx.x; i <= E.parts; i += kB)
         s_b[i] = E.bounds[i];
     load_giant_labels(E, s_gl);
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (uint32_t blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
-        const uint64_t v0 = (uint64_t)blk * kMaskBlock;
-        for (int p = 0; p < E.parts; ++p) {
-            uint64_t at = off[(uint64_t)p * nblk + blk];
-            const uint64_t rep = s_gl[p] - s_b[p];
-            for (int k = 0; k < 8; ++k) {
-                const uint64_t u = v0 + (uint64_t)k * kB + threadIdx.x;
-                const bool has = u < E.n && ((E.pmask[u] >> p) & 1u);
-                const unsigned bal = __ballot_sync(0xffffffffu, has);
-                if (lane == 0)
-                    s_w[warp] = __popc(bal);
-                __syncthreads();
-                uint32_t pre = 0, tot = 0;
+        const uint64_t u0 = (uint64_t)blk * kMaskBlock + (uint64_t)threadIdx.x * kMaskV;
+        uint32_t bits[kMaskV];
+        mask_load(E, u0, bits);
+        uint32_t excl[PMAX];
 #pragma unroll
-                for (int w = 0; w < kW; ++w) {
-                    pre += w < warp ? s_w[w] : 0u;
-                    tot += s_w[w];
+        for (int p = 0; p < PMAX; ++p) {
+            excl[p] = 0;
+            if (p < E.parts) {
+                uint32_t c = 0;
+#pragma unroll
+                for (int k = 0; k < kMaskV; ++k)
+                    c += (bits[k] >> p) & 1u;
+                uint32_t incl = c;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o)
+                        incl += y;
                 }
-                if (has)
-                    out[at + pre + __popc(bal & ((1u << lane) - 1u))] =
-                        make_key(E, p, (uint32_t)u, (uint32_t)rep);
-                at += tot;
-                __syncthreads();
+                if (lane == 31)
+                    s_w[warp][p] = incl;
+                excl[p] = incl - c;
             }
         }
+        __syncthreads();
+#pragma unroll
+        for (int p = 0; p < PMAX; ++p) {
+            if (p < E.parts) {
+                uint64_t at = off[(uint64_t)p * nblk + blk] + excl[p];
+#pragma unroll
+                for (int w = 0; w < kW; ++w)
+                    at += w < warp ? s_w[w][p] : 0u;
+                const uint32_t rep = s_gl[p] - s_b[p];
+#pragma unroll
+                for (int k = 0; k < kMaskV; ++k)
+                    if ((bits[k] >> p) & 1u)
+                        out[at++] = make_key(E, p, (uint32_t)(u0 + k), rep);
+            }
+        }
+        __syncthreads(); /* s_w is rewritten by the next step */
     }
 }
 
-/* Stable merge of two ascending key arrays (ties take a first): each block
- * finds where its kMergeTile outputs start on the merge path by binary
- * search, stages those inputs in shared memory, and each thread merges
- * kMergeItems outputs from its own split point. */
+/* Stable merge of two ascending key arrays (ties take a first): where each
+ * tile of kMergeTile outputs starts on the merge path is found first, all
+ * tiles' binary searches at once (k_merge_splits); each block then stages
+ * its tile's inputs in shared memory, and each thread merges kMergeItems
+ * outputs from its own split point. */
 constexpr int kMergeItems = 8;
 constexpr int kMergeTile = kB * kMergeItems;
 
@@ -1210,21 +1247,32 @@ __device__ __forceinline__ uint64_t merge_split(const uint64_t *a, uint64_t na, 
     return lo;
 }
 
+/* split[t] = merge_split(min(t * kMergeTile, na + nb)), t = 0..tiles. */
+__global__ void __launch_bounds__(kB) k_merge_splits(const uint64_t *__restrict__ a, uint64_t na,
+                                                     const uint64_t *__restrict__ b, uint64_t nb,
+                                                     uint64_t tiles, uint64_t *split)
+{
+    const uint64_t total = na + nb;
+    const uint64_t stride = (uint64_t)gridDim.x * kB;
+    for (uint64_t t = (uint64_t)blockIdx.x * kB + threadIdx.x; t <= tiles; t += stride) {
+        const uint64_t d = t * kMergeTile < total ? t * kMergeTile : total;
+        split[t] = merge_split(a, na, b, nb, d);
+    }
+}
+
 __global__ void __launch_bounds__(kB) k_merge(const uint64_t *__restrict__ a, uint64_t na,
                                               const uint64_t *__restrict__ b, uint64_t nb,
+                                              const uint64_t *__restrict__ split,
                                               uint64_t *__restrict__ out)
 {
     __shared__ uint64_t s_k[kMergeTile];
     __shared__ uint64_t s_o[kMergeTile];
-    __shared__ uint64_t s_ia[2];
     const uint64_t total = na + nb;
     for (uint64_t d0 = (uint64_t)blockIdx.x * kMergeTile; d0 < total;
          d0 += (uint64_t)gridDim.x * kMergeTile) {
         const uint64_t d1 = d0 + kMergeTile < total ? d0 + kMergeTile : total;
-        if (threadIdx.x < 2)
-            s_ia[threadIdx.x] = merge_split(a, na, b, nb, threadIdx.x ? d1 : d0);
-        __syncthreads();
-        const uint64_t ia0 = s_ia[0], ia1 = s_ia[1];
+        const uint64_t t = d0 / kMergeTile;
+        const uint64_t ia0 = __ldg(split + t), ia1 = __ldg(split + t + 1);
         const uint64_t ib0 = d0 - ia0, ib1 = d1 - ia1;
         const uint32_t la = (uint32_t)(ia1 - ia0), lb = (uint32_t)(ib1 - ib0);
         for (uint32_t i = threadIdx.x; i < la + lb; i += kB)
@@ -1901,40 +1949,57 @@ __global__ void __launch_bounds__(kB) k_upd(MergeParams M)
  * label fell below what was last sent (prev_sent, ~0 before the first
  * exchange) the label goes straight into ghost_labels[g], and g is appended
  * to the exchange's delta list - the in-HBM compaction of the changed
- * boundary labels - with one slot reservation per block.  The delta list
+ * boundary labels - with one slot reservation per block step of
+ * kExchRounds * kB ghosts (a counter taken once per 256 ghosts was the
+ * kernel's bottleneck).  The delta list
  * drives the hook update (k_delta_push) and its length is the reference's
  * count of sent pairs. */
+constexpr int kExchRounds = 8; /* ghosts per thread per block step */
+
 __global__ void __launch_bounds__(kB) k_exchange(MergeParams M)
 {
     __shared__ uint32_t s_wcnt[kB / 32];
     __shared__ uint32_t s_base;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint64_t stride = (uint64_t)gridDim.x * kB;
-    for (uint64_t base = (uint64_t)blockIdx.x * kB; base < M.ghosts; base += stride) {
-        const uint64_t g = base + threadIdx.x;
-        bool send = false;
-        if (g < M.ghosts) {
-            uint32_t rep;
-            bool look = true;
-            if (M.ghost_rep_ready) {
-                rep = __ldg(M.ghost_rep + g);
-                /* a rep whose label did not fall since the last exchange
-                 * still has the label last sent: nothing to send */
-                look = M.dirty[rep] != 0;
-            } else {
-                rep = __ldg(M.label + __ldg(M.ghost_v + g)); /* fixed by the local solve */
-                M.ghost_rep[g] = rep;
-            }
-            const uint32_t lbl = look ? M.cur[rep] : 0xffffffffu;
-            if (look && lbl < M.prev_sent[g]) {
-                M.prev_sent[g] = lbl;
-                M.ghost_labels[g] = lbl;
-                send = true;
+    const uint64_t span = (uint64_t)kB * kExchRounds;
+    for (uint64_t base = (uint64_t)blockIdx.x * span; base < M.ghosts;
+         base += (uint64_t)gridDim.x * span) {
+        uint32_t sendmask = 0;
+#pragma unroll
+        for (int i = 0; i < kExchRounds; ++i) {
+            const uint64_t g = base + (uint64_t)i * kB + threadIdx.x;
+            if (g < M.ghosts) {
+                uint32_t rep;
+                bool look = true;
+                if (M.ghost_rep_ready) {
+                    rep = __ldg(M.ghost_rep + g);
+                    /* a rep whose label did not fall since the last
+                     * exchange still has the label last sent: nothing to
+                     * send */
+                    look = M.dirty[rep] != 0;
+                } else {
+                    rep = __ldg(M.label + __ldg(M.ghost_v + g)); /* fixed by the local solve */
+                    M.ghost_rep[g] = rep;
+                }
+                const uint32_t lbl = look ? M.cur[rep] : 0xffffffffu;
+                if (look && lbl < M.prev_sent[g]) {
+                    M.prev_sent[g] = lbl;
+                    M.ghost_labels[g] = lbl;
+                    sendmask |= 1u << i;
+                }
             }
         }
-        const unsigned bal = __ballot_sync(0xffffffffu, send);
-        if (lane == 0)
-            s_wcnt[warp] = __popc(bal);
+        /* one slot reservation for the block's step */
+        const uint32_t cnt = __popc(sendmask);
+        uint32_t incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o)
+                incl += y;
+        }
+        if (lane == 31)
+            s_wcnt[warp] = incl;
         __syncthreads();
         if (threadIdx.x == 0) {
             uint32_t acc = 0;
@@ -1944,13 +2009,15 @@ __global__ void __launch_bounds__(kB) k_exchange(MergeParams M)
                 acc += c;
             }
             s_base = acc ? atomicAdd(M.delta_count, acc) : 0u;
-            if (acc)
-                atomicAdd(M.sent, (unsigned long long)acc);
         }
         __syncthreads();
-        if (send)
-            M.delta[s_base + s_wcnt[warp] + __popc(bal & ((1u << lane) - 1u))] = (uint32_t)g;
-        __syncthreads(); /* s_wcnt / s_base are rewritten by the next tile */
+        uint32_t pos = s_base + s_wcnt[warp] + incl - cnt;
+        while (sendmask) {
+            const int i = __ffs(sendmask) - 1;
+            sendmask &= sendmask - 1u;
+            M.delta[pos++] = (uint32_t)(base + (uint64_t)i * kB + threadIdx.x);
+        }
+        __syncthreads(); /* s_wcnt / s_base are rewritten by the next step */
     }
 }
 
@@ -1966,6 +2033,8 @@ __global__ void __launch_bounds__(kB) k_exchange(MergeParams M)
 __global__ void __launch_bounds__(kB) k_delta_push(MergeParams M)
 {
     const uint32_t total = *M.delta_count;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && total)
+        atomicAdd(M.sent, (unsigned long long)total); /* the exchange's sent pairs */
     if (pull_hooks(M, total))
         return;
     const int lane = threadIdx.x & 31;
@@ -2222,21 +2291,28 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
                 /* [0] local entries, [1] symmetry sum */
                 CC_TRY(cc_bufs_get(&B, (void **)&local_total, 2 * sizeof(unsigned long long)));
                 CC_CUDA(cudaMemsetAsync(local_total, 0, 2 * sizeof(unsigned long long), st));
-                /* tile starts (the same array tiles_of() builds) and the
+                /* the row holding each warp chunk's first entry and the
                  * empty rows' offsets */
-                CC_TRY(cc_bufs_get(&B, (void **)&tile_first, (Lp.tiles + 1) * sizeof(uint32_t)));
-                col_tiles = Lp.tiles;
+                const uint64_t chunks = (m + kChunk - 1) / kChunk;
+                uint32_t *chunk_first = nullptr;
+                CC_TRY(cc_bufs_get(&B, (void **)&chunk_first, (chunks + 1) * sizeof(uint32_t)));
                 CC_KLAUNCH(ctx, CCK_DIST_TILES, k_scan_prep, vb, kB, 0, st, d_row_ptr, n, m,
-                           Lp.tiles, tile_first, P, roff, rlb, rle);
-                const unsigned scan_b = cc_blocks(Lp.tiles, 1, (unsigned)ctx->sm_count * 8);
-                if (P <= 4)
-                    CC_KLAUNCH(ctx, CCK_DIST_LOCAL_COUNT, k_row_scan<4>, scan_b, kB, 0, st,
-                               d_row_ptr, d_col, n, m, bounds, P, Lp.vec, tile_first, roff, rlb, rle, rflags,
-                               local_total, local_total + 1);
-                else
-                    CC_KLAUNCH(ctx, CCK_DIST_LOCAL_COUNT, k_row_scan<8>, scan_b, kB, 0, st,
-                               d_row_ptr, d_col, n, m, bounds, P, Lp.vec, tile_first, roff, rlb, rle, rflags,
-                               local_total, local_total + 1);
+                           chunks, chunk_first, P, roff, rlb, rle);
+                const unsigned scan_b = cc_blocks(chunks, kW, (unsigned)ctx->sm_count * 16);
+#define CC_ROW_SCAN(PP)                                                                    \
+    CC_KLAUNCH(ctx, CCK_DIST_LOCAL_COUNT, k_row_scan<PP>, scan_b, kB, 0, st, d_row_ptr, d_col, n, \
+               m, bounds, Lp.vec, chunk_first, roff, rlb, rle, rflags, local_total,           \
+               local_total + 1)
+                switch (P) {
+                case 2: CC_ROW_SCAN(2); break;
+                case 3: CC_ROW_SCAN(3); break;
+                case 4: CC_ROW_SCAN(4); break;
+                case 5: CC_ROW_SCAN(5); break;
+                case 6: CC_ROW_SCAN(6); break;
+                case 7: CC_ROW_SCAN(7); break;
+                default: CC_ROW_SCAN(8); break;
+                }
+#undef CC_ROW_SCAN
             }
             l_rp = rlb;
             l_end = rle;
@@ -2461,7 +2537,13 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
         CC_TRY(cc_bufs_get(&B, (void **)&mcnt, (size_t)P * nblk * sizeof(uint32_t)));
         CC_TRY(cc_bufs_get(&B, (void **)&moff, ((size_t)P * nblk + 1) * sizeof(uint64_t)));
         const unsigned mb = cc_blocks(nblk, 1, (unsigned)ctx->sm_count * 8);
-        CC_KLAUNCH(ctx, CCK_DIST_PAIRS_BITMAP, k_mask_count, mb, kB, 0, st, E, nblk, mcnt);
+        if (P <= 4)
+            CC_KLAUNCH(ctx, CCK_DIST_PAIRS_BITMAP, k_mask_count<4>, mb, kB, 0, st, E, nblk, mcnt);
+        else if (P <= 8)
+            CC_KLAUNCH(ctx, CCK_DIST_PAIRS_BITMAP, k_mask_count<8>, mb, kB, 0, st, E, nblk, mcnt);
+        else
+            CC_KLAUNCH(ctx, CCK_DIST_PAIRS_BITMAP, k_mask_count<32>, mb, kB, 0, st, E, nblk,
+                       mcnt);
         CC_TRY(cc_scan_u32(ctx, mcnt, moff, (uint64_t)P * nblk, &B, st));
         uint64_t M_keys = 0;
         CC_CUDA(cudaMemcpyAsync(&M_keys, moff + (uint64_t)P * nblk, sizeof(uint64_t),
@@ -2469,14 +2551,26 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
         CC_CUDA(cudaStreamSynchronize(st));
         if (M_keys) {
             CC_TRY(cc_bufs_get(&B, (void **)&mkeys, (size_t)M_keys * sizeof(uint64_t)));
-            CC_KLAUNCH(ctx, CCK_DIST_PAIRS_BITMAP, k_mask_write, mb, kB, 0, st, E, nblk,
-                       (const uint64_t *)moff, mkeys);
+            if (P <= 4)
+                CC_KLAUNCH(ctx, CCK_DIST_PAIRS_BITMAP, k_mask_write<4>, mb, kB, 0, st, E, nblk,
+                           (const uint64_t *)moff, mkeys);
+            else if (P <= 8)
+                CC_KLAUNCH(ctx, CCK_DIST_PAIRS_BITMAP, k_mask_write<8>, mb, kB, 0, st, E, nblk,
+                           (const uint64_t *)moff, mkeys);
+            else
+                CC_KLAUNCH(ctx, CCK_DIST_PAIRS_BITMAP, k_mask_write<32>, mb, kB, 0, st, E, nblk,
+                           (const uint64_t *)moff, mkeys);
             if (R > 0) {
                 CC_TRY(cc_bufs_get(&B, (void **)&merged, (size_t)(R + M_keys) * sizeof(uint64_t)));
                 const uint64_t tiles = (R + M_keys + kMergeTile - 1) / kMergeTile;
+                uint64_t *split = nullptr;
+                CC_TRY(cc_bufs_get(&B, (void **)&split, (tiles + 1) * sizeof(uint64_t)));
+                CC_KLAUNCH(ctx, CCK_DIST_MERGE_KEYS, k_merge_splits,
+                           cc_blocks(tiles + 1, kB, (unsigned)ctx->sm_count * 8), kB, 0, st, sorted,
+                           R, mkeys, M_keys, tiles, split);
                 CC_KLAUNCH(ctx, CCK_DIST_MERGE_KEYS, k_merge,
                            cc_blocks(tiles, 1, (unsigned)ctx->sm_count * 8), kB, 0, st, sorted, R,
-                           mkeys, M_keys, merged);
+                           mkeys, M_keys, (const uint64_t *)split, merged);
                 sorted = merged;
             } else {
                 sorted = mkeys;
@@ -2658,7 +2752,8 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
         if (steps >= interval || !any_changed) {
             M.cur = pc;
             CC_CUDA(cudaMemsetAsync(M.delta_count, 0, sizeof(uint32_t), st));
-            CC_KLAUNCH(ctx, CCK_MERGE_EXCH_PACK, k_exchange, cc_blocks(G, kB, gbk), kB, 0, st, M);
+            CC_KLAUNCH(ctx, CCK_MERGE_EXCH_PACK, k_exchange,
+                       cc_blocks(G, (unsigned)(kB * kExchRounds), gbk), kB, 0, st, M);
             M.ghost_rep_ready = 1;
             CC_KLAUNCH(ctx, CCK_MERGE_EXCH_SCATTER, k_delta_push, cc_blocks(G, kB, gbk), kB, 0,
                        st, M);
