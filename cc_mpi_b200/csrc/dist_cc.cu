@@ -1832,6 +1832,15 @@ __global__ void __launch_bounds__(kB) k_ghost_buckets(const uint32_t *__restrict
 
 /* ------------------------------------------------------------- merge */
 
+/* Round state of a merge driven on the device (k_merge_ctl, one graph
+ * launch for all rounds); NULL in MergeParams when the host drives it. */
+struct MergeCtl {
+    uint32_t *cur, *next;         /* labels before / after the round     */
+    int pending[CCGPU_MAX_PARTS];
+    int steps, done, do_exch, rep_ready;
+    int rounds, exchanges, launch_rounds;
+};
+
 struct MergeParams {
     const uint32_t *label;        /* comp_of as global rep ids          */
     const uint32_t *bounds;
@@ -1862,7 +1871,28 @@ struct MergeParams {
     uint8_t *dirty;               /* [n] 1: the rep's label fell since the last
                                    * exchange (set by k_upd, cleared after an
                                    * exchange); read from the second exchange on */
+    uint64_t n;                   /* vertices (the dirty bytes)                    */
+    MergeCtl *ctl;                /* device-driven rounds, or NULL                 */
 };
+
+/* Labels before the round (cur) and after it (next): the host's pointers,
+ * or the device-driven merge's current pair. */
+__device__ __forceinline__ const uint32_t *merge_cur(const MergeParams &M)
+{
+    return M.ctl ? M.ctl->cur : M.cur;
+}
+
+__device__ __forceinline__ uint32_t *merge_next(const MergeParams &M)
+{
+    return M.ctl ? M.ctl->next : M.next;
+}
+
+/* Whether this round's exchange runs (always when the host drives the
+ * rounds: it launches the exchange only when one is due). */
+__device__ __forceinline__ bool merge_exchanges(const MergeParams &M)
+{
+    return !M.ctl || M.ctl->do_exch;
+}
 
 /* An exchange lowers the hook minima by one pass over every pair (pull)
  * when it changes more than one ghost label per 8 pairs; below that, the
@@ -1872,28 +1902,55 @@ __device__ __forceinline__ bool pull_hooks(const MergeParams &M, uint64_t messag
     return messages * 8 > M.pairs;
 }
 
-/* hook[rep] = min over the rep's cut pairs of the ghost labels. */
-__global__ void __launch_bounds__(kB) k_hook_init(MergeParams M)
+/* hook[r] lowered to the minimum ghost label over r's pairs, every pair:
+ * kHookRounds pairs per thread per step, loaded in phases (reps and ghost
+ * ids, then labels, then the hook values) so the loads of a step overlap.
+ * Lanes whose pairs share a rep (consecutive pairs of a rep are
+ * contiguous) combine first and one of them issues the atomicMin; a hook
+ * already <= the minimum needs no atomic. */
+constexpr int kHookRounds = 4;
+
+__device__ __forceinline__ void hook_all_pairs(const MergeParams &M)
 {
     const int lane = threadIdx.x & 31;
-    const uint64_t stride = (uint64_t)gridDim.x * kB;
-    for (uint64_t base = (uint64_t)blockIdx.x * kB; base < M.pairs; base += stride) {
-        uint64_t k = base + threadIdx.x;
-        bool ok = k < M.pairs;
-        uint32_t r = ok ? M.pair_rep[k] : 0xffffffffu;
-        uint32_t l = ok ? M.ghost_labels[M.pair_g[k]] : 0xffffffffu;
-        unsigned peers = __match_any_sync(0xffffffffu, r);
-        uint32_t mn = __reduce_min_sync(peers, l);
-        if (ok && (__ffs(peers) - 1) == lane && mn < M.hook[r])
-            atomicMin(M.hook + r, mn);
+    const uint64_t span = (uint64_t)kB * kHookRounds;
+    for (uint64_t base = (uint64_t)blockIdx.x * span; base < M.pairs;
+         base += (uint64_t)gridDim.x * span) {
+        uint32_t r[kHookRounds], g[kHookRounds], l[kHookRounds], h[kHookRounds];
+#pragma unroll
+        for (int i = 0; i < kHookRounds; ++i) {
+            const uint64_t k = base + (uint64_t)i * kB + threadIdx.x;
+            const bool ok = k < M.pairs;
+            r[i] = ok ? __ldg(M.pair_rep + k) : 0xffffffffu;
+            g[i] = ok ? __ldg(M.pair_g + k) : 0xffffffffu;
+        }
+#pragma unroll
+        for (int i = 0; i < kHookRounds; ++i)
+            l[i] = g[i] != 0xffffffffu ? M.ghost_labels[g[i]] : 0xffffffffu;
+#pragma unroll
+        for (int i = 0; i < kHookRounds; ++i)
+            h[i] = r[i] != 0xffffffffu ? M.hook[r[i]] : 0u;
+#pragma unroll
+        for (int i = 0; i < kHookRounds; ++i) {
+            const unsigned peers = __match_any_sync(0xffffffffu, r[i]);
+            const uint32_t mn = __reduce_min_sync(peers, l[i]);
+            if (r[i] != 0xffffffffu && (__ffs(peers) - 1) == lane && mn < h[i])
+                atomicMin(M.hook + r[i], mn);
+        }
     }
 }
 
-__device__ __forceinline__ bool label_of(const MergeParams &M, const uint32_t *s_b, int p,
-                                         uint32_t x, uint32_t &y)
+/* hook[rep] = min over the rep's cut pairs of the ghost labels. */
+__global__ void __launch_bounds__(kB) k_hook_init(MergeParams M)
+{
+    hook_all_pairs(M);
+}
+
+__device__ __forceinline__ bool label_of(const MergeParams &M, const uint32_t *cur,
+                                         const uint32_t *s_b, int p, uint32_t x, uint32_t &y)
 {
     if (x >= s_b[p] && x < s_b[p + 1]) {
-        y = M.cur[__ldg(M.label + x)];
+        y = cur[__ldg(M.label + x)];
         return true;
     }
     /* p's ghosts are ascending; the bucket of x narrows the search */
@@ -1921,19 +1978,21 @@ __global__ void __launch_bounds__(kB) k_upd(MergeParams M)
     for (int i = threadIdx.x; i <= M.parts; i += kB)
         s_b[i] = M.bounds[i];
     __syncthreads();
+    const uint32_t *cur = merge_cur(M);
+    uint32_t *next = merge_next(M);
     const uint64_t stride = (uint64_t)gridDim.x * kB;
     for (uint64_t i = (uint64_t)blockIdx.x * kB + threadIdx.x; i < M.rep_count; i += stride) {
         uint32_t r = M.rep_list[i];
         int p = part_of(s_b, M.parts, r);
-        uint32_t c = M.cur[r], h = M.hook[r];
+        uint32_t c = cur[r], h = M.hook[r];
         uint32_t x = h < c ? h : c;
         for (int t = 0; t < 4; ++t) {
             uint32_t y;
-            if (!label_of(M, s_b, p, x, y) || y >= x)
+            if (!label_of(M, cur, s_b, p, x, y) || y >= x)
                 break;
             x = y;
         }
-        M.next[r] = x;
+        next[r] = x;
         if (x < c) {
             M.changed[p] = 1;
             M.dirty[r] = 1;
@@ -1960,33 +2019,54 @@ __global__ void __launch_bounds__(kB) k_exchange(MergeParams M)
 {
     __shared__ uint32_t s_wcnt[kB / 32];
     __shared__ uint32_t s_base;
+    if (!merge_exchanges(M))
+        return;
+    const int ready = M.ctl ? M.ctl->rep_ready : M.ghost_rep_ready;
+    const uint32_t *cur = merge_cur(M);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint64_t span = (uint64_t)kB * kExchRounds;
     for (uint64_t base = (uint64_t)blockIdx.x * span; base < M.ghosts;
          base += (uint64_t)gridDim.x * span) {
-        uint32_t sendmask = 0;
+        /* the step's loads in phases (reps, then dirty bytes, then labels
+         * and last-sent values), so each thread keeps kExchRounds loads in
+         * flight instead of one dependent chain per ghost */
+        uint32_t rep[kExchRounds];
+        bool look[kExchRounds];
 #pragma unroll
         for (int i = 0; i < kExchRounds; ++i) {
             const uint64_t g = base + (uint64_t)i * kB + threadIdx.x;
-            if (g < M.ghosts) {
-                uint32_t rep;
-                bool look = true;
-                if (M.ghost_rep_ready) {
-                    rep = __ldg(M.ghost_rep + g);
-                    /* a rep whose label did not fall since the last
-                     * exchange still has the label last sent: nothing to
-                     * send */
-                    look = M.dirty[rep] != 0;
-                } else {
-                    rep = __ldg(M.label + __ldg(M.ghost_v + g)); /* fixed by the local solve */
-                    M.ghost_rep[g] = rep;
-                }
-                const uint32_t lbl = look ? M.cur[rep] : 0xffffffffu;
-                if (look && lbl < M.prev_sent[g]) {
-                    M.prev_sent[g] = lbl;
-                    M.ghost_labels[g] = lbl;
-                    sendmask |= 1u << i;
-                }
+            look[i] = g < M.ghosts;
+            rep[i] = 0;
+            if (look[i])
+                rep[i] = ready ? __ldg(M.ghost_rep + g) : __ldg(M.label + __ldg(M.ghost_v + g));
+        }
+        if (ready) {
+            /* a rep whose label did not fall since the last exchange still
+             * has the label last sent: nothing to send */
+#pragma unroll
+            for (int i = 0; i < kExchRounds; ++i)
+                look[i] = look[i] && M.dirty[rep[i]] != 0;
+        } else {
+#pragma unroll
+            for (int i = 0; i < kExchRounds; ++i)
+                if (look[i]) /* fixed by the local solve */
+                    M.ghost_rep[base + (uint64_t)i * kB + threadIdx.x] = rep[i];
+        }
+        uint32_t lbl[kExchRounds], ps[kExchRounds];
+#pragma unroll
+        for (int i = 0; i < kExchRounds; ++i) {
+            const uint64_t g = base + (uint64_t)i * kB + threadIdx.x;
+            lbl[i] = look[i] ? cur[rep[i]] : 0xffffffffu;
+            ps[i] = look[i] ? M.prev_sent[g] : 0u;
+        }
+        uint32_t sendmask = 0;
+#pragma unroll
+        for (int i = 0; i < kExchRounds; ++i) {
+            if (look[i] && lbl[i] < ps[i]) {
+                const uint64_t g = base + (uint64_t)i * kB + threadIdx.x;
+                M.prev_sent[g] = lbl[i];
+                M.ghost_labels[g] = lbl[i];
+                sendmask |= 1u << i;
             }
         }
         /* one slot reservation for the block's step */
@@ -2032,9 +2112,15 @@ __global__ void __launch_bounds__(kB) k_exchange(MergeParams M)
  * side. */
 __global__ void __launch_bounds__(kB) k_delta_push(MergeParams M)
 {
+    if (!merge_exchanges(M))
+        return;
     const uint32_t total = *M.delta_count;
-    if (blockIdx.x == 0 && threadIdx.x == 0 && total)
-        atomicAdd(M.sent, (unsigned long long)total); /* the exchange's sent pairs */
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (total)
+            atomicAdd(M.sent, (unsigned long long)total); /* the exchange's sent pairs */
+        if (M.ctl)
+            M.ctl->rep_ready = 1; /* k_exchange has filled ghost_rep */
+    }
     if (pull_hooks(M, total))
         return;
     const int lane = threadIdx.x & 31;
@@ -2073,20 +2159,65 @@ __global__ void __launch_bounds__(kB) k_delta_push(MergeParams M)
  * nothing when the exchange takes the push side. */
 __global__ void __launch_bounds__(kB) k_hook_pull(MergeParams M)
 {
-    if (!pull_hooks(M, *M.delta_count))
+    if (!merge_exchanges(M) || !pull_hooks(M, *M.delta_count))
         return;
-    const int lane = threadIdx.x & 31;
-    const uint64_t stride = (uint64_t)gridDim.x * kB;
-    for (uint64_t base = (uint64_t)blockIdx.x * kB; base < M.pairs; base += stride) {
-        const uint64_t k = base + threadIdx.x;
-        const bool ok = k < M.pairs;
-        const uint32_t r = ok ? M.pair_rep[k] : 0xffffffffu;
-        const uint32_t l = ok ? M.ghost_labels[M.pair_g[k]] : 0xffffffffu;
-        const unsigned peers = __match_any_sync(0xffffffffu, r);
-        const uint32_t mn = __reduce_min_sync(peers, l);
-        if (ok && (__ffs(peers) - 1) == lane && mn < M.hook[r])
-            atomicMin(M.hook + r, mn);
+    hook_all_pairs(M);
+}
+
+/* dirty[] cleared after an exchange. */
+__global__ void __launch_bounds__(kB) k_dirty_clear(MergeParams M)
+{
+    if (!merge_exchanges(M))
+        return;
+    const uint64_t words = M.n / 16, stride = (uint64_t)gridDim.x * kB;
+    uint4 *d4 = reinterpret_cast<uint4 *>(M.dirty);
+    for (uint64_t i = (uint64_t)blockIdx.x * kB + threadIdx.x; i < words; i += stride)
+        d4[i] = make_uint4(0u, 0u, 0u, 0u);
+    for (uint64_t i = words * 16 + (uint64_t)blockIdx.x * kB + threadIdx.x; i < M.n; i += stride)
+        M.dirty[i] = 0;
+}
+
+/* The round bookkeeping of the reference's merge loop (src/cc_mpi.c:
+ * 624-710) on the device, one thread, after each k_upd: partitions whose
+ * labels changed become pending, the labels swap, the loop ends when
+ * nothing is pending, and an exchange is due after `interval` rounds or a
+ * round that changed nothing.  The graph's while node repeats the round
+ * while this sets its condition: until the merge ends, or after
+ * kLaunchRounds rounds, when the host reads the state and launches again. */
+constexpr int kLaunchRounds = 4096;
+
+__global__ void k_merge_ctl(MergeCtl *ctl, int *changed, int parts, int interval,
+                            cudaGraphConditionalHandle loop)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0)
+        return;
+    int any = 0, pending = 0;
+    for (int p = 0; p < parts; ++p) {
+        const int c = changed[p];
+        if (c)
+            ctl->pending[p] = 1;
+        any |= c;
+        pending |= ctl->pending[p];
     }
+    ctl->rounds++;
+    ctl->launch_rounds++;
+    uint32_t *t = ctl->cur;
+    ctl->cur = ctl->next;
+    ctl->next = t;
+    ctl->do_exch = 0;
+    if (!pending) {
+        ctl->done = 1;
+        cudaGraphSetConditional(loop, 0u);
+        return;
+    }
+    if (++ctl->steps >= interval || !any) {
+        ctl->do_exch = 1;
+        ctl->exchanges++;
+        for (int p = 0; p < parts; ++p)
+            ctl->pending[p] = 0;
+        ctl->steps = 0;
+    }
+    cudaGraphSetConditional(loop, ctl->launch_rounds < kLaunchRounds ? 1u : 0u);
 }
 
 __global__ void __launch_bounds__(kB) k_final(const uint32_t *__restrict__ label,
@@ -2172,6 +2303,117 @@ extern "C" int ccgpu_partition_bounds(const uint64_t *d_row_ptr, uint32_t n, int
     }
     cc_bufs_release(&b);
     return rc;
+}
+
+/* The rest of a merge driven on the device (see k_merge_ctl), from the
+ * host loop's state: labels cur / nxt, pending flags, rounds since the last
+ * exchange, whether ghost_rep is filled.  Sets *used to false, with nothing
+ * launched, when conditional graph nodes are not available; the caller
+ * then goes on driving the rounds from the host. */
+static int merge_on_device(ccgpu_ctx *ctx, const MergeParams &M0, uint32_t *cur, uint32_t *nxt,
+                           const std::vector<int> &pending, int steps, int P, int interval,
+                           uint64_t act_count, uint64_t G, uint64_t U, uint32_t n, DevBufs *B,
+                           cudaStream_t st, uint32_t **final_labels, ccgpu_dist_stats *S,
+                           bool *used)
+{
+    *used = false;
+    MergeCtl h;
+    memset(&h, 0, sizeof(h));
+    h.cur = cur;
+    h.next = nxt;
+    for (int p = 0; p < P; ++p)
+        h.pending[p] = pending[p];
+    h.steps = steps;
+    h.rep_ready = M0.ghost_rep_ready;
+    MergeCtl *d_ctl = nullptr;
+    CC_TRY(cc_bufs_get(B, (void **)&d_ctl, sizeof(MergeCtl)));
+    CC_CUDA(cudaMemcpyAsync(d_ctl, &h, sizeof(h), cudaMemcpyHostToDevice, st));
+    MergeParams M = M0;
+    M.ctl = d_ctl;
+    M.cur = nullptr;
+    M.next = nullptr;
+    const unsigned gbk = (unsigned)ctx->sm_count * 8;
+
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    cudaStream_t cs = nullptr;
+    int rc = CCGPU_OK;
+    auto fail = [&](cudaError_t e, int line) {
+        if (rc == CCGPU_OK && e != cudaSuccess)
+            rc = ccgpu_cuda_fail(e, "merge rounds graph", __FILE__, line);
+    };
+    cudaGraphConditionalHandle loop = 0;
+    if (cudaGraphCreate(&g, 0) != cudaSuccess ||
+        cudaGraphConditionalHandleCreate(&loop, g, 1u, cudaGraphCondAssignDefault) !=
+            cudaSuccess) {
+        cudaGetLastError();
+        if (g)
+            cudaGraphDestroy(g);
+        return CCGPU_OK; /* not available: the host drives the rounds */
+    }
+    cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+    cp.conditional.handle = loop;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t wn = nullptr;
+    fail(cudaGraphAddNode(&wn, g, nullptr, 0, &cp), __LINE__);
+    if (rc == CCGPU_OK)
+        fail(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), __LINE__);
+    if (rc == CCGPU_OK) {
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        fail(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0,
+                                           cudaStreamCaptureModeThreadLocal),
+             __LINE__);
+        if (rc == CCGPU_OK) {
+            const cudaStream_t st = cs; /* CC_* macros launch on `st` */
+            int lrc = [&]() -> int {
+                CC_CUDA(cudaMemsetAsync(M.changed, 0, P * sizeof(int), st));
+                CC_KLAUNCH(ctx, CCK_MERGE_UPD, k_upd, cc_blocks(act_count, kB, gbk), kB, 0, st, M);
+                CC_KLAUNCH(ctx, CCK_MERGE_UPD, k_merge_ctl, 1, 32, 0, st, d_ctl, M.changed, P,
+                           interval, loop);
+                CC_CUDA(cudaMemsetAsync(M.delta_count, 0, sizeof(uint32_t), st));
+                CC_KLAUNCH(ctx, CCK_MERGE_EXCH_PACK, k_exchange,
+                           cc_blocks(G, (unsigned)(kB * kExchRounds), gbk), kB, 0, st, M);
+                CC_KLAUNCH(ctx, CCK_MERGE_EXCH_SCATTER, k_delta_push, cc_blocks(G, kB, gbk), kB,
+                           0, st, M);
+                CC_KLAUNCH(ctx, CCK_MERGE_EXCH_PULL, k_hook_pull,
+                           cc_blocks(U, (unsigned)(kB * kHookRounds), gbk), kB, 0, st, M);
+                CC_KLAUNCH(ctx, CCK_MERGE_EXCH_PULL, k_dirty_clear,
+                           cc_blocks((uint64_t)n / 16 + 1, kB, gbk), kB, 0, st, M);
+                return CCGPU_OK;
+            }();
+            cudaGraph_t out = nullptr;
+            fail(cudaStreamEndCapture(cs, &out), __LINE__);
+            if (rc == CCGPU_OK)
+                rc = lrc;
+        }
+    }
+    if (rc == CCGPU_OK)
+        fail(cudaGraphInstantiate(&ge, g, 0), __LINE__);
+    for (int launch = 0; rc == CCGPU_OK; ++launch) {
+        if (launch)
+            fail(cudaMemsetAsync(&d_ctl->launch_rounds, 0, sizeof(int), st), __LINE__);
+        fail(cudaGraphLaunch(ge, st), __LINE__);
+        fail(cudaMemcpyAsync(&h, d_ctl, sizeof(h), cudaMemcpyDeviceToHost, st), __LINE__);
+        fail(cudaStreamSynchronize(st), __LINE__);
+        if (h.done)
+            break;
+        if (rc == CCGPU_OK && h.rounds >= (1 << 22))
+            rc = ccgpu_set_error(CCGPU_ERR_LIMIT, "merge rounds: no end after %d rounds",
+                                 h.rounds);
+    }
+    if (ge)
+        cudaGraphExecDestroy(ge);
+    cudaGraphDestroy(g);
+    if (cs)
+        cudaStreamDestroy(cs);
+    if (rc != CCGPU_OK)
+        return rc;
+    S->rounds += h.rounds;
+    S->exchanges += h.exchanges;
+    *final_labels = h.cur;
+    *used = true;
+    return CCGPU_OK;
 }
 
 static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d_col, uint32_t n,
@@ -2691,6 +2933,8 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
     CC_TRY(cc_bufs_get(&B, (void **)&M.changed, P * sizeof(int)));
     CC_TRY(cc_bufs_get(&B, (void **)&M.ghost_rep, (size_t)(G ? G : 1) * sizeof(uint32_t)));
     M.ghost_rep_ready = 0;
+    M.n = n;
+    M.ctl = nullptr;
     CC_TRY(cc_bufs_get(&B, (void **)&M.dirty, (size_t)n));
     CC_CUDA(cudaMemsetAsync(M.dirty, 0, (size_t)n, st));
     const unsigned gbk = (unsigned)ctx->sm_count * 8;
@@ -2700,7 +2944,8 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
          * (ghost labels start as vertex ids) */
         M.cur = cur;
         M.next = nxt;
-        CC_KLAUNCH(ctx, CCK_MERGE_HOOK, k_hook_init, cc_blocks(U, kB, gbk), kB, 0, st, M);
+        CC_KLAUNCH(ctx, CCK_MERGE_HOOK, k_hook_init,
+                   cc_blocks(U, (unsigned)(kB * kHookRounds), gbk), kB, 0, st, M);
         uint32_t *act = nullptr;
         CC_TRY(cc_bufs_get(&B, (void **)&act, (size_t)S.rep_count * sizeof(uint32_t) + 4));
         CC_CUDA(cudaMemsetAsync(counters + 5, 0, sizeof(unsigned long long), st));
@@ -2723,7 +2968,23 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
         pending[p] = global_pending;
     int steps = 0;
     uint32_t *pc = cur, *pn = nxt;
+    /* The host drives the first kHostRounds rounds (most merges end within
+     * them, and a round costs the host one small read); a longer merge goes
+     * on as one CUDA graph: a while node repeats k_upd, k_merge_ctl and the
+     * exchange kernels (which return at once in a round without an
+     * exchange) until the merge ends, the host reading the round state once
+     * per launch of kLaunchRounds rounds at most. */
+    constexpr int kHostRounds = 8;
+    bool device_rounds = !ctx->prof && o.verbose < 2;
     while (global_pending) {
+        if (device_rounds && S.rounds >= kHostRounds) {
+            bool used = false;
+            CC_TRY(merge_on_device(ctx, M, pc, pn, pending, steps, P, interval, act_count, G, U,
+                                   n, &B, st, &pc, &S, &used));
+            if (used)
+                break;
+            device_rounds = false;
+        }
         M.cur = pc;
         M.next = pn;
         CC_CUDA(cudaMemsetAsync(M.changed, 0, P * sizeof(int), st));
@@ -2757,8 +3018,8 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
             M.ghost_rep_ready = 1;
             CC_KLAUNCH(ctx, CCK_MERGE_EXCH_SCATTER, k_delta_push, cc_blocks(G, kB, gbk), kB, 0,
                        st, M);
-            CC_KLAUNCH(ctx, CCK_MERGE_EXCH_PULL, k_hook_pull, cc_blocks(U, kB, gbk), kB, 0, st,
-                       M);
+            CC_KLAUNCH(ctx, CCK_MERGE_EXCH_PULL, k_hook_pull,
+                       cc_blocks(U, (unsigned)(kB * kHookRounds), gbk), kB, 0, st, M);
             CC_CUDA(cudaMemsetAsync(M.dirty, 0, (size_t)n, st));
             S.exchanges++;
             for (int p = 0; p < P; ++p)

@@ -4,6 +4,7 @@
  * device.
  */
 #include <cstdlib>
+#include <mutex>
 
 #include "ccgpu_internal.h"
 #include "primitives.h"
@@ -14,7 +15,74 @@ struct ccgpu_graph {
     uint32_t n;
     uint64_t m;
     int device;
+    size_t rp_cap, col_cap; /* bytes allocated for row_ptr / col */
 };
+
+namespace {
+
+/* The arrays of the last freed graph of each device, kept for the next
+ * upload: a caller that uploads, solves and frees a graph of the same size
+ * over and over (the reference's load / solve / free cycle) maps its
+ * gigabytes once instead of on every call. */
+constexpr int kGraphCacheDevices = 64;
+struct GraphCache {
+    uint64_t *row_ptr = nullptr;
+    uint32_t *col = nullptr;
+    size_t rp_cap = 0, col_cap = 0;
+};
+GraphCache g_gcache[kGraphCacheDevices];
+std::mutex g_gcache_mu;
+
+/* Arrays for a graph on the current device: the cached ones when they are
+ * large enough, else new ones (the cache is released first if cudaMalloc
+ * fails). */
+cudaError_t graph_arrays(ccgpu_graph *g, size_t rp_bytes, size_t col_bytes)
+{
+    {
+        std::lock_guard<std::mutex> lk(g_gcache_mu);
+        if (g->device >= 0 && g->device < kGraphCacheDevices) {
+            GraphCache &c = g_gcache[g->device];
+            if (c.row_ptr && c.rp_cap >= rp_bytes && c.col_cap >= col_bytes) {
+                g->row_ptr = c.row_ptr;
+                g->col = c.col;
+                g->rp_cap = c.rp_cap;
+                g->col_cap = c.col_cap;
+                c = GraphCache();
+                return cudaSuccess;
+            }
+        }
+    }
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        cudaError_t e = cudaMalloc((void **)&g->row_ptr, rp_bytes);
+        if (e == cudaSuccess) {
+            e = cudaMalloc((void **)&g->col, col_bytes);
+            if (e != cudaSuccess) {
+                cudaFree(g->row_ptr);
+                g->row_ptr = nullptr;
+            }
+        }
+        if (e == cudaSuccess) {
+            g->rp_cap = rp_bytes;
+            g->col_cap = col_bytes;
+            return cudaSuccess;
+        }
+        cudaGetLastError();
+        if (attempt == 0) { /* give the cached arrays back and try again */
+            std::lock_guard<std::mutex> lk(g_gcache_mu);
+            if (g->device >= 0 && g->device < kGraphCacheDevices) {
+                GraphCache &c = g_gcache[g->device];
+                cudaFree(c.row_ptr);
+                cudaFree(c.col);
+                c = GraphCache();
+            }
+        } else {
+            return e;
+        }
+    }
+    return cudaErrorMemoryAllocation;
+}
+
+} // namespace
 
 extern "C" int ccgpu_alloc(void **d_ptr, size_t bytes)
 {
@@ -61,12 +129,8 @@ extern "C" int ccgpu_graph_upload(const uint64_t *h_row_ptr, const uint32_t *h_c
     cudaGetDevice(&g->device);
     g->n = n;
     g->m = m;
-    /* stream-ordered pool memory: a graph uploaded again after one was
-     * freed reuses the pool's pages instead of mapping new ones */
-    CC_TRY(cc_pool_tune());
-    cudaError_t e = cudaMallocAsync((void **)&g->row_ptr, ((size_t)n + 1) * sizeof(uint64_t), 0);
-    if (e == cudaSuccess)
-        e = cudaMallocAsync((void **)&g->col, (size_t)(m ? m : 1) * sizeof(uint32_t), 0);
+    cudaError_t e = graph_arrays(g, ((size_t)n + 1) * sizeof(uint64_t),
+                                 (size_t)(m ? m : 1) * sizeof(uint32_t));
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(g->row_ptr, h_row_ptr, ((size_t)n + 1) * sizeof(uint64_t),
                             cudaMemcpyHostToDevice, 0);
@@ -88,18 +152,30 @@ extern "C" void ccgpu_graph_free(ccgpu_graph *g)
 {
     if (!g)
         return;
-    /* like cudaFree, wait for work that may still read the arrays; the
-     * pool memory goes back on the graph's own device */
+    /* like cudaFree, wait for work that may still read the arrays; then
+     * keep them for the next upload on this device, or free them when the
+     * cache already holds a graph's arrays */
     int cur = -1;
     cudaGetDevice(&cur);
     if (cur != g->device)
         cudaSetDevice(g->device);
     cudaDeviceSynchronize();
-    if (g->row_ptr)
-        cudaFreeAsync(g->row_ptr, 0);
-    if (g->col)
-        cudaFreeAsync(g->col, 0);
-    cudaStreamSynchronize(0);
+    bool kept = false;
+    if (g->row_ptr && g->col && g->device >= 0 && g->device < kGraphCacheDevices) {
+        std::lock_guard<std::mutex> lk(g_gcache_mu);
+        GraphCache &c = g_gcache[g->device];
+        if (!c.row_ptr) {
+            c.row_ptr = g->row_ptr;
+            c.col = g->col;
+            c.rp_cap = g->rp_cap;
+            c.col_cap = g->col_cap;
+            kept = true;
+        }
+    }
+    if (!kept) {
+        cudaFree(g->row_ptr);
+        cudaFree(g->col);
+    }
     if (cur >= 0 && cur != g->device)
         cudaSetDevice(cur);
     free(g);
@@ -206,11 +282,8 @@ extern "C" int ccgpu_graph_from_csc(const uint64_t *h_jc, const uint32_t *h_ir, 
     if (rc == CCGPU_OK) {
         cudaGetDevice(&g->device);
         g->n = nrows;
-        rc = cc_pool_tune();
-    }
-    if (rc == CCGPU_OK) {
-        cuda(cudaMallocAsync((void **)&g->row_ptr, ((size_t)nrows + 1) * sizeof(uint64_t), st),
-             __LINE__);
+        cuda(cudaMalloc((void **)&g->row_ptr, ((size_t)nrows + 1) * sizeof(uint64_t)), __LINE__);
+        g->rp_cap = ((size_t)nrows + 1) * sizeof(uint64_t);
     }
     if (rc == CCGPU_OK)
         rc = cc_bufs_get(&B, (void **)&d_jc, ((size_t)ncols + 1) * sizeof(uint64_t));
@@ -244,8 +317,8 @@ extern "C" int ccgpu_graph_from_csc(const uint64_t *h_jc, const uint32_t *h_ir, 
     }
     if (rc == CCGPU_OK) {
         g->m = m;
-        cuda(cudaMallocAsync((void **)&g->col, (size_t)(m ? m : 1) * sizeof(uint32_t), st),
-             __LINE__);
+        cuda(cudaMalloc((void **)&g->col, (size_t)(m ? m : 1) * sizeof(uint32_t)), __LINE__);
+        g->col_cap = (size_t)(m ? m : 1) * sizeof(uint32_t);
     }
     if (rc == CCGPU_OK && m) {
         CC_KLAUNCH(ctx, CCK_MISC, k_csc_cols, cc_blocks(m, kCsc, grid), kCsc, 0, st, sorted, m,

@@ -85,7 +85,10 @@ void ccgpu_free(void *d_ptr);
 int ccgpu_memcpy_h2d(void *d_dst, const void *h_src, size_t bytes);
 int ccgpu_memcpy_d2h(void *h_dst, const void *d_src, size_t bytes);
 
-/* A CSR copied to HBM once and reused by many solves. */
+/* A CSR copied to HBM once and reused by many solves.  ccgpu_graph_free
+ * waits for the device and keeps the arrays of one freed graph per device
+ * for the next upload or CSC transposition that fits in them (they are
+ * freed when a later graph needs more memory than is left). */
 typedef struct ccgpu_graph ccgpu_graph;
 int ccgpu_graph_upload(const uint64_t *h_row_ptr, const uint32_t *h_col_idx, uint32_t n,
                        uint64_t m, ccgpu_graph **out);

@@ -257,3 +257,26 @@ def test_boundary_sort_random_bits(torch):
         torch.cuda.synchronize()
         assert k == len(want)
         assert (t[:k].cpu().numpy().view(np.uint64) == want.view(np.uint64)).all()
+
+
+def test_host_and_device_driven_rounds_agree(torch):
+    """After its first rounds a merge goes on as one CUDA graph (a while node
+    over k_upd, the round bookkeeping and the exchange) unless the
+    per-kernel profiler is on, when the host drives every round: both give
+    the oracle's labels and the same round, exchange and sent-pair counts -
+    on a graph with over a thousand rounds (zigzag), one with a few dozen
+    (ER) and one with about ten (R-MAT)."""
+    from cc_mpi_b200 import _lib
+    L = _lib.lib()
+    sc = graphs.small_cases()
+    cases = {"zigzag": sc["zigzag"], "er": sc["er2k"], "rmat": graphs.rmat_csr(12, 8, seed=44)}
+    for name, (rp, col) in cases.items():
+        for parts, interval in ((7, 1), (4, 3)):
+            dev_st = check_against_oracle(torch, rp, col, parts, 1, interval)
+            _lib.check(L.ccgpu_prof_enable(None, 1))
+            try:
+                host_st = check_against_oracle(torch, rp, col, parts, 1, interval)
+            finally:
+                _lib.check(L.ccgpu_prof_enable(None, 0))
+            assert dev_st.rounds == host_st.rounds and dev_st.exchanges == host_st.exchanges, name
+            assert dev_st.sent_pairs == host_st.sent_pairs, name
