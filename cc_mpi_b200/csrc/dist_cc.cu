@@ -463,17 +463,16 @@ __global__ void __launch_bounds__(kB) k_emit_sorted(EmitParams E, const uint32_t
  * not contiguous); repeated entries are allowed.  local_total counts the
  * entries inside their row's own partition, from the events: each own-run
  * segment adds its end and subtracts its start.  symsum checks symmetry:
- * each entry (r, c) with c < n adds r*B(c) - B(r)*c (mod 2^32) for a
- * multiply-xorshift mix B, antisymmetric in (r, c), so a symmetric graph
- * sums to zero; an entry without its mirror leaves a term that cancels only
- * by chance (self loops add zero). */
+ * each entry (r, c) with c < n adds r*B(c) - B(r)*c (mod 2^32) for
+ * B(x) = x*x + K, i.e. (c - r)(r*c - K): antisymmetric in (r, c), so a
+ * symmetric graph sums to zero; an entry without its mirror leaves a term
+ * that cancels only by chance (self loops add zero). */
 constexpr int kChunk = 32 * kTileE;           /* entries per warp chunk          */
 constexpr int kChunkWords = kChunk / 32 + 2;  /* start bits 0..kChunk, one spare */
 
 __device__ __forceinline__ uint32_t sym_mix(uint32_t x)
 {
-    x = (x ^ 0x9E3779B9u) * 0x85EBCA6Bu;
-    return x ^ (x >> 16);
+    return x * x + 0x9E3779B9u;
 }
 
 /* Offsets and empty runs of every empty row, and the row holding each

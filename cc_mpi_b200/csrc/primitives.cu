@@ -177,9 +177,9 @@ namespace {
 
 constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
-constexpr int kKeysPerThread = 16;
-constexpr int kSortTile = kSortThreads * kKeysPerThread; /* 4096 */
-constexpr int kWarpKeys = kSortTile / kSortWarps;        /* 512  */
+constexpr int kKeysPerThread = 8;
+constexpr int kSortTile = kSortThreads * kKeysPerThread; /* 2048 */
+constexpr int kWarpKeys = kSortTile / kSortWarps;        /* 256  */
 constexpr uint32_t kInvalidDigit = 256;
 
 __global__ void __launch_bounds__(kSortThreads) k_sort_upsweep(const uint64_t *__restrict__ keys,
@@ -228,9 +228,13 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_downsweep(const uint64_t 
     uint64_t k[kKeysPerThread];
     uint32_t rank[kKeysPerThread];
 #pragma unroll
+    for (int j = 0; j < kKeysPerThread; ++j) { /* all loads first, then the ranks */
+        const uint64_t i = wbase + (uint64_t)j * 32 + lane;
+        k[j] = i < count ? keys[i] : 0;
+    }
+#pragma unroll
     for (int j = 0; j < kKeysPerThread; ++j) {
         uint64_t i = wbase + (uint64_t)j * 32 + lane;
-        k[j] = i < count ? keys[i] : 0;
         uint32_t d = i < count ? (uint32_t)((k[j] >> shift) & 0xff) : kInvalidDigit;
         unsigned peers = __match_any_sync(0xffffffffu, d);
         uint32_t before = 0;
