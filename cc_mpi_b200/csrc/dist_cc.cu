@@ -455,7 +455,7 @@ __global__ void __launch_bounds__(kB) k_emit_sorted(EmitParams E, const uint32_t
  * start at or before it - found from the bitmap and a warp max-scan of each
  * lane's last start - or, before the chunk's first start, the row holding
  * the chunk's first entry (chunk_first, k_scan_prep).  Empty rows hold no
- * entry; k_scan_prep writes their offsets.
+ * entry; the chunk where they start writes their offsets.
  *
  * roff[v*P + q-1] = entries of row v below bounds[q], q = 1..P (bounds[P] =
  * n, so the last is the count of valid ids); lb/le: v's own run, its local
@@ -475,12 +475,10 @@ __device__ __forceinline__ uint32_t sym_mix(uint32_t x)
     return x * x + 0x9E3779B9u;
 }
 
-/* Offsets and empty runs of every empty row, and the row holding each
- * chunk's first entry (as k_tile_first, width kChunk). */
+/* The row holding each chunk's first entry (as k_tile_first, width
+ * kChunk). */
 __global__ void __launch_bounds__(kB) k_scan_prep(const uint64_t *__restrict__ row_ptr, uint32_t n,
-                                                  uint64_t m, uint64_t chunks, uint32_t *first,
-                                                  int P, uint32_t *roff, uint64_t *lb,
-                                                  uint64_t *le)
+                                                  uint64_t m, uint64_t chunks, uint32_t *first)
 {
     const uint64_t stride = (uint64_t)gridDim.x * kB;
     for (uint64_t v = (uint64_t)blockIdx.x * kB + threadIdx.x; v <= n; v += stride) {
@@ -502,12 +500,6 @@ __global__ void __launch_bounds__(kB) k_scan_prep(const uint64_t *__restrict__ r
             a = b;
         for (uint64_t t = (a + kChunk - 1) / kChunk; t * kChunk < b; ++t)
             first[t] = (uint32_t)v;
-        if (a == b) {
-            for (int q = 0; q < P; ++q)
-                roff[(v - 1) * P + q] = 0u;
-            lb[v - 1] = a;
-            le[v - 1] = a;
-        }
     }
 }
 
@@ -569,18 +561,39 @@ __global__ void __launch_bounds__(kB, 4) k_row_scan(const uint64_t *__restrict__
         if (lane < kChunkWords)
             bits[lane] = 0u;
         __syncwarp();
-        /* starts of the non-empty rows in [j0, jend]; the array's end */
+        /* starts of the non-empty rows in [j0, jend]; the array's end.  The
+         * empty rows starting in [j0, jend) (and, in the last chunk, at the
+         * array's end) get their zero offsets and empty runs here, next to
+         * the chunk's other rows, so their partial sectors are written
+         * together */
+        auto empty_row = [&](uint64_t r, uint64_t a) {
+#pragma unroll
+            for (int q = 0; q < P; ++q)
+                roff[r * P + q] = 0u;
+            lb[r] = a;
+            le[r] = a;
+        };
         for (uint32_t r = r_lo + lane; r < r_hi; r += 32) {
             const uint64_t a = __ldg(row_ptr + r), b = __ldg(row_ptr + r + 1);
-            if (a < b && a >= j0 && a <= jend) {
-                const uint32_t o = (uint32_t)(a - j0);
-                atomicOr(&bits[o >> 5], 1u << (o & 31));
-                rowat[o] = r;
+            if (a < b) {
+                if (a >= j0 && a <= jend) {
+                    const uint32_t o = (uint32_t)(a - j0);
+                    atomicOr(&bits[o >> 5], 1u << (o & 31));
+                    rowat[o] = r;
+                }
+            } else if (a >= j0 && (a < jend || jend == m)) {
+                empty_row(r, a);
             }
         }
-        if (lane == 0 && jend == m) {
-            const uint32_t o = (uint32_t)(jend - j0);
-            atomicOr(&bits[o >> 5], 1u << (o & 31));
+        if (lane == 0) {
+            if (jend == m) {
+                const uint32_t o = (uint32_t)(jend - j0);
+                atomicOr(&bits[o >> 5], 1u << (o & 31));
+            }
+            /* empty rows just before the row holding j0, starting at j0 */
+            if (__ldg(row_ptr + r_lo) == j0)
+                for (uint64_t e = r_lo; e > 0 && __ldg(row_ptr + e - 1) == j0; --e)
+                    empty_row(e - 1, j0);
         }
         __syncwarp();
         /* this lane's start bits (and the one after them), and the last
@@ -723,7 +736,7 @@ __global__ void __launch_bounds__(kB, 4) k_row_scan(const uint64_t *__restrict__
 /* Sorted-row mode, remote end, from the partition offsets: row u's run in
  * partition q != u's own sets bit q of pmask[u] when it holds a neighbour
  * in q's giant tree, i.e. when the run is longer than the count of its
- * entries outside that tree (qcnt, written by the local end, k_ng_emit,
+ * entries outside that tree (qcnt, written by the local end, k_ng_emit_runs,
  * which also wrote their keys).  The thread owning row u stores pmask[u]
  * whole.  The raw cut count takes every valid entry outside u's own run. */
 template <int PMAX>
@@ -975,52 +988,6 @@ __global__ void __launch_bounds__(kB) k_ng_emit(EmitParams E, const uint64_t *of
                                                 uint64_t *work)
 {
     NG_PROLOGUE;
-    const int lane = threadIdx.x & 31;
-    if (E.roff) {
-        /* partition runs: a row's cut entries are its runs before and after
-         * its own; rows with at least 32 of them are walked by the whole
-         * warp, the others by their thread */
-        for (uint64_t base = (uint64_t)blockIdx.x * kB; base < E.n; base += stride) {
-            const uint64_t v = base + threadIdx.x;
-            uint64_t b = 0, e = 0, a1 = 0, c0 = 0, c1 = 0, o = 0;
-            int pv = 0;
-            uint32_t rep = 0;
-            bool on = v < E.n && ng_row<PMAX>(E, s_b, sb, (uint32_t)v, b, e, pv);
-            if (on) {
-                cut_runs(E, (uint32_t)v, pv, b, a1, c0, c1);
-                o = off[v];
-                rep = __ldg(E.label + v) - s_b[pv];
-            }
-            const uint64_t na = a1 - b, cnt = on ? na + (c1 - c0) : 0;
-            unsigned big = __ballot_sync(0xffffffffu, cnt >= 32);
-            if (cnt && cnt < 32) {
-                for (uint64_t i = 0; i < cnt; ++i) {
-                    const uint32_t u = __ldg(E.col + (i < na ? b + i : c0 + (i - na)));
-                    E.out[o + i] = make_key(E, pv, u, rep);
-                    /* the graph is symmetric: v is an entry of row u's run
-                     * in pv, and not one of pv's giant tree */
-                    atomicAdd(E.qcnt + (uint64_t)u * E.parts + pv, 1u);
-                }
-            }
-            while (big) {
-                const int src = __ffs(big) - 1;
-                big &= big - 1;
-                const uint64_t wb = __shfl_sync(0xffffffffu, b, src);
-                const uint64_t wna = __shfl_sync(0xffffffffu, na, src);
-                const uint64_t wc0 = __shfl_sync(0xffffffffu, c0, src);
-                const uint64_t wcnt = __shfl_sync(0xffffffffu, cnt, src);
-                const uint64_t wo = __shfl_sync(0xffffffffu, o, src);
-                const int wpv = __shfl_sync(0xffffffffu, pv, src);
-                const uint32_t wrep = __shfl_sync(0xffffffffu, rep, src);
-                for (uint64_t i = lane; i < wcnt; i += 32) {
-                    const uint32_t u = __ldg(E.col + (i < wna ? wb + i : wc0 + (i - wna)));
-                    E.out[wo + i] = make_key(E, wpv, u, wrep);
-                    atomicAdd(E.qcnt + (uint64_t)u * E.parts + wpv, 1u);
-                }
-            }
-        }
-        return;
-    }
     for (uint64_t v = (uint64_t)blockIdx.x * kB + threadIdx.x; v < E.n; v += stride) {
         uint64_t b, e;
         int pv;
@@ -1036,6 +1003,71 @@ __global__ void __launch_bounds__(kB) k_ng_emit(EmitParams E, const uint64_t *of
             E.out[o] = make_key(E, pv, u, rep);
             work[o] = ((uint64_t)u << 32) | (uint32_t)v;
             ++o;
+        }
+    }
+}
+
+/* Local end with partition runs: the cut entries of 32 consecutive rows
+ * (counted by k_ng_count) are one flat list for their warp, each lane
+ * taking every 32nd entry - the row of entry i is the first lane whose
+ * inclusive count exceeds i - so short and long rows alike keep every lane
+ * busy.  Each entry writes its key at the row's offset and counts itself in
+ * qcnt for the remote row (the graph is symmetric: v is an entry of row
+ * u's run in pv, and not one of pv's giant tree). */
+template <int PMAX>
+__global__ void __launch_bounds__(kB) k_ng_emit_runs(EmitParams E, const uint32_t *cnt,
+                                                     const uint64_t *off)
+{
+    NG_PROLOGUE;
+    (void)stride;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t wstride = (uint64_t)gridDim.x * kW * 32;
+    for (uint64_t base = ((uint64_t)blockIdx.x * kW + warp) * 32; base < E.n; base += wstride) {
+        const uint64_t v = base + lane;
+        const uint32_t c = v < E.n ? __ldg(cnt + v) : 0u;
+        if (!__any_sync(0xffffffffu, c != 0))
+            continue;
+        uint32_t incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o)
+                incl += y;
+        }
+        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+        const uint64_t o0 = __ldg(off + base);
+        uint64_t b = 0, a1 = 0, c0 = 0;
+        int pv = 0;
+        uint32_t rep = 0;
+        if (c) {
+            uint64_t c1;
+            b = __ldg(E.row_ptr + v);
+            pv = part_fast<PMAX>(s_b, sb, E.parts, (uint32_t)v);
+            cut_runs(E, (uint32_t)v, pv, b, a1, c0, c1);
+            rep = __ldg(E.label + v) - s_b[pv];
+        }
+        const uint32_t na = (uint32_t)(a1 - b);
+        for (uint32_t i0 = 0; i0 < total; i0 += 32) {
+            const uint32_t i = i0 + lane;
+            int ow = 0;
+#pragma unroll
+            for (int st = 16; st > 0; st >>= 1) {
+                const uint32_t y = __shfl_sync(0xffffffffu, incl, ow + st - 1);
+                if (y <= i)
+                    ow += st;
+            }
+            const uint32_t oex = __shfl_sync(0xffffffffu, incl - c, ow);
+            const uint64_t ob = __shfl_sync(0xffffffffu, b, ow);
+            const uint32_t ona = __shfl_sync(0xffffffffu, na, ow);
+            const uint64_t oc0 = __shfl_sync(0xffffffffu, c0, ow);
+            const int opv = __shfl_sync(0xffffffffu, pv, ow);
+            const uint32_t orep = __shfl_sync(0xffffffffu, rep, ow);
+            if (i < total) {
+                const uint32_t t = i - oex;
+                const uint32_t u = __ldg(E.col + (t < ona ? ob + t : oc0 + (t - ona)));
+                E.out[o0 + i] = make_key(E, opv, u, orep);
+                atomicAdd(E.qcnt + (uint64_t)u * E.parts + opv, 1u);
+            }
         }
     }
 }
@@ -2532,13 +2564,12 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
                 /* [0] local entries, [1] symmetry sum */
                 CC_TRY(cc_bufs_get(&B, (void **)&local_total, 2 * sizeof(unsigned long long)));
                 CC_CUDA(cudaMemsetAsync(local_total, 0, 2 * sizeof(unsigned long long), st));
-                /* the row holding each warp chunk's first entry and the
-                 * empty rows' offsets */
+                /* the row holding each warp chunk's first entry */
                 const uint64_t chunks = (m + kChunk - 1) / kChunk;
                 uint32_t *chunk_first = nullptr;
                 CC_TRY(cc_bufs_get(&B, (void **)&chunk_first, (chunks + 1) * sizeof(uint32_t)));
                 CC_KLAUNCH(ctx, CCK_DIST_TILES, k_scan_prep, vb, kB, 0, st, d_row_ptr, n, m,
-                           chunks, chunk_first, P, roff, rlb, rle);
+                           chunks, chunk_first);
                 const unsigned scan_b = cc_blocks(chunks, kW, (unsigned)ctx->sm_count * 16);
 #define CC_ROW_SCAN(PP)                                                                    \
     CC_KLAUNCH(ctx, CCK_DIST_LOCAL_COUNT, k_row_scan<PP>, scan_b, kB, 0, st, d_row_ptr, d_col, n, \
@@ -2664,7 +2695,14 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
                 }
                 CC_TRY(cc_bufs_get(&B, (void **)&work,
                                    (size_t)(items ? items : 1) * sizeof(uint64_t)));
-                if (P <= 4)
+                const unsigned wlb = cc_blocks((n + 31) / 32, kW, (unsigned)ctx->sm_count * 8);
+                if (E.roff && P <= 4)
+                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_emit_runs<4>, wlb, kB, 0, st, E,
+                               (const uint32_t *)cnt, (const uint64_t *)off);
+                else if (E.roff)
+                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_emit_runs<8>, wlb, kB, 0, st, E,
+                               (const uint32_t *)cnt, (const uint64_t *)off);
+                else if (P <= 4)
                     CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_emit<4>, lb, kB, 0, st, E, off,
                                work);
                 else if (P <= 8)
