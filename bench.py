@@ -547,16 +547,24 @@ NCU_TRAFFIC = {
     # scale 22 (4,194,304 vertices)
     "sample": {"per": "vertex", "bytes_per_unit": 103_996_544 / 4_194_304,
                "source": "profiles/local_cc_sample_stash_rmat22_ncu.md"},
+    # k_row_scan<4> on R-MAT scale 22 with 4 partitions: 675.1 MB moved for
+    # 681.0 MB of algorithmic bytes (its traffic follows both n and m, so it
+    # scales as a fraction of the launch's algorithmic bytes)
+    "dist_local_count": {"per": "algorithmic", "bytes_per_unit": 675_100_160 / 681_006_024,
+                         "source": "profiles/dist_row_scan_rmat22p4_ncu.md"},
 }
 
 
-def ncu_traffic(kernel, n, m):
+def ncu_traffic(kernel, n, m, algorithmic=0):
+    """DRAM bytes per launch of `kernel` from NCU_TRAFFIC, scaled by the
+    launch's units: CSR entries, vertices, or its algorithmic bytes."""
     t = NCU_TRAFFIC.get(kernel)
     if not t:
         return None
-    units = m if t["per"] == "entry" else n
-    return {"bytes_per_launch": t["bytes_per_unit"] * units, "source": t["source"],
-            "scaled": f"{t['bytes_per_unit']:.3f} bytes per {t['per']} x {units}"}
+    units = {"entry": m, "vertex": n, "algorithmic": algorithmic}[t["per"]]
+    how = (f"{t['bytes_per_unit']:.3f} x {units} algorithmic bytes" if t["per"] == "algorithmic"
+           else f"{t['bytes_per_unit']:.3f} bytes per {t['per']} x {units}")
+    return {"bytes_per_launch": t["bytes_per_unit"] * units, "source": t["source"], "scaled": how}
 
 
 def roofline_dict(dom, achieved, peak, peak_kind, traffic, bytes_per, bytes_lists, per,
@@ -684,7 +692,7 @@ def run_dist(args, torch, dist_mod, rank, world, dev):
     step_bytes = step_bytes_of(bytes_lists, per, args.steps)
     whole = step_bytes / (t_ms / 1e3) / 1e9
     value = (m // 2) * world / (t_ms / 1e3) / 1e9
-    traffic = ncu_traffic(dom, n, m)
+    traffic = ncu_traffic(dom, n, m, bytes_per.get(dom, 0))
 
     # e2e through the reference-facing calls with host buffers
     rp_h = torch.empty(n + 1, dtype=torch.int64, pin_memory=True)
@@ -1472,7 +1480,7 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
             "data": "synthetic", "config": cfg,
-            "roofline": roofline_dict(dom, achieved, peak, peak_kind, ncu_traffic(dom, n, m),
+            "roofline": roofline_dict(dom, achieved, peak, peak_kind, ncu_traffic(dom, n, m, bytes_per.get(dom, 0)),
                                       bytes_per, bytes_lists, per, total_bytes, whole),
             "kernels": {kk: {"ms": round(v[0], 5), "launches": v[1],
                              "gbs": round(bytes_per.get(kk, 0) / (v[0] / 1e3) / 1e9, 1)}
