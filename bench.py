@@ -1213,8 +1213,8 @@ def run_served(args, torch, dist_mod, rank, world, dev):
         srv = serve.Server(**srv_kw)
         # warm-up and capacity: a closed loop of requests submitted at once
         serve_run(srv, pool, order[:64], 0, 0, want_comps, want_labels, 16, closed=True)
-        cap_n = (1500 if srv_kw.get("max_batch", 4096) > 1 else 300) * \
-            (8 if spec_w["n_max"] <= 100_000 else 1)
+        # the same requests for both servers, so the capacities compare
+        cap_n = 1500 * (8 if spec_w["n_max"] <= 100_000 else 1)
         cap = serve_run(srv, pool, order[64:64 + cap_n], 0, 0, want_comps, want_labels, 16,
                         closed=True)
         out = {"capacity_graphs_per_s": cap["graphs_per_s"], "capacity_bad": cap["bad"]}
