@@ -1011,9 +1011,9 @@ __global__ void __launch_bounds__(kB) k_ng_emit(EmitParams E, const uint64_t *of
  * (counted by k_ng_count) are one flat list for their warp, each lane
  * taking every 32nd entry - the row of entry i is the first lane whose
  * inclusive count exceeds i - so short and long rows alike keep every lane
- * busy.  Each entry writes its key at the row's offset and counts itself in
- * qcnt for the remote row (the graph is symmetric: v is an entry of row
- * u's run in pv, and not one of pv's giant tree). */
+ * busy.  Each entry writes its key at the row's offset; the keys are
+ * counted per (partition, remote row) once they are sorted
+ * (k_qcnt_from_keys). */
 template <int PMAX>
 __global__ void __launch_bounds__(kB) k_ng_emit_runs(EmitParams E, const uint32_t *cnt,
                                                      const uint64_t *off)
@@ -1066,8 +1066,32 @@ __global__ void __launch_bounds__(kB) k_ng_emit_runs(EmitParams E, const uint32_
                 const uint32_t t = i - oex;
                 const uint32_t u = __ldg(E.col + (t < ona ? ob + t : oc0 + (t - ona)));
                 E.out[o0 + i] = make_key(E, opv, u, orep);
-                atomicAdd(E.qcnt + (uint64_t)u * E.parts + opv, 1u);
             }
+        }
+    }
+}
+
+/* qcnt[u*P + p] = the local-end keys (p, u, rep) with partition p and
+ * remote row u - row u's entries in partition p whose vertex lies outside
+ * p's giant tree (the graph is symmetric: v in p lists u, so u lists v).
+ * The keys are sorted, so equal (p, u) sit together: lanes holding the same
+ * pair add once, with their count. */
+__global__ void __launch_bounds__(kB) k_qcnt_from_keys(const uint64_t *__restrict__ keys,
+                                                       uint64_t count, int rb, int gb, int parts,
+                                                       uint32_t *qcnt)
+{
+    const int lane = threadIdx.x & 31;
+    const uint64_t stride = (uint64_t)gridDim.x * kB;
+    const uint64_t umask = (1ull << gb) - 1ull;
+    for (uint64_t base = (uint64_t)blockIdx.x * kB + (threadIdx.x & ~31u); base < count;
+         base += stride) {
+        const uint64_t i = base + lane;
+        const bool ok = i < count;
+        const uint64_t pu = ok ? __ldg(keys + i) >> rb : ~0ull;
+        const unsigned peers = __match_any_sync(0xffffffffu, pu);
+        if (ok && (__ffs(peers) - 1) == lane) {
+            const uint64_t u = pu & umask, p = pu >> gb;
+            atomicAdd(qcnt + u * (uint64_t)parts + p, (uint32_t)__popc(peers));
         }
     }
 }
@@ -2714,10 +2738,8 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
                 CC_CUDA(cudaMemcpyAsync(E.count, off + n, sizeof(unsigned long long),
                                         cudaMemcpyDeviceToDevice, st));
                 if (E.roff) {
-                    if (P <= 4)
-                        CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit_ranges<4>, lb, kB, 0, st, E);
-                    else
-                        CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit_ranges<8>, lb, kB, 0, st, E);
+                    /* the remote end (k_emit_ranges) runs once the local
+                     * end's keys are sorted, from their counts */
                 } else {
                     CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_mark, lb, kB, 0, st, E, work,
                                off + n);
@@ -2809,6 +2831,23 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
                                  st));
     }
     uint64_t R_all = R;
+    if (E.roff && E.qcnt) {
+        /* row-run mode: the remote end's masks from the counts of the
+         * sorted local-end keys */
+        if (R > 0)
+            CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_qcnt_from_keys,
+                       cc_blocks(R, kB, (unsigned)ctx->sm_count * 8), kB, 0, st,
+                       (const uint64_t *)sorted, R, rb, gb, P, E.qcnt);
+        const unsigned lb = cc_blocks(n, kB, (unsigned)ctx->sm_count * 8);
+        if (P <= 4)
+            CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit_ranges<4>, lb, kB, 0, st, E);
+        else
+            CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit_ranges<8>, lb, kB, 0, st, E);
+        unsigned long long raw = 0;
+        CC_CUDA(cudaMemcpyAsync(&raw, counters + 4, sizeof(raw), cudaMemcpyDeviceToHost, st));
+        CC_CUDA(cudaStreamSynchronize(st));
+        S.boundary_raw = raw;
+    }
     if (use_mask) {
         const uint32_t nblk = (uint32_t)(((uint64_t)n + kMaskBlock - 1) / kMaskBlock);
         uint32_t *mcnt = nullptr;
