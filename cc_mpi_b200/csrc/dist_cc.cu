@@ -443,8 +443,9 @@ __global__ void __launch_bounds__(kB) k_emit_sorted(EmitParams E, const uint32_t
  * position of its first entry >= b_q, so a row's offsets change only at a
  * few entries: its first entry (S), the entries where the partition of the
  * column rises (C) and its last entry (E).  The per-entry path is the same
- * for every lane - the entry's partition, the order test, the symmetry
- * hash and one event bit - and the events are resolved afterwards, the
+ * for every lane - the entry's partition, a rise bit (C), a below-its-
+ * predecessor bit and the symmetry hash; S and E bits come from the row
+ * starts as whole masks - and the events are resolved afterwards, the
  * warp's lanes spread evenly over the chunk's events, each re-reading its
  * entry and the one before it (in L1).
  *
@@ -469,6 +470,7 @@ __global__ void __launch_bounds__(kB) k_emit_sorted(EmitParams E, const uint32_t
  * that cancels only by chance (self loops add zero). */
 constexpr int kChunk = 32 * kTileE;           /* entries per warp chunk          */
 constexpr int kChunkWords = kChunk / 32 + 2;  /* start bits 0..kChunk, one spare */
+static_assert(kTileE == 16, "k_row_scan keeps a lane's start bits and the next lane's first in 17 bits");
 
 __device__ __forceinline__ uint32_t sym_mix(uint32_t x)
 {
@@ -613,7 +615,9 @@ __global__ void __launch_bounds__(kB, 4) k_row_scan(const uint64_t *__restrict__
         int excl = __shfl_up_sync(0xffffffffu, incl, 1);
         if (lane == 0)
             excl = -1;
-        uint32_t evmask = 0;
+        /* evmask: the lane's events; dmask: its entries below their
+         * predecessor (a descent unless the entry starts a row) */
+        uint32_t evmask = 0, dmask = 0;
         const uint32_t up = __shfl_up_sync(0xffffffffu, c[kTileE - 1], 1);
         if (kv > 0) {
             uint32_t r = excl >= 0 ? rowat[excl] : r_lo;
@@ -630,9 +634,8 @@ __global__ void __launch_bounds__(kB, 4) k_row_scan(const uint64_t *__restrict__
                     r = rowat[tb + k];
                     br = sym_mix(r);
                 }
-                desc |= !st && x < prev;
-                const bool ev = st || p > pp || ((sb >> (k + 1)) & 1u);
-                evmask |= (uint32_t)ev << k;
+                dmask |= (uint32_t)(x < prev) << k;
+                evmask |= (uint32_t)(p > pp) << k; /* C; S and E come from sb */
                 if (p < P)
                     sym += r * sym_mix(x) - br * x;
                 prev = x;
@@ -648,6 +651,10 @@ __global__ void __launch_bounds__(kB, 4) k_row_scan(const uint64_t *__restrict__
                     if (k < kv)
                         entry(k);
             }
+            /* S at a start bit, E before one (bit kTileE: the next lane's
+             * first entry); none past the lane's kv entries */
+            evmask |= (sb | (sb >> 1)) & (0xFFFFu >> (kTileE - kv));
+            desc |= (dmask & ~own) != 0u;
         }
         /* the chunk's events, spread over the lanes: event i is the
          * (i - before)-th set bit of the lane that holds it */
@@ -676,10 +683,21 @@ __global__ void __launch_bounds__(kB, 4) k_row_scan(const uint64_t *__restrict__
             const int oex = __shfl_sync(0xffffffffu, excl, ow);
             if (i >= total)
                 continue;
-            uint32_t mm = om; /* drop the lower set bits, then the lowest left */
-            for (uint32_t d = i - ob; d > 0; --d)
-                mm &= mm - 1u;
-            const int k = __ffs(mm) - 1;
+            /* k = the position of set bit number i - ob of om: a binary
+             * search on the bit counts of the halves (fixed cost, where
+             * dropping the lower bits one by one diverges) */
+            uint32_t mm = om, dd = i - ob;
+            int k = 0;
+#pragma unroll
+            for (int h = 8; h > 1; h >>= 1) {
+                const uint32_t lo = __popc(mm & ((1u << h) - 1u));
+                if (dd >= lo) {
+                    dd -= lo;
+                    mm >>= h;
+                    k += h;
+                }
+            }
+            k += (int)(dd >= (mm & 1u));
             const uint32_t o = (uint32_t)ow * kTileE + k;
             const uint64_t j = j0 + o;
             /* the row of j: the last start at or before it */
