@@ -710,31 +710,33 @@ __global__ void __launch_bounds__(kB, 4) k_row_scan(const uint64_t *__restrict__
             const int pj = part(__ldg(col + j));
             const int pp = st || j == 0 ? -1 : part(__ldg(col + j - 1));
             uint32_t *ro = roff + (uint64_t)r * P;
-            if (st || pj > pp) {
-                for (int q = pp + 1; q <= pj; ++q) {
+            /* S / C: bounds pp+1..pj are first reached at j; E: bounds
+             * above pj are never reached, they take the row's end.  One
+             * unrolled pass over the bounds, predicated, for every lane */
+            const bool lo_ev = st || pj > pp;
+            const uint32_t vlo = (uint32_t)(j - rbase);
+#pragma unroll
+            for (int q = 0; q <= P; ++q) {
+                const bool wl = lo_ev && q > pp && q <= pj;
+                const bool wh = en && q > pj;
+                if (wl || wh) {
+                    const uint64_t at = wh ? j + 1 : j;
                     if (q >= 1)
-                        ro[q - 1] = (uint32_t)(j - rbase);
+                        ro[q - 1] = wh ? vlo + 1u : vlo;
                     if (q == pr)
-                        lb[r] = j;
+                        lb[r] = at;
                     if (q == pr + 1)
-                        le[r] = j;
+                        le[r] = at;
                 }
+            }
+            if (lo_ev) {
                 if (pj == pr)
                     local -= j;
                 if (pp == pr)
                     local += j;
             }
-            if (en) {
-                for (int q = pj + 1; q <= P; ++q) {
-                    ro[q - 1] = (uint32_t)(j + 1 - rbase);
-                    if (q == pr)
-                        lb[r] = j + 1;
-                    if (q == pr + 1)
-                        le[r] = j + 1;
-                }
-                if (pj == pr)
-                    local += j + 1;
-            }
+            if (en && pj == pr)
+                local += j + 1;
         }
         __syncwarp(); /* bits, rowat are rewritten by the next chunk */
     }
@@ -1885,95 +1887,28 @@ __global__ void k_plan(const uint32_t *__restrict__ ghost_v, const uint64_t *__r
     seg[t] = lo;
 }
 
-/* A run of buckets [lo, hi) of the flattened bucket table that all hold
- * val: a range too long for one warp, filled by the whole grid. */
-struct BucketFill {
-    uint64_t lo, hi;
-    uint32_t val;
-};
-constexpr uint64_t kWarpFill = 4096; /* longest range one warp fills */
-
 /* Id buckets of every partition's ghost list: gbucket[p*(nb+1) + b] = the
  * first of p's ghosts with id >= b << shift (p's ghosts ascend), for
- * b = 0..nb.  One pass over the ghosts: ghost g owns the buckets from just
- * after its predecessor's up to its own (so each bucket is written once),
- * p's last ghost the buckets after it, and a partition without ghosts has
- * every bucket at gh_off[p].  Ranges up to 32 buckets are written by their
- * lane, up to kWarpFill by the warp; longer ones (the gap over a
- * partition's own ids) go to `fills` for k_bucket_fill.  `fills` holds
- * parts * ((nb + 1) / kWarpFill + 2) entries: the long ranges of one
- * partition are disjoint and each longer than kWarpFill. */
+ * b = 0..nb; one binary search per bucket. */
 __global__ void __launch_bounds__(kB) k_ghost_buckets(const uint32_t *__restrict__ ghost_v,
                                                       const uint64_t *__restrict__ gh_off,
                                                       int parts, uint32_t nb, int shift,
-                                                      uint32_t *gbucket, BucketFill *fills,
-                                                      uint32_t *nfill)
+                                                      uint32_t *gbucket)
 {
-    __shared__ uint64_t s_off[CCGPU_MAX_PARTS + 1];
-    for (int i = threadIdx.x; i <= parts; i += kB)
-        s_off[i] = gh_off[i];
-    __syncthreads();
-    const uint64_t row = (uint64_t)nb + 1;
-    if (blockIdx.x == 0 && threadIdx.x < parts && s_off[threadIdx.x] == s_off[threadIdx.x + 1]) {
-        const uint32_t at = atomicAdd(nfill, 1u);
-        fills[at] = {threadIdx.x * row, (threadIdx.x + 1) * row, (uint32_t)s_off[threadIdx.x]};
-    }
-    const uint64_t G = s_off[parts];
+    const uint64_t total = (uint64_t)parts * (nb + 1);
     const uint64_t stride = (uint64_t)gridDim.x * kB;
-    const int lane = threadIdx.x & 31;
-    for (uint64_t base = (uint64_t)blockIdx.x * kB + (threadIdx.x & ~31u); base < G;
-         base += stride) {
-        const uint64_t g = base + lane;
-        /* this ghost's flattened bucket range [lo, hi), then p's tail */
-        uint64_t lo = 0, hi = 0, tlo = 0, thi = 0;
-        if (g < G) {
-            int p = 0;
-            while (p + 1 < parts && s_off[p + 1] <= g)
-                ++p;
-            const uint64_t b0 = (uint64_t)p * row;
-            lo = b0 + (g == s_off[p] ? 0 : (uint64_t)(__ldg(ghost_v + g - 1) >> shift) + 1);
-            hi = b0 + (__ldg(ghost_v + g) >> shift) + 1;
-            if (g + 1 == s_off[p + 1]) {
-                tlo = hi;
-                thi = b0 + row;
-            }
+    for (uint64_t i = (uint64_t)blockIdx.x * kB + threadIdx.x; i < total; i += stride) {
+        const int p = (int)(i / (nb + 1));
+        const uint64_t key = (uint64_t)(i % (nb + 1)) << shift;
+        uint64_t lo = gh_off[p], hi = gh_off[p + 1];
+        while (lo < hi) {
+            const uint64_t mid = lo + (hi - lo) / 2;
+            if (__ldg(ghost_v + mid) < key)
+                lo = mid + 1;
+            else
+                hi = mid;
         }
-        auto fill = [&](uint64_t a, uint64_t z, uint32_t v) {
-            const uint64_t len = z - a;
-            if (len <= 32)
-                for (uint64_t bb = a; bb < z; ++bb)
-                    gbucket[bb] = v;
-            else if (len > kWarpFill) {
-                const uint32_t at = atomicAdd(nfill, 1u);
-                fills[at] = {a, z, v};
-            }
-            unsigned many = __ballot_sync(0xffffffffu, len > 32 && len <= kWarpFill);
-            while (many) {
-                const int src = __ffs(many) - 1;
-                many &= many - 1;
-                const uint64_t wa = __shfl_sync(0xffffffffu, a, src);
-                const uint64_t wz = __shfl_sync(0xffffffffu, z, src);
-                const uint32_t wv = __shfl_sync(0xffffffffu, v, src);
-                for (uint64_t bb = wa + lane; bb < wz; bb += 32)
-                    gbucket[bb] = wv;
-            }
-        };
-        fill(lo, hi, (uint32_t)g);
-        fill(tlo, thi, (uint32_t)g + 1);
-    }
-}
-
-/* The long bucket ranges k_ghost_buckets recorded, spread over the grid. */
-__global__ void __launch_bounds__(kB) k_bucket_fill(const BucketFill *__restrict__ fills,
-                                                    const uint32_t *__restrict__ nfill,
-                                                    uint32_t *gbucket)
-{
-    const uint32_t nf = *nfill;
-    const uint64_t stride = (uint64_t)gridDim.x * kB;
-    for (uint32_t f = 0; f < nf; ++f) {
-        const BucketFill F = fills[f];
-        for (uint64_t bb = F.lo + (uint64_t)blockIdx.x * kB + threadIdx.x; bb < F.hi; bb += stride)
-            gbucket[bb] = F.val;
+        gbucket[i] = (uint32_t)lo;
     }
 }
 
@@ -3061,20 +2996,9 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
     const uint32_t gnb = (uint32_t)((n >> gshift) + 1);
     uint32_t *gbucket = nullptr;
     CC_TRY(cc_bufs_get(&B, (void **)&gbucket, (size_t)P * (gnb + 1) * sizeof(uint32_t)));
-    {
-        BucketFill *fills = nullptr;
-        uint32_t *nfill = nullptr;
-        const size_t nf = (size_t)P * ((gnb + 1) / kWarpFill + 2);
-        CC_TRY(cc_bufs_get(&B, (void **)&fills, nf * sizeof(BucketFill)));
-        CC_TRY(cc_bufs_get(&B, (void **)&nfill, sizeof(uint32_t)));
-        CC_CUDA(cudaMemsetAsync(nfill, 0, sizeof(uint32_t), st));
-        CC_KLAUNCH(ctx, CCK_DIST_PLAN, k_ghost_buckets,
-                   cc_blocks(G ? G : 1, kB, (unsigned)ctx->sm_count * 8), kB, 0, st, D.ghost_v,
-                   gh_off, P, gnb, gshift, gbucket, fills, nfill);
-        CC_KLAUNCH(ctx, CCK_DIST_PLAN, k_bucket_fill,
-                   cc_blocks((uint64_t)P * (gnb + 1), kB, (unsigned)ctx->sm_count * 4), kB, 0,
-                   st, fills, nfill, gbucket);
-    }
+    CC_KLAUNCH(ctx, CCK_DIST_PLAN, k_ghost_buckets,
+               cc_blocks((uint64_t)P * (gnb + 1), kB, (unsigned)ctx->sm_count * 8), kB, 0, st,
+               D.ghost_v, gh_off, P, gnb, gshift, gbucket);
     CC_TRY(clock_mark(clk, st)); /* 5 */
     if (o.verbose >= 2) {
         for (int p = 0; p < P; ++p)

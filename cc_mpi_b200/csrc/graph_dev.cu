@@ -16,6 +16,8 @@ struct ccgpu_graph {
     uint64_t m;
     int device;
     size_t rp_cap, col_cap; /* bytes allocated for row_ptr / col */
+    uint32_t *labels;       /* ccgpu_graph_label_array, lab_cap bytes */
+    size_t lab_cap;
 };
 
 namespace {
@@ -29,6 +31,8 @@ struct GraphCache {
     uint64_t *row_ptr = nullptr;
     uint32_t *col = nullptr;
     size_t rp_cap = 0, col_cap = 0;
+    uint32_t *labels = nullptr;
+    size_t lab_cap = 0;
 };
 GraphCache g_gcache[kGraphCacheDevices];
 std::mutex g_gcache_mu;
@@ -47,6 +51,8 @@ cudaError_t graph_arrays(ccgpu_graph *g, size_t rp_bytes, size_t col_bytes)
                 g->col = c.col;
                 g->rp_cap = c.rp_cap;
                 g->col_cap = c.col_cap;
+                g->labels = c.labels;
+                g->lab_cap = c.lab_cap;
                 c = GraphCache();
                 return cudaSuccess;
             }
@@ -73,6 +79,7 @@ cudaError_t graph_arrays(ccgpu_graph *g, size_t rp_bytes, size_t col_bytes)
                 GraphCache &c = g_gcache[g->device];
                 cudaFree(c.row_ptr);
                 cudaFree(c.col);
+                cudaFree(c.labels);
                 c = GraphCache();
             }
         } else {
@@ -169,12 +176,15 @@ extern "C" void ccgpu_graph_free(ccgpu_graph *g)
             c.col = g->col;
             c.rp_cap = g->rp_cap;
             c.col_cap = g->col_cap;
+            c.labels = g->labels;
+            c.lab_cap = g->lab_cap;
             kept = true;
         }
     }
     if (!kept) {
         cudaFree(g->row_ptr);
         cudaFree(g->col);
+        cudaFree(g->labels);
     }
     if (cur >= 0 && cur != g->device)
         cudaSetDevice(cur);
@@ -185,6 +195,32 @@ extern "C" const uint64_t *ccgpu_graph_row_ptr(const ccgpu_graph *g) { return g 
 extern "C" const uint32_t *ccgpu_graph_col_idx(const ccgpu_graph *g) { return g ? g->col : nullptr; }
 extern "C" uint32_t ccgpu_graph_n(const ccgpu_graph *g) { return g ? g->n : 0; }
 extern "C" uint64_t ccgpu_graph_m(const ccgpu_graph *g) { return g ? g->m : 0; }
+
+extern "C" int ccgpu_graph_label_array(ccgpu_graph *g, uint32_t **d_labels)
+{
+    if (!g || !d_labels)
+        return ccgpu_set_error(CCGPU_ERR_INVALID, "ccgpu_graph_label_array: NULL argument");
+    const size_t bytes = (size_t)(g->n ? g->n : 1) * sizeof(uint32_t);
+    if (!g->labels || g->lab_cap < bytes) {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (cur != g->device)
+            cudaSetDevice(g->device);
+        cudaFree(g->labels);
+        g->labels = nullptr;
+        g->lab_cap = 0;
+        cudaError_t e = cudaMalloc((void **)&g->labels, bytes);
+        if (cur >= 0 && cur != g->device)
+            cudaSetDevice(cur);
+        if (e != cudaSuccess) {
+            g->labels = nullptr;
+            return ccgpu_cuda_fail(e, "ccgpu_graph_label_array", __FILE__, __LINE__);
+        }
+        g->lab_cap = bytes;
+    }
+    *d_labels = g->labels;
+    return CCGPU_OK;
+}
 
 /* ------------------------------------------------- CSC -> CSR on device */
 

@@ -21,8 +21,7 @@
 
 typedef struct mirror {
     const uint64_t *host_row_ptr;
-    ccgpu_graph *dev;
-    uint32_t *d_labels; /* [n] scratch labels for solves with host output */
+    ccgpu_graph *dev; /* its label array holds solves with host output */
     struct mirror *next;
 } mirror;
 
@@ -68,7 +67,6 @@ static void reg_drop(const uint64_t *row_ptr)
             mirror *m = *pp;
             *pp = m->next;
             ccgpu_graph_free(m->dev);
-            ccgpu_free(m->d_labels);
             free(m);
             break;
         }
@@ -270,8 +268,9 @@ int cc_mpi_solve(const DistCSRGraph *Gd, uint32_t *labels_global, int chunk_size
     int rc = reg_get(Gd, &m);
     if (rc != CCGPU_OK)
         return rc;
-    if (labels_global && !m->d_labels) {
-        rc = ccgpu_alloc((void **)&m->d_labels, (size_t)Gd->n_global * sizeof(uint32_t));
+    uint32_t *d_labels = NULL;
+    if (labels_global) {
+        rc = ccgpu_graph_label_array(m->dev, &d_labels);
         if (rc != CCGPU_OK)
             return rc;
     }
@@ -284,12 +283,12 @@ int cc_mpi_solve(const DistCSRGraph *Gd, uint32_t *labels_global, int chunk_size
     o.verbose = cc_group_verbose(grp);
     ccgpu_dist_stats s;
     rc = ccgpu_dist_cc(NULL, ccgpu_graph_row_ptr(m->dev), ccgpu_graph_col_idx(m->dev),
-                       Gd->n_global, Gd->m_global, &o, labels_global ? m->d_labels : NULL, NULL,
+                       Gd->n_global, Gd->m_global, &o, d_labels, NULL,
                        &s, NULL);
     if (rc != CCGPU_OK)
         return rc;
     if (labels_global) {
-        rc = ccgpu_memcpy_d2h(labels_global, m->d_labels, (size_t)Gd->n_global * sizeof(uint32_t));
+        rc = ccgpu_memcpy_d2h(labels_global, d_labels, (size_t)Gd->n_global * sizeof(uint32_t));
         if (rc != CCGPU_OK)
             return rc;
     }

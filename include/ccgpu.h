@@ -106,6 +106,10 @@ const uint64_t *ccgpu_graph_row_ptr(const ccgpu_graph *g);
 const uint32_t *ccgpu_graph_col_idx(const ccgpu_graph *g);
 uint32_t ccgpu_graph_n(const ccgpu_graph *g);
 uint64_t ccgpu_graph_m(const ccgpu_graph *g);
+/* A device array of n labels that belongs to the graph: allocated on the
+ * first call, kept with the graph's arrays by ccgpu_graph_free, so a load /
+ * solve / free cycle with host output allocates it once. */
+int ccgpu_graph_label_array(ccgpu_graph *g, uint32_t **d_labels);
 
 /* ------------------------------------------------------------------------
  * Local CC (the kernel behind compute_connected_components_pthreads,
