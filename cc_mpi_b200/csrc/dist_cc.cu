@@ -33,6 +33,7 @@
  * without re-reading every pair.
  */
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -44,6 +45,19 @@ namespace {
 constexpr int kB = 256;
 constexpr int kW = kB / 32;
 constexpr int kTileE = 16;              /* column entries per thread in a tile */
+constexpr uint64_t kGhostMapBytes = 2ull << 30; /* direct ghost map budget  */
+
+/* The direct ghost map's budget in bytes: kGhostMapBytes, or the value of
+ * CCGPU_GHOST_MAP_BYTES when set (0 keeps every solve on the id buckets). */
+static uint64_t ghost_map_budget()
+{
+    const char *e = getenv("CCGPU_GHOST_MAP_BYTES");
+    if (!e || !*e)
+        return kGhostMapBytes;
+    char *end = nullptr;
+    const unsigned long long v = strtoull(e, &end, 10);
+    return end && *end == '\0' ? (uint64_t)v : kGhostMapBytes;
+}
 constexpr int kTile = kB * kTileE;      /* column entries per tile             */
 constexpr int kDedupItems = 16;
 constexpr uint64_t kDedupTile = kB * kDedupItems;
@@ -1912,6 +1926,28 @@ __global__ void __launch_bounds__(kB) k_ghost_buckets(const uint32_t *__restrict
     }
 }
 
+/* Direct ghost map, for graphs where parts * n words fit the budget:
+ * gmap[p*n + v] = the index of ghost v in p's list, ~0u (set by a memset
+ * beforehand) for ids that are not p's ghosts.  One write per ghost; p's
+ * ghosts ascend, so a warp's writes fall in a few lines. */
+__global__ void __launch_bounds__(kB) k_ghost_map(const uint32_t *__restrict__ ghost_v,
+                                                  const uint64_t *__restrict__ gh_off, int parts,
+                                                  uint64_t n, uint32_t *gmap)
+{
+    __shared__ uint64_t s_off[CCGPU_MAX_PARTS + 1];
+    for (int i = threadIdx.x; i <= parts; i += kB)
+        s_off[i] = gh_off[i];
+    __syncthreads();
+    const uint64_t G = s_off[parts];
+    const uint64_t stride = (uint64_t)gridDim.x * kB;
+    for (uint64_t g = (uint64_t)blockIdx.x * kB + threadIdx.x; g < G; g += stride) {
+        int p = 0;
+        while (p + 1 < parts && s_off[p + 1] <= g)
+            ++p;
+        gmap[(uint64_t)p * n + __ldg(ghost_v + g)] = (uint32_t)g;
+    }
+}
+
 /* ------------------------------------------------------------- merge */
 
 /* Round state of a merge driven on the device (k_merge_ctl, one graph
@@ -1947,6 +1983,8 @@ struct MergeParams {
     unsigned long long *sent;
     uint32_t *ghost_rep;          /* [ghosts] local rep of each ghost vertex */
     int ghost_rep_ready;          /* 0: k_exchange fills ghost_rep from label[] */
+    const uint32_t *gmap;         /* [parts*n] ghost index per (p, id), ~0u: none;
+                                   * NULL: the buckets below are used      */
     const uint32_t *gbucket;      /* [parts*(gnb+1)] first ghost of each id bucket */
     uint32_t gnb;                 /* id buckets per partition                      */
     int gshift;                   /* bucket = id >> gshift                         */
@@ -2033,6 +2071,13 @@ __device__ __forceinline__ bool label_of(const MergeParams &M, const uint32_t *c
 {
     if (x >= s_b[p] && x < s_b[p + 1]) {
         y = cur[__ldg(M.label + x)];
+        return true;
+    }
+    if (M.gmap) {
+        const uint32_t gi = x < M.n ? __ldg(M.gmap + (uint64_t)p * M.n + x) : 0xffffffffu;
+        if (gi == 0xffffffffu)
+            return false;
+        y = M.ghost_labels[gi];
         return true;
     }
     /* p's ghosts are ascending; the bucket of x narrows the search */
@@ -2988,17 +3033,30 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
         CC_KLAUNCH(ctx, CCK_DIST_PLAN, k_plan, (tot + kB - 1) / kB, kB, 0, st, D.ghost_v, gh_off,
                    bounds, P, segs);
     }
-    /* id buckets of the ghost lists for the merge's lookups: about 16 ids
-     * per bucket, at most ~64 MB in all */
+    /* the merge's ghost lookups: a direct map when parts * n words fit in
+     * the budget (one load per lookup), else id buckets of the ghost
+     * lists (about 16 ids per bucket, at most ~64 MB in all) and a short
+     * binary search */
+    uint32_t *gmap = nullptr, *gbucket = nullptr;
     int gshift = 4;
-    while (gshift < 31 && (uint64_t)P * ((n >> gshift) + 2) * 4 > (64ull << 20))
-        ++gshift;
-    const uint32_t gnb = (uint32_t)((n >> gshift) + 1);
-    uint32_t *gbucket = nullptr;
-    CC_TRY(cc_bufs_get(&B, (void **)&gbucket, (size_t)P * (gnb + 1) * sizeof(uint32_t)));
-    CC_KLAUNCH(ctx, CCK_DIST_PLAN, k_ghost_buckets,
-               cc_blocks((uint64_t)P * (gnb + 1), kB, (unsigned)ctx->sm_count * 8), kB, 0, st,
-               D.ghost_v, gh_off, P, gnb, gshift, gbucket);
+    uint32_t gnb = 0;
+    const uint64_t map_bytes = (uint64_t)P * n * sizeof(uint32_t);
+    if (map_bytes <= ghost_map_budget()) {
+        CC_TRY(cc_bufs_get(&B, (void **)&gmap, (size_t)map_bytes));
+        CC_CUDA(cudaMemsetAsync(gmap, 0xff, (size_t)map_bytes, st));
+        if (G)
+            CC_KLAUNCH(ctx, CCK_DIST_PLAN, k_ghost_map,
+                       cc_blocks(G, kB, (unsigned)ctx->sm_count * 8), kB, 0, st, D.ghost_v,
+                       gh_off, P, (uint64_t)n, gmap);
+    } else {
+        while (gshift < 31 && (uint64_t)P * ((n >> gshift) + 2) * 4 > (64ull << 20))
+            ++gshift;
+        gnb = (uint32_t)((n >> gshift) + 1);
+        CC_TRY(cc_bufs_get(&B, (void **)&gbucket, (size_t)P * (gnb + 1) * sizeof(uint32_t)));
+        CC_KLAUNCH(ctx, CCK_DIST_PLAN, k_ghost_buckets,
+                   cc_blocks((uint64_t)P * (gnb + 1), kB, (unsigned)ctx->sm_count * 8), kB, 0,
+                   st, D.ghost_v, gh_off, P, gnb, gshift, gbucket);
+    }
     CC_TRY(clock_mark(clk, st)); /* 5 */
     if (o.verbose >= 2) {
         for (int p = 0; p < P; ++p)
@@ -3026,6 +3084,7 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
     M.prev_sent = D.prev_sent;
     M.ghosts = G;
     M.gh_off = gh_off;
+    M.gmap = gmap;
     M.gbucket = gbucket;
     M.gnb = gnb;
     M.gshift = gshift;

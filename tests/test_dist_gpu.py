@@ -280,3 +280,23 @@ def test_host_and_device_driven_rounds_agree(torch):
                 _lib.check(L.ccgpu_prof_enable(None, 0))
             assert dev_st.rounds == host_st.rounds and dev_st.exchanges == host_st.exchanges, name
             assert dev_st.sent_pairs == host_st.sent_pairs, name
+
+
+@pytest.mark.gpu
+def test_ghost_map_and_buckets_agree(torch, monkeypatch):
+    """The merge finds a ghost's slot through a direct (partition, id) map
+    when parts * n words fit the budget, else through id buckets and a
+    binary search; CCGPU_GHOST_MAP_BYTES=0 forces the buckets.  Both give
+    the oracle's labels and the same round, exchange and sent-pair counts."""
+    sc = graphs.small_cases()
+    cases = {"zigzag": sc["zigzag"], "er": sc["er2k"], "rmat": graphs.rmat_csr(12, 8, seed=45)}
+    for name, (rp, col) in cases.items():
+        for parts, interval in ((3, 1), (8, 2)):
+            monkeypatch.delenv("CCGPU_GHOST_MAP_BYTES", raising=False)
+            map_st = check_against_oracle(torch, rp, col, parts, 1, interval)
+            monkeypatch.setenv("CCGPU_GHOST_MAP_BYTES", "0")
+            bucket_st = check_against_oracle(torch, rp, col, parts, 1, interval)
+            monkeypatch.delenv("CCGPU_GHOST_MAP_BYTES")
+            assert map_st.rounds == bucket_st.rounds, name
+            assert map_st.exchanges == bucket_st.exchanges, name
+            assert map_st.sent_pairs == bucket_st.sent_pairs, name
