@@ -1927,9 +1927,11 @@ __global__ void __launch_bounds__(kB) k_ghost_buckets(const uint32_t *__restrict
 }
 
 /* Direct ghost map, for graphs where parts * n words fit the budget:
- * gmap[p*n + v] = the index of ghost v in p's list, ~0u (set by a memset
- * beforehand) for ids that are not p's ghosts.  One write per ghost; p's
- * ghosts ascend, so a warp's writes fall in a few lines. */
+ * gmap[p*n + v] = the index of ghost v in p's list.  Only ghosts' slots are
+ * written (one write per ghost; p's ghosts ascend, so a warp's writes fall
+ * in a few lines); the others keep whatever the memory held, and a lookup
+ * accepts a slot only when its index lies in p's list and that ghost is
+ * the id looked up (label_of). */
 __global__ void __launch_bounds__(kB) k_ghost_map(const uint32_t *__restrict__ ghost_v,
                                                   const uint64_t *__restrict__ gh_off, int parts,
                                                   uint64_t n, uint32_t *gmap)
@@ -2074,11 +2076,14 @@ __device__ __forceinline__ bool label_of(const MergeParams &M, const uint32_t *c
         return true;
     }
     if (M.gmap) {
+        /* the map is not cleared: a slot of an id that is not p's ghost
+         * holds anything, so the index must fall in p's list and name x */
         const uint32_t gi = x < M.n ? __ldg(M.gmap + (uint64_t)p * M.n + x) : 0xffffffffu;
-        if (gi == 0xffffffffu)
+        if (gi < M.gh_off[p] || gi >= M.gh_off[p + 1])
             return false;
+        const uint32_t gv = __ldg(M.ghost_v + gi);
         y = M.ghost_labels[gi];
-        return true;
+        return gv == x;
     }
     /* p's ghosts are ascending; the bucket of x narrows the search */
     const uint32_t *bk = M.gbucket + (uint64_t)p * (M.gnb + 1) + (x >> M.gshift);
@@ -3034,7 +3039,8 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
                    bounds, P, segs);
     }
     /* the merge's ghost lookups: a direct map when parts * n words fit in
-     * the budget (one load per lookup), else id buckets of the ghost
+     * the budget (one load per lookup, then the ghost's id and label
+     * together), else id buckets of the ghost
      * lists (about 16 ids per bucket, at most ~64 MB in all) and a short
      * binary search */
     uint32_t *gmap = nullptr, *gbucket = nullptr;
@@ -3043,7 +3049,6 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
     const uint64_t map_bytes = (uint64_t)P * n * sizeof(uint32_t);
     if (map_bytes <= ghost_map_budget()) {
         CC_TRY(cc_bufs_get(&B, (void **)&gmap, (size_t)map_bytes));
-        CC_CUDA(cudaMemsetAsync(gmap, 0xff, (size_t)map_bytes, st));
         if (G)
             CC_KLAUNCH(ctx, CCK_DIST_PLAN, k_ghost_map,
                        cc_blocks(G, kB, (unsigned)ctx->sm_count * 8), kB, 0, st, D.ghost_v,
