@@ -521,14 +521,14 @@ def dist_bytes(torch, ldeg, n, m, st, chunk):
         "dist_reps": [4 * n + 12 * reps],
         "dist_pairs_local": [n // 8 + 8 * R],
         "sort_hist": [8 * R], "sort_scatter": [16 * R], "dist_dedup": [8 * R],
-        "dist_ghosts": [8 * R + 8 * U + 24 * G], "merge_hook": [12 * U],
-        # an exchange reads each ghost's cached rep and last-sent label (8G)
-        # and writes last-sent, ghost label and delta entry of every changed
-        # ghost (12 per sent pair); the first exchange changes all G ghosts,
+        "dist_ghosts": [8 * R + 8 * U + 20 * G], "merge_hook": [12 * U],
+        # an exchange reads each ghost's cached rep and its label, the last
+        # one sent (8G), and writes the ghost label and delta entry of every
+        # changed ghost (8 per sent pair); the first exchange changes all G ghosts,
         # so its hook update is the pull pass over all pairs (12U) whenever
         # G > U/8 - later ones are counted as push (pairs walked not counted)
         "merge_upd": [12 * reps],
-        "merge_exchange": [8 * G + 12 * int(st.sent_pairs) // max(int(st.exchanges), 1)],
+        "merge_exchange": [8 * G + 8 * int(st.sent_pairs) // max(int(st.exchanges), 1)],
         "merge_exch_push": [0],
         "merge_exch_pull": [12 * U * (1 if 8 * G > U else 0) // max(int(st.exchanges), 1)],
         "dist_labels": [12 * n], "dist_plan": [0], "dist_bounds": [0], "scan": [0],

@@ -1728,7 +1728,7 @@ struct DedupParams {
     uint32_t *pair_rep, *pair_g;       /* [U]               */
     uint32_t *ghost_v;                 /* [G]               */
     uint64_t *ghost_pairs;             /* [G+1] first pair  */
-    uint32_t *ghost_labels, *prev_sent;
+    uint32_t *ghost_labels;
     uint64_t *gh_first;                /* [parts] first ghost of each partition, ~0 if none */
 };
 
@@ -1861,8 +1861,7 @@ __global__ void __launch_bounds__(kB) k_dedup_write(DedupParams D)
                 D.gh_first[p] = my; /* first ghost of partition p */
             D.ghost_v[my] = remote;
             D.ghost_pairs[my] = up + __popc(bu & lt);
-            D.ghost_labels[my] = remote;   /* src/cc_mpi.c:456-457 */
-            D.prev_sent[my] = 0xffffffffu; /* src/cc_mpi.c:480-487 */
+            D.ghost_labels[my] = remote; /* src/cc_mpi.c:456-457 */
         }
         if (u) {
             const uint64_t my = up + __popc(bu & lt);
@@ -1975,7 +1974,6 @@ struct MergeParams {
     const uint32_t *ghost_v;
     const uint64_t *ghost_pairs;
     uint32_t *ghost_labels;
-    uint32_t *prev_sent;
     uint64_t ghosts;
     const uint64_t *gh_off;       /* [parts+1] */
     const uint64_t *seg;          /* [parts*(parts+1)] */
@@ -2137,14 +2135,17 @@ __global__ void __launch_bounds__(kB) k_upd(MergeParams M)
  * for q, which is the index range of p's ghosts owned by q, so a message's
  * slot at the reader is its ghost.  One pass therefore does the sender's
  * pack and the reader's scatter: for every ghost g whose owner's current
- * label fell below what was last sent (prev_sent, ~0 before the first
- * exchange) the label goes straight into ghost_labels[g], and g is appended
+ * label fell below what was last sent the label goes straight into
+ * ghost_labels[g], and g is appended
  * to the exchange's delta list - the in-HBM compaction of the changed
  * boundary labels - with one slot reservation per block step of
  * kExchRounds * kB ghosts (a counter taken once per 256 ghosts was the
  * kernel's bottleneck).  The delta list
  * drives the hook update (k_delta_push) and its length is the reference's
- * count of sent pairs. */
+ * count of sent pairs.  The reference's prev_sent (src/cc_mpi.c:480-487,
+ * ~0 at first) needs no array here: the first exchange sends every label
+ * (each is below ~0), and from then on a slot's last sent label and its
+ * ghost label change together, so ghost_labels[g] is the last sent label. */
 constexpr int kExchRounds = 8; /* ghosts per thread per block step */
 
 __global__ void __launch_bounds__(kB) k_exchange(MergeParams M)
@@ -2189,14 +2190,13 @@ __global__ void __launch_bounds__(kB) k_exchange(MergeParams M)
         for (int i = 0; i < kExchRounds; ++i) {
             const uint64_t g = base + (uint64_t)i * kB + threadIdx.x;
             lbl[i] = look[i] ? cur[rep[i]] : 0xffffffffu;
-            ps[i] = look[i] ? M.prev_sent[g] : 0u;
+            ps[i] = look[i] ? (ready ? M.ghost_labels[g] : 0xffffffffu) : 0u;
         }
         uint32_t sendmask = 0;
 #pragma unroll
         for (int i = 0; i < kExchRounds; ++i) {
             if (look[i] && lbl[i] < ps[i]) {
                 const uint64_t g = base + (uint64_t)i * kB + threadIdx.x;
-                M.prev_sent[g] = lbl[i];
                 M.ghost_labels[g] = lbl[i];
                 sendmask |= 1u << i;
             }
@@ -3017,7 +3017,6 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
     CC_TRY(cc_bufs_get(&B, (void **)&D.ghost_v, (size_t)(G ? G : 1) * sizeof(uint32_t)));
     CC_TRY(cc_bufs_get(&B, (void **)&D.ghost_pairs, (size_t)(G + 1) * sizeof(uint64_t)));
     CC_TRY(cc_bufs_get(&B, (void **)&D.ghost_labels, (size_t)(G ? G : 1) * sizeof(uint32_t)));
-    CC_TRY(cc_bufs_get(&B, (void **)&D.prev_sent, (size_t)(G ? G : 1) * sizeof(uint32_t)));
     if (R_all > 0) {
         CC_KLAUNCH(ctx, CCK_DIST_GHOSTS, k_dedup_write, (unsigned)T, kB, 0, st, D);
         CC_CUDA(cudaMemcpyAsync(D.ghost_pairs + G, &U, sizeof(uint64_t), cudaMemcpyHostToDevice,
@@ -3086,7 +3085,6 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
     M.ghost_v = D.ghost_v;
     M.ghost_pairs = D.ghost_pairs;
     M.ghost_labels = D.ghost_labels;
-    M.prev_sent = D.prev_sent;
     M.ghosts = G;
     M.gh_off = gh_off;
     M.gmap = gmap;
