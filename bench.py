@@ -502,8 +502,9 @@ def dist_bytes(torch, ldeg, n, m, st, chunk):
             # k_row_scan: every column entry and row pointer in; P offsets
             # and the own run (begin, end) of every row out
             "dist_local_count": [4 * m + 8 * (n + 1) + 4 * P * n + 16 * n],
-            # k_emit_ranges: P offsets and P run counts in, mask out
-            "dist_pairs": [8 * P * n + 4 * n],
+            # k_emit_ranges: P offsets in, mask out; k_mask_fix: the sorted
+            # local-end keys in (the run lengths and masks it touches are few)
+            "dist_pairs": [4 * P * n + 4 * n, 8 * R],
         })
     else:
         out.update({

@@ -157,9 +157,6 @@ struct EmitParams {
                               * mirror entry is missing: sorted-row mode invalid */
     const uint32_t *roff;    /* [n*parts] partition offsets of sorted rows
                               * (k_row_scan), NULL = not computed        */
-    uint32_t *qcnt;          /* [n*parts] with roff: entries of row u's run in
-                              * partition q whose vertex is outside q's giant
-                              * tree, counted from their local end         */
 };
 
 /* Plain keys are rare (most cut entries fall in a giant tree), so a block
@@ -767,12 +764,11 @@ __global__ void __launch_bounds__(kB, 4) k_row_scan(const uint64_t *__restrict__
         atomicOr(flags, 1u);
 }
 
-/* Sorted-row mode, remote end, from the partition offsets: row u's run in
- * partition q != u's own sets bit q of pmask[u] when it holds a neighbour
- * in q's giant tree, i.e. when the run is longer than the count of its
- * entries outside that tree (qcnt, written by the local end, k_ng_emit_runs,
- * which also wrote their keys).  The thread owning row u stores pmask[u]
- * whole.  The raw cut count takes every valid entry outside u's own run. */
+/* Sorted-row mode, remote end, from the partition offsets: every non-empty
+ * run of row u in a partition q != u's own sets bit q of pmask[u]; the runs
+ * that hold no neighbour in q's giant tree have their bit cleared after the
+ * key sort (k_mask_fix).  The thread owning row u stores pmask[u] whole.
+ * The raw cut count takes every valid entry outside u's own run. */
 template <int PMAX>
 __global__ void __launch_bounds__(kB) k_emit_ranges(EmitParams E)
 {
@@ -802,8 +798,7 @@ __global__ void __launch_bounds__(kB) k_emit_ranges(EmitParams E)
                 own = o[q + 1] - o[q];
                 continue;
             }
-            if (o[q + 1] - o[q] > __ldg(E.qcnt + u * (uint64_t)P + q))
-                bits |= 1u << q;
+            bits |= 1u << q;
         }
         raw += (uint64_t)(o[P < PMAX ? P : PMAX] - own);
         E.pmask[u] = bits;
@@ -1045,9 +1040,9 @@ __global__ void __launch_bounds__(kB) k_ng_emit(EmitParams E, const uint64_t *of
  * (counted by k_ng_count) are one flat list for their warp, each lane
  * taking every 32nd entry - the row of entry i is the first lane whose
  * inclusive count exceeds i - so short and long rows alike keep every lane
- * busy.  Each entry writes its key at the row's offset; the keys are
- * counted per (partition, remote row) once they are sorted
- * (k_qcnt_from_keys). */
+ * busy.  Each entry writes its key at the row's offset; once sorted, the
+ * keys of each (partition, remote row) settle that row's mask bit
+ * (k_mask_fix). */
 template <int PMAX>
 __global__ void __launch_bounds__(kB) k_ng_emit_runs(EmitParams E, const uint32_t *cnt,
                                                      const uint64_t *off)
@@ -1105,14 +1100,18 @@ __global__ void __launch_bounds__(kB) k_ng_emit_runs(EmitParams E, const uint32_
     }
 }
 
-/* qcnt[u*P + p] = the local-end keys (p, u, rep) with partition p and
- * remote row u - row u's entries in partition p whose vertex lies outside
- * p's giant tree (the graph is symmetric: v in p lists u, so u lists v).
- * The keys are sorted, so equal (p, u) sit together: the first lane of each
- * run within a warp adds the run's length. */
-__global__ void __launch_bounds__(kB) k_qcnt_from_keys(const uint64_t *__restrict__ keys,
-                                                       uint64_t count, int rb, int gb, int parts,
-                                                       uint32_t *qcnt)
+/* Clears bit p of pmask[u] when u's run in partition p holds no neighbour
+ * in p's giant tree.  The local-end keys (p, u, rep) hold one key per entry
+ * of u's run in p whose vertex lies outside that tree (the graph is
+ * symmetric: v in p lists u, so u lists v), so there are never more keys
+ * with (p, u) than the run has entries, and as many exactly when none of
+ * them is in the tree.  The keys are sorted, so those with (p, u) sit
+ * together: the first of them compares the key as many places on as the
+ * run is long (from the offsets) - it still has (p, u) only then. */
+__global__ void __launch_bounds__(kB) k_mask_fix(const uint64_t *__restrict__ keys,
+                                                 uint64_t count, int rb, int gb, int parts,
+                                                 const uint32_t *__restrict__ roff,
+                                                 uint32_t *pmask)
 {
     const int lane = threadIdx.x & 31;
     const uint64_t stride = (uint64_t)gridDim.x * kB;
@@ -1122,18 +1121,18 @@ __global__ void __launch_bounds__(kB) k_qcnt_from_keys(const uint64_t *__restric
         const uint64_t i = base + lane;
         const bool ok = i < count;
         const uint64_t pu = ok ? __ldg(keys + i) >> rb : ~0ull;
-        /* runs of equal (p, u) among the warp's keys: each run's first lane
-         * adds the run's length */
-        const uint64_t before = __shfl_up_sync(0xffffffffu, pu, 1);
-        const bool head = ok && (lane == 0 || pu != before);
-        const unsigned heads = __ballot_sync(0xffffffffu, head);
-        const unsigned valid = __ballot_sync(0xffffffffu, ok);
-        if (head) {
-            const unsigned later = heads & ~((2u << lane) - 1u);
-            const int next = later ? __ffs(later) - 1 : 32 - __clz(valid);
-            const uint64_t u = pu & umask, p = pu >> gb;
-            atomicAdd(qcnt + u * (uint64_t)parts + p, (uint32_t)(next - lane));
-        }
+        uint64_t before = __shfl_up_sync(0xffffffffu, pu, 1);
+        if (lane == 0)
+            before = ok && i > 0 ? __ldg(keys + i - 1) >> rb : ~0ull;
+        if (!ok || pu == before)
+            continue;
+        const uint32_t u = (uint32_t)(pu & umask);
+        const int p = (int)(pu >> gb);
+        const uint32_t *r = roff + (uint64_t)u * parts;
+        const uint32_t len = __ldg(r + p) - (p ? __ldg(r + p - 1) : 0u);
+        const uint64_t last = i + len - 1;
+        if (len > 0 && last < count && (__ldg(keys + last) >> rb) == pu)
+            atomicAnd(pmask + u, ~(1u << p));
     }
 }
 
@@ -2651,6 +2650,8 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
     EmitParams E;
     unsigned long long hc[7];
     bool sorted_mode = false;
+    bool run_masks = false; /* remote-end masks from the row runs, settled
+                             * after the key sort by k_mask_fix */
     for (int pass = 0;; ++pass) {
         clk.n = 2 < clk.n ? 2 : clk.n; /* a second pass re-records phases 2-3 */
         const uint64_t *l_rp = d_row_ptr, *l_end = nullptr;
@@ -2845,11 +2846,8 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
             }
             return CCGPU_OK;
         };
-        E.qcnt = nullptr;
-        if (sorted_mode && ranges) {
-            CC_TRY(cc_bufs_get(&B, (void **)&E.qcnt, (size_t)n * P * sizeof(uint32_t)));
-            CC_CUDA(cudaMemsetAsync(E.qcnt, 0, (size_t)n * P * sizeof(uint32_t), st));
-        } else if (sorted_mode) {
+        run_masks = sorted_mode && ranges;
+        if (sorted_mode && !ranges) {
             const size_t words = (size_t)((m + 31) / 32);
             CC_TRY(cc_bufs_get(&B, (void **)&E.ngbits, words * 4));
             CC_CUDA(cudaMemsetAsync(E.ngbits, 0, words * 4, st));
@@ -2877,7 +2875,7 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
         if (sorted_mode && redo) {
             E.ngbits = nullptr;
             E.roff = nullptr;
-            E.qcnt = nullptr;
+            run_masks = false;
             CC_CUDA(cudaMemsetAsync(counters, 0, sizeof(unsigned long long), st));
             CC_CUDA(cudaMemsetAsync(counters + 4, 0, sizeof(unsigned long long), st));
             CC_CUDA(cudaMemsetAsync(counters + 6, 0, sizeof(unsigned long long), st));
@@ -2908,18 +2906,18 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
                                  st));
     }
     uint64_t R_all = R;
-    if (E.roff && E.qcnt) {
-        /* row-run mode: the remote end's masks from the counts of the
-         * sorted local-end keys */
-        if (R > 0)
-            CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_qcnt_from_keys,
-                       cc_blocks(R, kB, (unsigned)ctx->sm_count * 8), kB, 0, st,
-                       (const uint64_t *)sorted, R, rb, gb, P, E.qcnt);
+    if (E.roff && run_masks) {
+        /* row-run mode: a mask bit for every foreign run, cleared where the
+         * sorted local-end keys cover the whole run */
         const unsigned lb = cc_blocks(n, kB, (unsigned)ctx->sm_count * 8);
         if (P <= 4)
             CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit_ranges<4>, lb, kB, 0, st, E);
         else
             CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit_ranges<8>, lb, kB, 0, st, E);
+        if (R > 0)
+            CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_mask_fix,
+                       cc_blocks(R, kB, (unsigned)ctx->sm_count * 8), kB, 0, st,
+                       (const uint64_t *)sorted, R, rb, gb, P, E.roff, E.pmask);
         unsigned long long raw = 0;
         CC_CUDA(cudaMemcpyAsync(&raw, counters + 4, sizeof(raw), cudaMemcpyDeviceToHost, st));
         CC_CUDA(cudaStreamSynchronize(st));
