@@ -988,27 +988,41 @@ __device__ __forceinline__ void cut_runs(const EmitParams &E, uint32_t v, int pv
     c1 = b + __ldg(r + E.parts - 1);
 }
 
+/* cnt[v] = the cut entries of row v; with wcnt also one total per 32
+ * consecutive rows (the rows k_ng_emit_runs gives one warp). */
 template <int PMAX>
-__global__ void __launch_bounds__(kB) k_ng_count(EmitParams E, uint32_t *cnt)
+__global__ void __launch_bounds__(kB) k_ng_count(EmitParams E, uint32_t *cnt, uint32_t *wcnt)
 {
     NG_PROLOGUE;
-    for (uint64_t v = (uint64_t)blockIdx.x * kB + threadIdx.x; v < E.n; v += stride) {
-        uint64_t b, e;
-        int pv;
+    const int lane = threadIdx.x & 31;
+    for (uint64_t base = (uint64_t)blockIdx.x * kB + (threadIdx.x & ~31u); base < E.n;
+         base += stride) {
+        const uint64_t v = base + lane;
         uint32_t c = 0;
-        if (ng_row<PMAX>(E, s_b, sb, (uint32_t)v, b, e, pv)) {
-            if (E.roff) {
-                uint64_t a1, c0, c1;
-                cut_runs(E, (uint32_t)v, pv, b, a1, c0, c1);
-                c = (uint32_t)((a1 - b) + (c1 - c0));
-            } else {
-                for (uint64_t j = b; j < e; ++j) {
-                    const uint32_t u = __ldg(E.col + j);
-                    c += u < E.n && part_fast<PMAX>(s_b, sb, E.parts, u) != pv;
+        if (v < E.n) {
+            uint64_t b, e;
+            int pv;
+            if (ng_row<PMAX>(E, s_b, sb, (uint32_t)v, b, e, pv)) {
+                if (E.roff) {
+                    uint64_t a1, c0, c1;
+                    cut_runs(E, (uint32_t)v, pv, b, a1, c0, c1);
+                    c = (uint32_t)((a1 - b) + (c1 - c0));
+                } else {
+                    for (uint64_t j = b; j < e; ++j) {
+                        const uint32_t u = __ldg(E.col + j);
+                        c += u < E.n && part_fast<PMAX>(s_b, sb, E.parts, u) != pv;
+                    }
                 }
             }
+            cnt[v] = c;
         }
-        cnt[v] = c;
+        if (wcnt) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+                c += __shfl_xor_sync(0xffffffffu, c, o);
+            if (lane == 0)
+                wcnt[base / 32] = c;
+        }
     }
 }
 
@@ -1045,7 +1059,7 @@ __global__ void __launch_bounds__(kB) k_ng_emit(EmitParams E, const uint64_t *of
  * (k_mask_fix). */
 template <int PMAX>
 __global__ void __launch_bounds__(kB) k_ng_emit_runs(EmitParams E, const uint32_t *cnt,
-                                                     const uint64_t *off)
+                                                     const uint64_t *woff)
 {
     NG_PROLOGUE;
     (void)stride;
@@ -1064,7 +1078,7 @@ __global__ void __launch_bounds__(kB) k_ng_emit_runs(EmitParams E, const uint32_
                 incl += y;
         }
         const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-        const uint64_t o0 = __ldg(off + base);
+        const uint64_t o0 = __ldg(woff + base / 32);
         uint64_t b = 0, a1 = 0, c0 = 0;
         int pv = 0;
         uint32_t rep = 0;
@@ -2759,7 +2773,8 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
         if (use_mask) {
             CC_TRY(cc_bufs_get(&B, (void **)&E.gflag, (((size_t)n + 31) / 32) * 4));
             CC_TRY(cc_bufs_get(&B, (void **)&E.pmask, (size_t)n * 4));
-            CC_CUDA(cudaMemsetAsync(E.pmask, 0, (size_t)n * 4, st));
+            if (!(ranges && P > 1 && P < 32)) /* else k_emit_ranges writes every word */
+                CC_CUDA(cudaMemsetAsync(E.pmask, 0, (size_t)n * 4, st));
             E.giants = ls.giants;
             CC_KLAUNCH(ctx, CCK_DIST_GFLAG, k_giant_flags,
                        cc_blocks(n, kB, (unsigned)ctx->sm_count * 8), kB, 0, st, E);
@@ -2776,35 +2791,56 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
         sorted_mode = use_mask && P > 1 && P < 32 && (ranges || col_tiles > 0);
         auto emit = [&]() -> int {
             const unsigned lb = cc_blocks(n, kB, (unsigned)ctx->sm_count * 8);
-            if (E.roff || E.ngbits) {
+            if (E.roff) {
+                /* row-run mode: the cut entries of every row and of every
+                 * warp's 32 rows, a scan over the warps only (2M entries on
+                 * C3 rather than one per row), and the emit pass; the remote
+                 * end (k_emit_ranges, k_mask_fix) runs once the keys are
+                 * sorted */
+                const uint64_t nw = ((uint64_t)n + 31) / 32;
+                uint32_t *cnt = nullptr, *wcnt = nullptr;
+                uint64_t *woff = nullptr;
+                CC_TRY(cc_bufs_get(&B, (void **)&cnt, (size_t)n * sizeof(uint32_t)));
+                CC_TRY(cc_bufs_get(&B, (void **)&wcnt, (size_t)nw * sizeof(uint32_t)));
+                CC_TRY(cc_bufs_get(&B, (void **)&woff, ((size_t)nw + 1) * sizeof(uint64_t)));
+                if (P <= 4)
+                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_count<4>, lb, kB, 0, st, E, cnt,
+                               wcnt);
+                else
+                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_count<8>, lb, kB, 0, st, E, cnt,
+                               wcnt);
+                CC_TRY(cc_scan_u32(ctx, wcnt, woff, nw, &B, st));
+                const unsigned wlb = cc_blocks(nw, kW, (unsigned)ctx->sm_count * 8);
+                if (P <= 4)
+                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_emit_runs<4>, wlb, kB, 0, st, E,
+                               (const uint32_t *)cnt, (const uint64_t *)woff);
+                else
+                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_emit_runs<8>, wlb, kB, 0, st, E,
+                               (const uint32_t *)cnt, (const uint64_t *)woff);
+                CC_CUDA(cudaMemcpyAsync(E.count, woff + nw, sizeof(unsigned long long),
+                                        cudaMemcpyDeviceToDevice, st));
+            } else if (E.ngbits) {
                 uint32_t *cnt = nullptr;
                 uint64_t *off = nullptr, *work = nullptr;
                 CC_TRY(cc_bufs_get(&B, (void **)&cnt, (size_t)n * sizeof(uint32_t)));
                 CC_TRY(cc_bufs_get(&B, (void **)&off, ((size_t)n + 1) * sizeof(uint64_t)));
                 if (P <= 4)
-                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_count<4>, lb, kB, 0, st, E, cnt);
+                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_count<4>, lb, kB, 0, st, E, cnt,
+                               (uint32_t *)nullptr);
                 else if (P <= 8)
-                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_count<8>, lb, kB, 0, st, E, cnt);
+                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_count<8>, lb, kB, 0, st, E, cnt,
+                               (uint32_t *)nullptr);
                 else
                     CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_count<CCGPU_MAX_PARTS>, lb, kB, 0,
-                               st, E, cnt);
+                               st, E, cnt, (uint32_t *)nullptr);
                 CC_TRY(cc_scan_u32(ctx, cnt, off, n, &B, st));
                 unsigned long long items = 0;
-                if (!E.roff) {
-                    CC_CUDA(cudaMemcpyAsync(&items, off + n, sizeof(items),
-                                            cudaMemcpyDeviceToHost, st));
-                    CC_CUDA(cudaStreamSynchronize(st));
-                }
+                CC_CUDA(cudaMemcpyAsync(&items, off + n, sizeof(items), cudaMemcpyDeviceToHost,
+                                        st));
+                CC_CUDA(cudaStreamSynchronize(st));
                 CC_TRY(cc_bufs_get(&B, (void **)&work,
                                    (size_t)(items ? items : 1) * sizeof(uint64_t)));
-                const unsigned wlb = cc_blocks((n + 31) / 32, kW, (unsigned)ctx->sm_count * 8);
-                if (E.roff && P <= 4)
-                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_emit_runs<4>, wlb, kB, 0, st, E,
-                               (const uint32_t *)cnt, (const uint64_t *)off);
-                else if (E.roff)
-                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_emit_runs<8>, wlb, kB, 0, st, E,
-                               (const uint32_t *)cnt, (const uint64_t *)off);
-                else if (P <= 4)
+                if (P <= 4)
                     CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_emit<4>, lb, kB, 0, st, E, off,
                                work);
                 else if (P <= 8)
@@ -2815,23 +2851,17 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
                                st, E, off, work);
                 CC_CUDA(cudaMemcpyAsync(E.count, off + n, sizeof(unsigned long long),
                                         cudaMemcpyDeviceToDevice, st));
-                if (E.roff) {
-                    /* the remote end (k_emit_ranges) runs once the local
-                     * end's keys are sorted, from their counts */
-                } else {
-                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_mark, lb, kB, 0, st, E, work,
-                               off + n);
-                    const unsigned wb = cc_blocks(wtiles, kW, (unsigned)ctx->sm_count * 8);
-                    if (P <= 4)
-                        CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit_sorted<4>, wb, kB, 0, st, E,
-                                   wt_first, wtiles);
-                    else if (P <= 8)
-                        CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit_sorted<8>, wb, kB, 0, st, E,
-                                   wt_first, wtiles);
-                    else
-                        CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit_sorted<CCGPU_MAX_PARTS>, wb, kB, 0,
-                                   st, E, wt_first, wtiles);
-                }
+                CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_mark, lb, kB, 0, st, E, work, off + n);
+                const unsigned wb = cc_blocks(wtiles, kW, (unsigned)ctx->sm_count * 8);
+                if (P <= 4)
+                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit_sorted<4>, wb, kB, 0, st, E, wt_first,
+                               wtiles);
+                else if (P <= 8)
+                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit_sorted<8>, wb, kB, 0, st, E, wt_first,
+                               wtiles);
+                else
+                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS, k_emit_sorted<CCGPU_MAX_PARTS>, wb, kB, 0,
+                               st, E, wt_first, wtiles);
             } else {
                 CC_TRY(tiles_of());
                 E.tiles = col_tiles;
