@@ -988,41 +988,46 @@ __device__ __forceinline__ void cut_runs(const EmitParams &E, uint32_t v, int pv
     c1 = b + __ldg(r + E.parts - 1);
 }
 
-/* cnt[v] = the cut entries of row v; with wcnt also one total per 32
- * consecutive rows (the rows k_ng_emit_runs gives one warp). */
 template <int PMAX>
-__global__ void __launch_bounds__(kB) k_ng_count(EmitParams E, uint32_t *cnt, uint32_t *wcnt)
+__global__ void __launch_bounds__(kB) k_ng_count(EmitParams E, uint32_t *cnt)
 {
     NG_PROLOGUE;
-    const int lane = threadIdx.x & 31;
-    for (uint64_t base = (uint64_t)blockIdx.x * kB + (threadIdx.x & ~31u); base < E.n;
-         base += stride) {
-        const uint64_t v = base + lane;
+    for (uint64_t v = (uint64_t)blockIdx.x * kB + threadIdx.x; v < E.n; v += stride) {
+        uint64_t b, e;
+        int pv;
         uint32_t c = 0;
-        if (v < E.n) {
-            uint64_t b, e;
-            int pv;
-            if (ng_row<PMAX>(E, s_b, sb, (uint32_t)v, b, e, pv)) {
-                if (E.roff) {
-                    uint64_t a1, c0, c1;
-                    cut_runs(E, (uint32_t)v, pv, b, a1, c0, c1);
-                    c = (uint32_t)((a1 - b) + (c1 - c0));
-                } else {
-                    for (uint64_t j = b; j < e; ++j) {
-                        const uint32_t u = __ldg(E.col + j);
-                        c += u < E.n && part_fast<PMAX>(s_b, sb, E.parts, u) != pv;
-                    }
+        if (ng_row<PMAX>(E, s_b, sb, (uint32_t)v, b, e, pv)) {
+            if (E.roff) {
+                uint64_t a1, c0, c1;
+                cut_runs(E, (uint32_t)v, pv, b, a1, c0, c1);
+                c = (uint32_t)((a1 - b) + (c1 - c0));
+            } else {
+                for (uint64_t j = b; j < e; ++j) {
+                    const uint32_t u = __ldg(E.col + j);
+                    c += u < E.n && part_fast<PMAX>(s_b, sb, E.parts, u) != pv;
                 }
             }
-            cnt[v] = c;
         }
-        if (wcnt) {
+        cnt[v] = c;
+    }
+}
+
+/* wcnt[w] = cnt[32w] + ... + cnt[32w + 31] (to n): the rows k_ng_emit_runs
+ * gives one warp.  One warp per group, a coalesced 128-byte read each. */
+__global__ void __launch_bounds__(kB) k_warp_sums(const uint32_t *__restrict__ cnt, uint64_t n,
+                                                  uint32_t *wcnt)
+{
+    const int lane = threadIdx.x & 31;
+    const uint64_t nw = (n + 31) / 32;
+    const uint64_t wstride = (uint64_t)gridDim.x * kW;
+    for (uint64_t w = (uint64_t)blockIdx.x * kW + (threadIdx.x >> 5); w < nw; w += wstride) {
+        const uint64_t v = w * 32 + lane;
+        uint32_t c = v < n ? __ldg(cnt + v) : 0u;
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1)
-                c += __shfl_xor_sync(0xffffffffu, c, o);
-            if (lane == 0)
-                wcnt[base / 32] = c;
-        }
+        for (int o = 16; o > 0; o >>= 1)
+            c += __shfl_xor_sync(0xffffffffu, c, o);
+        if (lane == 0)
+            wcnt[w] = c;
     }
 }
 
@@ -2792,9 +2797,9 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
         auto emit = [&]() -> int {
             const unsigned lb = cc_blocks(n, kB, (unsigned)ctx->sm_count * 8);
             if (E.roff) {
-                /* row-run mode: the cut entries of every row and of every
-                 * warp's 32 rows, a scan over the warps only (2M entries on
-                 * C3 rather than one per row), and the emit pass; the remote
+                /* row-run mode: the cut entries of every row, their sums
+                 * per warp's 32 rows, a scan over the warps only (2M entries
+                 * on C3 rather than one per row), and the emit pass; the remote
                  * end (k_emit_ranges, k_mask_fix) runs once the keys are
                  * sorted */
                 const uint64_t nw = ((uint64_t)n + 31) / 32;
@@ -2804,13 +2809,13 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
                 CC_TRY(cc_bufs_get(&B, (void **)&wcnt, (size_t)nw * sizeof(uint32_t)));
                 CC_TRY(cc_bufs_get(&B, (void **)&woff, ((size_t)nw + 1) * sizeof(uint64_t)));
                 if (P <= 4)
-                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_count<4>, lb, kB, 0, st, E, cnt,
-                               wcnt);
+                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_count<4>, lb, kB, 0, st, E, cnt);
                 else
-                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_count<8>, lb, kB, 0, st, E, cnt,
-                               wcnt);
-                CC_TRY(cc_scan_u32(ctx, wcnt, woff, nw, &B, st));
+                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_count<8>, lb, kB, 0, st, E, cnt);
                 const unsigned wlb = cc_blocks(nw, kW, (unsigned)ctx->sm_count * 8);
+                CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_warp_sums, wlb, kB, 0, st,
+                           (const uint32_t *)cnt, (uint64_t)n, wcnt);
+                CC_TRY(cc_scan_u32(ctx, wcnt, woff, nw, &B, st));
                 if (P <= 4)
                     CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_emit_runs<4>, wlb, kB, 0, st, E,
                                (const uint32_t *)cnt, (const uint64_t *)woff);
@@ -2825,14 +2830,12 @@ static int dist_run(ccgpu_ctx *ctx, const uint64_t *d_row_ptr, const uint32_t *d
                 CC_TRY(cc_bufs_get(&B, (void **)&cnt, (size_t)n * sizeof(uint32_t)));
                 CC_TRY(cc_bufs_get(&B, (void **)&off, ((size_t)n + 1) * sizeof(uint64_t)));
                 if (P <= 4)
-                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_count<4>, lb, kB, 0, st, E, cnt,
-                               (uint32_t *)nullptr);
+                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_count<4>, lb, kB, 0, st, E, cnt);
                 else if (P <= 8)
-                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_count<8>, lb, kB, 0, st, E, cnt,
-                               (uint32_t *)nullptr);
+                    CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_count<8>, lb, kB, 0, st, E, cnt);
                 else
                     CC_KLAUNCH(ctx, CCK_DIST_PAIRS_LOCAL, k_ng_count<CCGPU_MAX_PARTS>, lb, kB, 0,
-                               st, E, cnt, (uint32_t *)nullptr);
+                               st, E, cnt);
                 CC_TRY(cc_scan_u32(ctx, cnt, off, n, &B, st));
                 unsigned long long items = 0;
                 CC_CUDA(cudaMemcpyAsync(&items, off + n, sizeof(items), cudaMemcpyDeviceToHost,
