@@ -548,10 +548,10 @@ NCU_TRAFFIC = {
     # scale 22 (4,194,304 vertices)
     "sample": {"per": "vertex", "bytes_per_unit": 103_996_544 / 4_194_304,
                "source": "profiles/local_cc_sample_stash_rmat22_ncu.md"},
-    # k_row_scan<4> on R-MAT scale 22 with 4 partitions: 675.1 MB moved for
+    # k_row_scan<4> on R-MAT scale 22 with 4 partitions: 671.7 MB moved for
     # 681.0 MB of algorithmic bytes (its traffic follows both n and m, so it
     # scales as a fraction of the launch's algorithmic bytes)
-    "dist_local_count": {"per": "algorithmic", "bytes_per_unit": 675_100_160 / 681_006_024,
+    "dist_local_count": {"per": "algorithmic", "bytes_per_unit": 671_661_568 / 681_006_024,
                          "source": "profiles/dist_row_scan_rmat22p4_ncu.md"},
 }
 
