@@ -1059,9 +1059,9 @@ __global__ void __launch_bounds__(kB) k_ng_emit(EmitParams E, const uint64_t *of
  * (counted by k_ng_count) are one flat list for their warp, each lane
  * taking every 32nd entry - the row of entry i is the first lane whose
  * inclusive count exceeds i - so short and long rows alike keep every lane
- * busy.  Each entry writes its key at the row's offset; once sorted, the
- * keys of each (partition, remote row) settle that row's mask bit
- * (k_mask_fix). */
+ * busy.  The warp's keys start at woff[warp's first row / 32], the scan of
+ * the per-warp sums (k_warp_sums); once sorted, the keys of each
+ * (partition, remote row) settle that row's mask bit (k_mask_fix). */
 template <int PMAX>
 __global__ void __launch_bounds__(kB) k_ng_emit_runs(EmitParams E, const uint32_t *cnt,
                                                      const uint64_t *woff)
